@@ -1,0 +1,219 @@
+/*
+ * libubolt_b200 - the B200 (sm_100a) fixed-source discrete-ordinates solve of
+ * UBOLT behind a C ABI.
+ *
+ * Every entry point returns an int status: UBOLT_OK (0) or a UBOLT_ERR_*
+ * code, with a message from ubolt_last_error() (thread-local). No entry point
+ * throws across the boundary.
+ *
+ * Vectors over the phase space are caller-owned DEVICE memory in UBOLT's row
+ * layout, row = (cell * n_basis + basis) * n_angles + angle, angle fastest
+ * (include/ubolt/phase_space.hpp:20-28). A (cell, basis) pair is a node and
+ * owns a contiguous run of n_angles rows. Every kernel runs on the stream the
+ * caller passes (a cudaStream_t as void *; NULL is the legacy default stream);
+ * nothing is synchronised unless the entry point says so, and no apply, block
+ * apply, rhs fill or sweep allocates device memory or copies host<->device
+ * (AGENTS.md:44-47 of the reference states the same contract).
+ *
+ * Each declaration cites the reference interface it replaces, as
+ * path:line within stevendargaville/UBOLT.
+ */
+#ifndef UBOLT_B200_H
+#define UBOLT_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+   UBOLT_OK = 0,
+   UBOLT_ERR_ARG = 1,           /* bad argument / size mismatch (PETSC_ERR_ARG_*) */
+   UBOLT_ERR_CUDA = 2,          /* a CUDA runtime call failed */
+   UBOLT_ERR_SINGULAR = 3,      /* singular element block (PETSC_ERR_MAT_LU_ZRPVT) */
+   UBOLT_ERR_STATE = 4,         /* called out of order (PETSC_ERR_ARG_WRONGSTATE) */
+   UBOLT_ERR_NOT_CONVERGED = 5, /* the solve hit its iteration limit */
+   UBOLT_ERR_TIMEOUT = 6,       /* a bounded device-side wait gave up */
+   UBOLT_ERR_NOMEM = 7,         /* device allocation failed at set-up */
+   UBOLT_ERR_BREAKDOWN = 8,     /* Krylov breakdown */
+   UBOLT_ERR_NONFINITE = 9      /* NaN / Inf met in a residual */
+};
+
+/* Cell shapes a mesh may hold (one shape per mesh). */
+enum { UBOLT_TRI = 3, UBOLT_QUAD = 4, UBOLT_TET = 10, UBOLT_HEX = 12 };
+
+/* Boundary families per box side (bc_spec.hpp:11-40): vacuum (ghost-flux
+ * inflow) or reflective (must be axis-aligned). */
+enum { UBOLT_BC_VACUUM = 0, UBOLT_BC_REFLECT = 1 };
+
+const char *ubolt_last_error(void);
+const char *ubolt_version(void);
+
+/* ~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~
+ * Angular quadrature (host)
+ * ~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~ */
+
+/* One octant of the level-symmetric set of order S2..S18: level cosines
+ * (n_levels), the lexicographic level triples (3 * n_points, 1-based) and
+ * each point's weight as a fraction of the whole sphere. Any output may be
+ * NULL. Replaces the generated table src/sn_lqn_table.hpp:55-368. */
+int ubolt_lqn_octant(int sn_order, double *mu, int *points, double *weight, int *n_levels, int *n_points);
+
+/* The 2D (XY, xi > 0 half, doubled weights) or 3D LQn ordinate set:
+ * omega (3 * A, xi = 0 in 2D), w (A), reflect (3 * A: the partner with cosine
+ * d negated, -1 past dim). Call with all three NULL to size A. sum_weights is
+ * the exact 4 pi. Replaces SNQuadrature2D/3D::create
+ * (src/sn_quadraturek.kokkos.cxx:309-427, include/ubolt/sn_quadrature.hpp:93-159). */
+int ubolt_quadrature_lqn(int dim, int sn_order, double *omega, double *w, int *reflect, int *n_angles,
+                         double *sum_weights);
+
+/* ~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~
+ * DG geometry (host). The data UnstructuredDG::create builds
+ * (include/ubolt/unstructured_dg.hpp:73-128), flat and per (cell, face slot)
+ * with every cell owning exactly faces_per_cell slots.
+ * ~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~ */
+typedef struct {
+   int32_t dim;            /* 2 or 3 */
+   int32_t n_basis;        /* 1 (DG0) or dim + 1 (DG1, orthonormal modal P1) */
+   int32_t faces_per_cell; /* F */
+   int32_t pad_;
+   int64_t n_cells;
+   const double *volume;         /* [n_cells] (fan volume at DG1) */
+   const double *centroid;       /* [n_cells * 3] */
+   const double *face_nA;        /* [n_cells * F * 3] outward area-weighted normal, z = 0 in 2D */
+   const int64_t *face_neighbour;/* [n_cells * F] neighbour cell, -1 on the boundary */
+   const int32_t *face_bc;       /* [n_cells * F] -1 interior, else UBOLT_BC_* of its side */
+   const int32_t *face_side;     /* [n_cells * F] boundary side 2 * axis + (0 low | 1 high), -1 interior */
+   const int32_t *face_axis;     /* [n_cells * F] dominant axis of the normal */
+   const double *face_centroid;  /* [n_cells * F * 3] */
+   const double *face_distance;  /* [n_cells * F * 2] centroid-to-face (own, neighbour) */
+   /* DG1 only, NULL at DG0 */
+   const double *face_own;       /* [n_cells * F * nb * nb] (1/(V A)) int_f phi_i phi_j, own basis */
+   const double *face_up;        /* [n_cells * F * nb * nb] the same against the upwind basis, 0 on vacuum */
+   const double *basis_grad;     /* [n_cells * nb * 3] grad phi_i (0 for i = 0) */
+   const double *face_neighbour_grad; /* [n_cells * F * nb * 3] the neighbour's grad phi_j, 0 on the boundary */
+   const double *face_basis_value;    /* [n_cells * F * nb] phi_i at the face centroid */
+} ubolt_dg_geometry;
+
+typedef struct ubolt_geometry_owned ubolt_geometry_owned;
+
+/* Build the DG0/DG1 geometry of a conforming mesh of one cell shape
+ * (UBOLT_TRI/QUAD in 2D, UBOLT_TET/HEX in 3D): vertices [n_vertices * dim],
+ * cell_vertices [n_cells * verts_per_cell] (tri/quad/hex in the usual
+ * counter-clockwise / bottom-then-top order, any tet orientation).
+ * side_bc[2 * dim] gives each box side's family, the box being the vertices'
+ * bounding box. Restates UnstructuredDG::create and build_dg1_geometry
+ * (src/unstructured_dgk.kokkos.cxx:27-218, 224-411, 706-821) with this
+ * library's own face enumeration in place of DMPlex cones. */
+int ubolt_geometry_build(int dim, int cell_type, int64_t n_vertices, const double *vertices, int64_t n_cells,
+                         const int64_t *cell_vertices, int order, const int32_t *side_bc,
+                         ubolt_geometry_owned **out);
+int ubolt_geometry_view(const ubolt_geometry_owned *g, ubolt_dg_geometry *view);
+void ubolt_geometry_free(ubolt_geometry_owned *g);
+
+/* ~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~
+ * Device context: the geometry and ordinates uploaded once
+ * ~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~ */
+typedef struct {
+   int32_t dim;
+   int32_t n_angles;
+   double sum_weights;    /* W: 4 pi for the LQn sets */
+   const double *omega;   /* [A * 3] */
+   const double *w;       /* [A] */
+   const int32_t *reflect;/* [3 * A] */
+} ubolt_quadrature;
+
+typedef struct ubolt_ctx ubolt_ctx;
+
+/* Upload geometry and ordinates to the current CUDA device (FP64 and FP32
+ * copies) and allocate the per-group FP32 cross-section slots. Replaces the
+ * device copies of UnstructuredDG::create (src/unstructured_dgk.kokkos.cxx:
+ * 585-661) and the term creates (src/termsk.kokkos.cxx:276-312, 541-572). */
+int ubolt_ctx_create(const ubolt_dg_geometry *geom, const ubolt_quadrature *quad, ubolt_ctx **ctx);
+int ubolt_ctx_destroy(ubolt_ctx *ctx);
+/* Rows, nodes and cells of the phase space (phase_space.hpp:44-50). */
+int ubolt_ctx_sizes(const ubolt_ctx *ctx, int64_t *rows, int64_t *nodes, int64_t *cells, int32_t *n_basis,
+                    int32_t *n_angles);
+
+/* Point the operator at a group's cross sections: DEVICE arrays of n_cells
+ * doubles, not owned, which must outlive their use (RemovalTerm::set_group /
+ * ScatteringTerm::set_group, src/termsk.kokkos.cxx:437-443, 574-579;
+ * DSAPrecon::set_group, dsa.hpp:92-93). Refreshes the FP32 copies on
+ * `stream` - no allocation. */
+int ubolt_set_group(ubolt_ctx *ctx, const double *sigma_t, const double *sigma_s_within, void *stream);
+
+/* ~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~
+ * Operator applies (the MatShell MULT). One fused pass: streaming + removal -
+ * scatter, matrix-free. y and x must not alias.
+ * ~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~ */
+
+/* y = (L - S) x. ShellMatMultApply, src/transport_operatork.kokkos.cxx:49-61
+ * (assembled StreamingTermDG0/DG1 + RemovalTerm, termsk.kokkos.cxx:170-539,
+ * plus ScatteringTerm::apply_add, termsk.kokkos.cxx:584-649). */
+int ubolt_apply(ubolt_ctx *ctx, const double *x, double *y, void *stream);
+int ubolt_apply_f32(ubolt_ctx *ctx, const float *x, float *y, void *stream);
+/* y = L x, no scatter. UnscatteredMatMultApply, transport_operatork.kokkos.cxx:66-78. */
+int ubolt_apply_unscattered(ubolt_ctx *ctx, const double *x, double *y, void *stream);
+int ubolt_apply_unscattered_f32(ubolt_ctx *ctx, const float *x, float *y, void *stream);
+/* y = (L - S)^T x, the reversed-angle (downwind-gather) operator. No
+ * reference counterpart: the reference has no transpose apply
+ * (docs/architecture.md:493-494); its (V A)^T = P (V A) P identity
+ * (docs/architecture.md:284-304) is what the tests hold it to. */
+int ubolt_apply_adjoint(ubolt_ctx *ctx, const double *x, double *y, void *stream);
+int ubolt_apply_adjoint_f32(ubolt_ctx *ctx, const float *x, float *y, void *stream);
+
+/* d = the streaming + removal diagonal, bitwise the composition of
+ * DG0OutflowDiagonal / DG1OutflowDiagonal + sigma_t.
+ * TransportOperator::diagonal, transport_operatork.kokkos.cxx:240-256. */
+int ubolt_diagonal(ubolt_ctx *ctx, double *d, void *stream);
+
+/* ~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~
+ * Element blocks: the nb x nb (cell, angle) blocks of streaming + removal,
+ * rebuilt on the fly from geometry and sigma_t and inverted by Gauss-Jordan
+ * with partial pivoting per (cell, angle) - nothing is stored.
+ * ~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~ */
+
+/* Count singular blocks of the current group (ElementBlockInverse::setup,
+ * src/block_inversek.kokkos.cxx:249-299). Synchronises `stream`. Returns
+ * UBOLT_ERR_SINGULAR with the count when any is singular. */
+int ubolt_block_setup(ubolt_ctx *ctx, int64_t *n_singular, void *stream);
+/* y = D^{-1} x (RemovalPCApply -> ElementBlockInverse::apply,
+ * transport_solverk.kokkos.cxx:84-94, block_inversek.kokkos.cxx:206-222). */
+int ubolt_block_apply(ubolt_ctx *ctx, const double *x, double *y, void *stream);
+int ubolt_block_apply_f32(ubolt_ctx *ctx, const float *x, float *y, void *stream);
+/* y = D^{-T} x, the adjoint solve's removal stage (no reference counterpart). */
+int ubolt_block_apply_transpose(ubolt_ctx *ctx, const double *x, double *y, void *stream);
+/* The inverted blocks, ((c * A + a) * nb + i) * nb + j, into a device array
+ * of n_cells * A * nb * nb doubles (ElementBlockInverse::inverse_d, for tests:
+ * block_inverse.hpp:71-73). */
+int ubolt_block_inverse(ubolt_ctx *ctx, double *inv, void *stream);
+
+/* ~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~
+ * Angular moment and right-hand sides. Every rhs fill ADDS to b.
+ * ~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~ */
+
+/* phi(node) = sum_a w_a psi(node, a). UboltAngularIntegral,
+ * sn_quadrature.hpp:163-171, src/sn_quadraturek.kokkos.cxx:400-427. */
+int ubolt_scalar_flux(ubolt_ctx *ctx, const double *psi, double *phi, void *stream);
+int ubolt_scalar_flux_f32(ubolt_ctx *ctx, const float *psi, float *phi, void *stream);
+/* b(cell, basis 0, a) += q(cell) / W, q the angle-integrated isotropic
+ * source per cell (device, n_cells). MaterialSourceTable::add_isotropic,
+ * src/material_speck.kokkos.cxx:164-213. */
+int ubolt_add_source(ubolt_ctx *ctx, const double *q_cell, double *b, void *stream);
+/* b(node, a) += sigma_s(g' -> g)(cell) phi_g'(node) / W on every angle.
+ * GroupTransfer::add_transfer, src/multigroupk.kokkos.cxx:306-365. */
+int ubolt_add_transfer(ubolt_ctx *ctx, const double *phi_from, const double *sigma_s_from_to, double *b,
+                       void *stream);
+/* b(c, i, a) += -(s / V) phi_i(x_f) inflow[side] / W over every vacuum face
+ * the ordinate enters through, s = Omega_a . nA_f < 0; side_inflow[2 * dim]
+ * is each side's angle-integrated inflow (HOST array). The ghost-flux rhs of
+ * UboltFillInflow, src/discretisationk.kokkos.cxx:173-210, with the per-row
+ * values of src/unstructured_dgk.kokkos.cxx:476-494 built on the fly. */
+int ubolt_add_ghost_inflow(ubolt_ctx *ctx, const double *side_inflow, double *b, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

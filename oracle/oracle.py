@@ -1,0 +1,184 @@
+"""Python face of the CPU oracle - TEST INFRASTRUCTURE ONLY.
+
+Loads oracle/_build/liboracle.so (built by `make -C oracle`), the plain-C
+restatement of UBOLT's assembled operator in oracle/ubolt_oracle.c, and
+returns SciPy CSR matrices and NumPy vectors. Only tests/, the smoke check
+and bench.py's CPU baseline use this module; the library never does.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+import scipy.sparse as sp
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_build", "liboracle.so")
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB
+
+
+if not os.path.exists(LIB):
+    build()
+_lib = C.CDLL(LIB)
+
+dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+i64p = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
+i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+
+
+def _sig(name, restype, *args):
+    f = getattr(_lib, name)
+    f.restype = restype
+    f.argtypes = list(args)
+    return f
+
+
+_sig("oracle_dg_nnz_bound", C.c_int64, C.c_int, C.c_int, C.c_int64, C.c_int)
+_sig("oracle_assemble_dg", C.c_int64, C.c_int, C.c_int, C.c_int64, C.c_int, dp, i64p, i32p, i32p, dp, C.c_void_p,
+     C.c_void_p, C.c_void_p, dp, i32p, dp, i64p, i64p, dp)
+_sig("oracle_assemble_fd2d", C.c_int64, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, dp, dp, i32p, i32p, dp,
+     i64p, i64p, dp)
+_sig("oracle_spmv", None, C.c_int64, i64p, i64p, dp, dp, dp)
+_sig("oracle_angular_integral", None, C.c_int64, C.c_int, dp, dp, dp)
+_sig("oracle_scatter_add", None, C.c_int64, C.c_int, C.c_int, dp, C.c_double, dp, dp, dp)
+_sig("oracle_add_source", None, C.c_int64, C.c_int, C.c_int, C.c_double, dp, dp)
+_sig("oracle_add_transfer", None, C.c_int64, C.c_int, C.c_int, C.c_double, dp, dp, dp)
+_sig("oracle_ghost_inflow", None, C.c_int, C.c_int, C.c_int64, C.c_int, dp, i64p, i32p, i32p, dp, C.c_void_p, dp,
+     C.c_double, dp, dp)
+_sig("oracle_block_inverse", C.c_int64, C.c_int64, C.c_int, C.c_int, i64p, i64p, dp, dp)
+_sig("oracle_block_apply", None, C.c_int64, C.c_int, C.c_int, dp, dp, dp)
+_sig("oracle_solve", C.c_int, C.c_int64, C.c_int, C.c_int, i64p, i64p, dp, dp, C.c_double, dp, dp, dp, C.c_double,
+     C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double))
+_sig("oracle_sweep", None, C.c_int64, C.c_int, C.c_int, i64p, i64p, dp, dp, dp)
+_sig("oracle_threads", C.c_int)
+
+PC_NONE, PC_BLOCK, PC_SWEEP = 0, 1, 2
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class Operator:
+    """The assembled streaming + removal CSR of one group plus the matrix-free
+    scatter: the reference's TransportOperator shell, on the CPU."""
+
+    def __init__(self, geometry, quad, sigma_t, sigma_s):
+        g = geometry
+        self.nb, self.F, self.nc, self.A = g.n_basis, g.faces_per_cell, g.n_cells, quad.n_angles
+        self.n = self.nc * self.nb * self.A
+        self.quad = quad
+        self.sigma_t = np.ascontiguousarray(sigma_t, dtype=np.float64)
+        self.sigma_s = np.ascontiguousarray(sigma_s, dtype=np.float64)
+        cap = _lib.oracle_dg_nnz_bound(self.nb, self.F, self.nc, self.A)
+        row_ptr = np.zeros(self.n + 1, dtype=np.int64)
+        col = np.zeros(cap, dtype=np.int64)
+        val = np.zeros(cap)
+        dg1 = self.nb > 1
+        nnz = _lib.oracle_assemble_dg(self.nb, self.F, self.nc, self.A, g.face_nA, g.face_neighbour, g.face_bc,
+                                      g.face_axis, g.volume, _ptr(g.face_own) if dg1 else None,
+                                      _ptr(g.face_up) if dg1 else None, _ptr(g.basis_grad) if dg1 else None,
+                                      quad.omega.ravel(), quad.reflect.ravel(), self.sigma_t, row_ptr, col, val)
+        if nnz < 0:
+            raise MemoryError("oracle_assemble_dg")
+        self.L = sp.csr_matrix((val[:nnz], col[:nnz], row_ptr), shape=(self.n, self.n))
+        self.L.has_sorted_indices = True
+
+    def apply(self, x, scatter=True):
+        """y = (L - S) x, or L x."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.empty(self.n)
+        _lib.oracle_spmv(self.n, self.L.indptr.astype(np.int64), self.L.indices.astype(np.int64), self.L.data, x, y)
+        if scatter:
+            _lib.oracle_scatter_add(self.nc, self.nb, self.A, self.quad.w, self.quad.sum_weights, self.sigma_s, x, y)
+        return y
+
+    def scatter_matrix(self):
+        """S as a sparse matrix: S[(node, a), (node, b)] = sigma_s w_b / W."""
+        nn = self.nc * self.nb
+        w = self.quad.w / self.quad.sum_weights
+        blocks = np.repeat(self.sigma_s, self.nb)
+        rows = (np.arange(nn)[:, None, None] * self.A + np.arange(self.A)[None, :, None]).repeat(self.A, axis=2)
+        cols = (np.arange(nn)[:, None, None] * self.A + np.arange(self.A)[None, None, :]).repeat(self.A, axis=1)
+        vals = blocks[:, None, None] * np.broadcast_to(w[None, None, :], (nn, self.A, self.A))
+        return sp.csr_matrix((vals.ravel(), (rows.ravel(), cols.ravel())), shape=(self.n, self.n))
+
+    def matrix(self):
+        return (self.L - self.scatter_matrix()).tocsr()
+
+    def block_inverse(self):
+        inv = np.zeros(self.nc * self.A * self.nb * self.nb)
+        n_sing = _lib.oracle_block_inverse(self.nc, self.nb, self.A, self.L.indptr.astype(np.int64),
+                                           self.L.indices.astype(np.int64), self.L.data, inv)
+        return inv, n_sing
+
+    def block_apply(self, inv, x):
+        y = np.empty(self.n)
+        _lib.oracle_block_apply(self.nc, self.nb, self.A, inv, np.ascontiguousarray(x, dtype=np.float64), y)
+        return y
+
+    def sweep(self, q):
+        psi = np.empty(self.n)
+        _lib.oracle_sweep(self.nc, self.nb, self.A, self.L.indptr.astype(np.int64), self.L.indices.astype(np.int64),
+                          self.L.data, np.ascontiguousarray(q, dtype=np.float64), psi)
+        return psi
+
+    def solve(self, b, rtol=1e-12, max_it=2000, restart=30, pc=PC_SWEEP, x0=None):
+        x = np.zeros(self.n) if x0 is None else np.array(x0, dtype=np.float64)
+        res = C.c_double()
+        it = _lib.oracle_solve(self.nc, self.nb, self.A, self.L.indptr.astype(np.int64),
+                               self.L.indices.astype(np.int64), self.L.data, self.quad.w, self.quad.sum_weights,
+                               self.sigma_s, np.ascontiguousarray(b, dtype=np.float64), x, rtol, max_it, restart, pc,
+                               C.byref(res))
+        return x, it, res.value
+
+
+def angular_integral(psi, n_nodes, quad):
+    phi = np.empty(n_nodes)
+    _lib.oracle_angular_integral(n_nodes, quad.n_angles, quad.w, np.ascontiguousarray(psi, dtype=np.float64), phi)
+    return phi
+
+
+def rhs(geometry, quad, source_cell, side_inflow=None):
+    """b = ghost inflow + isotropic source, added onto zero as the driver does."""
+    g = geometry
+    n = g.n_cells * g.n_basis * quad.n_angles
+    b = np.zeros(n)
+    if side_inflow is not None and np.any(np.asarray(side_inflow) != 0.0):
+        inflow = np.zeros(6)
+        inflow[:len(side_inflow)] = side_inflow
+        _lib.oracle_ghost_inflow(g.n_basis, g.faces_per_cell, g.n_cells, quad.n_angles, g.face_nA, g.face_neighbour,
+                                 g.face_bc, g.face_side, g.volume,
+                                 _ptr(g.face_basis_value) if g.n_basis > 1 else None, quad.omega.ravel(),
+                                 quad.sum_weights, inflow, b)
+    _lib.oracle_add_source(g.n_cells, g.n_basis, quad.n_angles, quad.sum_weights,
+                           np.ascontiguousarray(source_cell, dtype=np.float64), b)
+    return b
+
+
+def add_transfer(b, phi, sigma_s, n_cells, nb, quad):
+    _lib.oracle_add_transfer(n_cells, nb, quad.n_angles, quad.sum_weights, np.ascontiguousarray(phi),
+                             np.ascontiguousarray(sigma_s, dtype=np.float64), b)
+    return b
+
+
+def fd2d(nx, ny, quad, sigma_t, side_bc=(0, 0, 0, 0), lx=1.0, ly=1.0):
+    """Streaming + removal of the structured 2D FD backend (ghost-flux rows)."""
+    A = quad.n_angles
+    n = nx * ny * A
+    row_ptr = np.zeros(n + 1, dtype=np.int64)
+    col = np.zeros(3 * n, dtype=np.int64)
+    val = np.zeros(3 * n)
+    nnz = _lib.oracle_assemble_fd2d(nx, ny, lx / nx, ly / ny, A, np.ascontiguousarray(quad.omega[:, 0]),
+                                    np.ascontiguousarray(quad.omega[:, 1]), quad.reflect.ravel(),
+                                    np.asarray(side_bc, dtype=np.int32), np.ascontiguousarray(sigma_t, dtype=np.float64),
+                                    row_ptr, col, val)
+    return sp.csr_matrix((val[:nnz], col[:nnz], row_ptr), shape=(n, n))
+
+
+def threads():
+    return _lib.oracle_threads()

@@ -1,0 +1,91 @@
+"""ctypes binding of libubolt_b200.so - the C ABI declared in include/ubolt_b200.h.
+
+The library is built in-tree (python -m ubolt_b200.build). There is no
+fallback: if the shared object is missing or does not load, importing this
+module raises.
+"""
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libubolt_b200.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(f"{LIB_PATH} is missing - build it with `python -m ubolt_b200.build`")
+lib = C.CDLL(LIB_PATH)
+
+OK = 0
+ERRORS = {1: "ARG", 2: "CUDA", 3: "SINGULAR", 4: "STATE", 5: "NOT_CONVERGED", 6: "TIMEOUT", 7: "NOMEM",
+          8: "BREAKDOWN", 9: "NONFINITE"}
+TRI, QUAD, TET, HEX = 3, 4, 10, 12
+BC_VACUUM, BC_REFLECT = 0, 1
+
+vp = C.c_void_p
+i32p = C.POINTER(C.c_int32)
+i64p = C.POINTER(C.c_int64)
+dp = C.POINTER(C.c_double)
+
+
+class UboltError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(f"UBOLT_ERR_{ERRORS.get(status, status)}: {message}")
+        self.status = status
+
+
+def check(status):
+    if status != OK:
+        raise UboltError(status, lib.ubolt_last_error().decode())
+    return status
+
+
+class DGGeometry(C.Structure):
+    _fields_ = [("dim", C.c_int32), ("n_basis", C.c_int32), ("faces_per_cell", C.c_int32), ("pad_", C.c_int32),
+                ("n_cells", C.c_int64),
+                ("volume", dp), ("centroid", dp), ("face_nA", dp), ("face_neighbour", i64p),
+                ("face_bc", i32p), ("face_side", i32p), ("face_axis", i32p), ("face_centroid", dp),
+                ("face_distance", dp), ("face_own", dp), ("face_up", dp), ("basis_grad", dp),
+                ("face_neighbour_grad", dp), ("face_basis_value", dp)]
+
+
+class Quadrature(C.Structure):
+    _fields_ = [("dim", C.c_int32), ("n_angles", C.c_int32), ("sum_weights", C.c_double),
+                ("omega", dp), ("w", dp), ("reflect", i32p)]
+
+
+def _sig(name, restype, *argtypes):
+    f = getattr(lib, name)
+    f.restype = restype
+    f.argtypes = list(argtypes)
+    return f
+
+
+_sig("ubolt_last_error", C.c_char_p)
+_sig("ubolt_version", C.c_char_p)
+_sig("ubolt_lqn_octant", C.c_int, C.c_int, dp, i32p, dp, i32p, i32p)
+_sig("ubolt_quadrature_lqn", C.c_int, C.c_int, C.c_int, dp, dp, i32p, i32p, dp)
+_sig("ubolt_geometry_build", C.c_int, C.c_int, C.c_int, C.c_int64, dp, C.c_int64, i64p, C.c_int, i32p,
+     C.POINTER(vp))
+_sig("ubolt_geometry_view", C.c_int, vp, C.POINTER(DGGeometry))
+_sig("ubolt_geometry_free", None, vp)
+_sig("ubolt_ctx_create", C.c_int, C.POINTER(DGGeometry), C.POINTER(Quadrature), C.POINTER(vp))
+_sig("ubolt_ctx_destroy", C.c_int, vp)
+_sig("ubolt_ctx_sizes", C.c_int, vp, i64p, i64p, i64p, i32p, i32p)
+_sig("ubolt_set_group", C.c_int, vp, vp, vp, vp)
+for _n in ("ubolt_apply", "ubolt_apply_f32", "ubolt_apply_unscattered", "ubolt_apply_unscattered_f32",
+           "ubolt_apply_adjoint", "ubolt_apply_adjoint_f32", "ubolt_block_apply", "ubolt_block_apply_f32",
+           "ubolt_block_apply_transpose", "ubolt_scalar_flux", "ubolt_scalar_flux_f32", "ubolt_add_source"):
+    _sig(_n, C.c_int, vp, vp, vp, vp)
+_sig("ubolt_diagonal", C.c_int, vp, vp, vp)
+_sig("ubolt_block_setup", C.c_int, vp, i64p, vp)
+_sig("ubolt_block_inverse", C.c_int, vp, vp, vp)
+_sig("ubolt_add_transfer", C.c_int, vp, vp, vp, vp, vp)
+_sig("ubolt_add_ghost_inflow", C.c_int, vp, dp, vp, vp)
+
+
+def declared_symbols(header=None):
+    """Every function name include/ubolt_b200.h declares."""
+    import re
+    header = header or os.path.join(os.path.dirname(_HERE), "include", "ubolt_b200.h")
+    text = open(header).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(ubolt_[a-z0-9_]+)\s*\(", text)))

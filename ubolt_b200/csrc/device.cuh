@@ -1,0 +1,166 @@
+// Device-side data layout and the per-(cell, angle) arithmetic shared by the
+// apply, block, sweep and adjoint kernels.
+//
+// HBM layout. Phase-space vectors keep UBOLT's row order (angle fastest), so
+// a cell's n_basis * n_angles values are one contiguous run. Geometry is
+// split into a per-CELL part - the face codes (neighbour or boundary side),
+// the mirror slot of each interior face, a geometry-class id - and a
+// per-CLASS part holding everything derived from shape: outward area
+// normals, face matrices, basis gradients, face basis values, volume. Cells
+// whose class data are bitwise equal share a class, so a uniform box reads
+// a few dozen classes from L1/L2 instead of kilobytes of geometry per cell.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace ubolt {
+
+constexpr int kMaxNb = 4;
+constexpr int kMaxFaces = 6;
+
+// Face code per (cell, slot): >= 0 the neighbour cell; -1 - side on the
+// boundary, side = 2 * axis + (0 low | 1 high).
+__host__ __device__ inline bool FaceInterior(int32_t code) { return code >= 0; }
+__host__ __device__ inline int FaceSide(int32_t code) { return -1 - code; }
+
+template <typename T>
+struct DevGeom {
+   int32_t dim, nb, F, A;
+   int64_t n_cells;
+   T sum_weights;
+   T inv_sum_weights;
+   // Per class
+   const T *nA;       // [class][F][3]
+   const T *fown;     // [class][F][nb][nb]
+   const T *fup;      // [class][F][nb][nb]
+   const T *bgrad;    // [class][nb][3]
+   const T *fbv;      // [class][F][nb]
+   const T *inv_vol;  // [class]
+   // Per cell
+   const int32_t *cls;     // [cell]
+   const int32_t *code;    // [cell][F]
+   const int8_t *mirror;   // [cell][F]: the neighbour's slot for the same face, -1 on the boundary
+   // Quadrature
+   const T *omega;         // [A][3]
+   const T *w;             // [A]
+   const int32_t *refl;    // [3][A]
+   int32_t side_bc[6];     // UBOLT_BC_* per side
+   // Group cross sections (per cell)
+   const T *sigma_t;
+   const T *sigma_s;
+};
+
+template <typename T>
+__device__ __forceinline__ T Dot3(const T *__restrict__ om, const T *__restrict__ n)
+{
+   // Omega . nA in the reference's term order (FaceFlux, plex_commonk.hpp:314-317)
+   return om[0] * n[0] + om[1] * n[1] + om[2] * n[2];
+}
+
+// The (cell, angle) element block of streaming + removal:
+//   B(i, j) = sum_{f: s_f > 0} s_f face_own_f(i, j) - [j == 0, i > 0] Omega . grad phi_i + sigma_t delta_ij
+// DG0: B = (sum_{s > 0} s) / V + sigma_t (DG0OutflowDiagonal then removal,
+// termsk.kokkos.cxx:183-196, 451-470). DG1: StreamingTermDG1::assemble_add,
+// termsk.kokkos.cxx:314-389.
+template <typename T, int NB, int F>
+__device__ __forceinline__ void BuildBlock(const DevGeom<T> &g, int32_t cl, const T om[3], T sigma_t, T B[NB][NB])
+{
+   if constexpr (NB == 1) {
+      T outflow = T(0);
+#pragma unroll
+      for (int f = 0; f < F; f++) {
+         const T s = Dot3(om, g.nA + ((int64_t)cl * F + f) * 3);
+         if (s > T(0)) outflow += s;
+      }
+      B[0][0] = outflow * g.inv_vol[cl] + sigma_t;
+   } else {
+#pragma unroll
+      for (int i = 0; i < NB; i++)
+#pragma unroll
+         for (int j = 0; j < NB; j++) B[i][j] = T(0);
+#pragma unroll
+      for (int f = 0; f < F; f++) {
+         const T s = Dot3(om, g.nA + ((int64_t)cl * F + f) * 3);
+         if (s > T(0)) {
+            const T *M = g.fown + ((int64_t)cl * F + f) * NB * NB;
+#pragma unroll
+            for (int i = 0; i < NB; i++)
+#pragma unroll
+               for (int j = 0; j < NB; j++) B[i][j] += s * M[i * NB + j];
+         }
+      }
+#pragma unroll
+      for (int i = 1; i < NB; i++) B[i][0] -= Dot3(om, g.bgrad + ((int64_t)cl * NB + i) * 3);
+#pragma unroll
+      for (int i = 0; i < NB; i++) B[i][i] += sigma_t;
+   }
+}
+
+// Solve B y = r in place by Gaussian elimination with partial pivoting.
+// Returns false for a singular block (a zero pivot), leaving r unchanged.
+template <typename T, int NB>
+__device__ __forceinline__ bool SolveBlock(T B[NB][NB], T r[NB])
+{
+   if constexpr (NB == 1) {
+      if (B[0][0] == T(0)) return false;
+      r[0] = r[0] / B[0][0];
+      return true;
+   } else {
+#pragma unroll
+      for (int k = 0; k < NB; k++) {
+         int piv = k;
+         T best = fabs(B[k][k]);
+#pragma unroll
+         for (int i = k + 1; i < NB; i++) {
+            const T v = fabs(B[i][k]);
+            if (v > best) { best = v; piv = i; }
+         }
+         if (best == T(0)) return false;
+         if (piv != k) {
+#pragma unroll
+            for (int i = k + 1; i < NB; i++)
+               if (i == piv) {
+#pragma unroll
+                  for (int j = 0; j < NB; j++) { const T t = B[k][j]; B[k][j] = B[i][j]; B[i][j] = t; }
+                  const T t = r[k]; r[k] = r[i]; r[i] = t;
+               }
+         }
+         const T inv = T(1) / B[k][k];
+#pragma unroll
+         for (int i = k + 1; i < NB; i++) {
+            const T f = B[i][k] * inv;
+#pragma unroll
+            for (int j = k + 1; j < NB; j++) B[i][j] -= f * B[k][j];
+            r[i] -= f * r[k];
+         }
+      }
+#pragma unroll
+      for (int k = NB - 1; k >= 0; k--) {
+         T s = r[k];
+#pragma unroll
+         for (int j = k + 1; j < NB; j++) s -= B[k][j] * r[j];
+         r[k] = s / B[k][k];
+      }
+      return true;
+   }
+}
+
+template <typename T, int NB>
+__device__ __forceinline__ void Transpose(T B[NB][NB])
+{
+#pragma unroll
+   for (int i = 0; i < NB; i++)
+#pragma unroll
+      for (int j = i + 1; j < NB; j++) { const T t = B[i][j]; B[i][j] = B[j][i]; B[j][i] = t; }
+}
+
+// Threads per block for the (cell, angle)-flattened kernels: whole cells per
+// block, about 256 threads.
+__host__ inline int CellsPerBlock(int A)
+{
+   int k = (256 + A / 2) / A;
+   return k < 1 ? 1 : k;
+}
+
+}  // namespace ubolt

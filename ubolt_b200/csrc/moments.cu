@@ -1,0 +1,148 @@
+// The angular moment and the right-hand-side fills.
+#include "ctx.h"
+
+namespace ubolt {
+
+// phi(node) = sum_a w_a psi(node, a): one warp per node, the node's angles
+// are one contiguous run (UboltAngularIntegral's gemm, sn_quadraturek.kokkos.cxx:400-427).
+template <typename T>
+__global__ void ScalarFluxKernel(const T *__restrict__ psi, const T *__restrict__ w, T *__restrict__ phi,
+                                 int64_t n_nodes, int A)
+{
+   const int64_t node = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+   const int lane = threadIdx.x & 31;
+   if (node >= n_nodes) return;
+   T s = T(0);
+   for (int a = lane; a < A; a += 32) s += w[a] * psi[node * A + a];
+#pragma unroll
+   for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+   if (lane == 0) phi[node] = s;
+}
+
+// b(cell, basis 0, a) += q(cell) / W (AddIsotropicKernel, material_speck.kokkos.cxx:164-187)
+__global__ void AddSourceKernel(const DevGeom<double> g, const double *__restrict__ q, double *__restrict__ b)
+{
+   const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+   if (tid >= g.n_cells * g.A) return;
+   const int64_t c = tid / g.A;
+   const int a = (int)(tid - c * g.A);
+   b[c * g.nb * g.A + a] += q[c] / g.sum_weights;
+}
+
+// b(node, a) += phi(node) (sigma_s(cell) / W) (GroupTransfer::add_transfer,
+// multigroupk.kokkos.cxx:329-362: scaled into scratch, then added)
+__global__ void AddTransferKernel(const DevGeom<double> g, const double *__restrict__ phi,
+                                  const double *__restrict__ sigma_s, double *__restrict__ b)
+{
+   const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+   if (r >= g.n_cells * g.nb * g.A) return;
+   const int64_t node = r / g.A;
+   b[r] += phi[node] * (sigma_s[node / g.nb] / g.sum_weights);
+}
+
+// Ghost-flux vacuum inflow, -(s / V) phi_i(x_f) inflow / W per entering face
+// (unstructured_dgk.kokkos.cxx:486-494 and 515-522), added per row
+// (FillGhostInflowKernel, discretisationk.kokkos.cxx:173-185)
+struct Inflow {
+   double v[6];
+};
+__global__ void GhostInflowKernel(const DevGeom<double> g, const double *__restrict__ volume, Inflow in,
+                                  double *__restrict__ b)
+{
+   const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+   if (tid >= g.n_cells * g.A) return;
+   const int64_t c = tid / g.A;
+   const int a = (int)(tid - c * g.A);
+   const int32_t cl = g.cls[c];
+   const double om[3] = {g.omega[3 * a], g.omega[3 * a + 1], g.omega[3 * a + 2]};
+   double add[kMaxNb] = {0, 0, 0, 0};
+   bool any = false;
+   for (int f = 0; f < g.F; f++) {
+      const int32_t code = g.code[c * g.F + f];
+      if (FaceInterior(code)) continue;
+      const int side = FaceSide(code);
+      if (g.side_bc[side] != UBOLT_BC_VACUUM || in.v[side] == 0.0) continue;
+      const double s = Dot3(om, g.nA + ((int64_t)cl * g.F + f) * 3);
+      if (!(s < 0.0)) continue;
+      const double inflow = in.v[side] / g.sum_weights;
+      for (int i = 0; i < g.nb; i++) {
+         const double phi_i = (g.nb == 1) ? 1.0 : g.fbv[((int64_t)cl * g.F + f) * g.nb + i];
+         add[i] += -s / volume[c] * phi_i * inflow;
+      }
+      any = true;
+   }
+   if (!any) return;
+   for (int i = 0; i < g.nb; i++) b[(c * g.nb + i) * g.A + a] += add[i];
+}
+
+template <typename T>
+static int ScalarFlux(ubolt_ctx *ctx, const T *psi, T *phi, void *stream)
+{
+   int rc = CheckReady(ctx, false);
+   if (rc) return rc;
+   if (!psi || !phi) return SetError(UBOLT_ERR_ARG, "scalar_flux: NULL array");
+   const int64_t threads = ctx->n_nodes * 32;
+   ScalarFluxKernel<T><<<(threads + 255) / 256, 256, 0, (cudaStream_t)stream>>>(psi, ctx->geom<T>().w, phi,
+                                                                                ctx->n_nodes, ctx->A);
+   return CheckLaunch("scalar_flux");
+}
+
+template <typename T>
+void LaunchScalarFlux(const ubolt_ctx *ctx, const T *psi, T *phi, cudaStream_t s)
+{
+   const int64_t threads = ctx->n_nodes * 32;
+   ScalarFluxKernel<T><<<(threads + 255) / 256, 256, 0, s>>>(psi, ctx->geom<T>().w, phi, ctx->n_nodes, ctx->A);
+}
+template void LaunchScalarFlux<double>(const ubolt_ctx *, const double *, double *, cudaStream_t);
+template void LaunchScalarFlux<float>(const ubolt_ctx *, const float *, float *, cudaStream_t);
+
+}  // namespace ubolt
+
+using namespace ubolt;
+
+extern "C" int ubolt_scalar_flux(ubolt_ctx *ctx, const double *psi, double *phi, void *stream)
+{
+   return ScalarFlux<double>(ctx, psi, phi, stream);
+}
+extern "C" int ubolt_scalar_flux_f32(ubolt_ctx *ctx, const float *psi, float *phi, void *stream)
+{
+   return ScalarFlux<float>(ctx, psi, phi, stream);
+}
+
+extern "C" int ubolt_add_source(ubolt_ctx *ctx, const double *q_cell, double *b, void *stream)
+{
+   int rc = CheckReady(ctx, false);
+   if (rc) return rc;
+   if (!q_cell || !b) return SetError(UBOLT_ERR_ARG, "add_source: NULL array");
+   const int64_t n = ctx->n_cells * ctx->A;
+   AddSourceKernel<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(ctx->g64, q_cell, b);
+   return CheckLaunch("add_source");
+}
+
+extern "C" int ubolt_add_transfer(ubolt_ctx *ctx, const double *phi_from, const double *sigma_s_from_to, double *b,
+                                  void *stream)
+{
+   int rc = CheckReady(ctx, false);
+   if (rc) return rc;
+   if (!phi_from || !sigma_s_from_to || !b) return SetError(UBOLT_ERR_ARG, "add_transfer: NULL array");
+   const int64_t n = ctx->n_rows;
+   AddTransferKernel<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(ctx->g64, phi_from, sigma_s_from_to, b);
+   return CheckLaunch("add_transfer");
+}
+
+extern "C" int ubolt_add_ghost_inflow(ubolt_ctx *ctx, const double *side_inflow, double *b, void *stream)
+{
+   int rc = CheckReady(ctx, false);
+   if (rc) return rc;
+   if (!side_inflow || !b) return SetError(UBOLT_ERR_ARG, "add_ghost_inflow: NULL array");
+   Inflow in{};
+   bool any = false;
+   for (int s = 0; s < 2 * ctx->dim; s++) {
+      in.v[s] = side_inflow[s];
+      if (in.v[s] != 0.0 && ctx->side_bc[s] == UBOLT_BC_VACUUM) any = true;
+   }
+   if (!any) return UBOLT_OK;
+   const int64_t n = ctx->n_cells * ctx->A;
+   GhostInflowKernel<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(ctx->g64, ctx->d_volume, in, b);
+   return CheckLaunch("add_ghost_inflow");
+}

@@ -1,0 +1,176 @@
+"""Host-side mirror of UBOLT's operator and preconditioner interface over the C ABI.
+
+Names and argument meaning follow the reference classes the library stands
+in for (stevendargaville/UBOLT):
+
+    TransportOperator  - MatShell MULT / unscattered MULT / diagonal
+                         (include/ubolt/transport_operator.hpp, src/transport_operatork.kokkos.cxx)
+    ElementBlockInverse - removal stage blocks (include/ubolt/block_inverse.hpp)
+    GroupTransfer      - external source, scalar-flux cache, group transfer
+                         (include/ubolt/multigroup.hpp:103-182)
+    angular_integral   - UboltAngularIntegral (include/ubolt/sn_quadrature.hpp:163-171)
+    fill_inflow        - UboltFillInflow, ghost-flux path (include/ubolt/coo_pattern.hpp:68)
+
+Vectors are torch CUDA tensors (float64, or float32 for the *_f32 paths)
+in UBOLT's row layout; torch only supplies device memory and the stream.
+Errors raise ubolt_b200._lib.UboltError carrying the library's status.
+"""
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import lib, check
+
+
+def _p(t):
+    return C.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def _stream(stream=None):
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+class Context:
+    """ubolt_ctx: geometry and ordinates on one device (the current one)."""
+
+    def __init__(self, geometry, quad):
+        self.geometry, self.quad = geometry, quad
+        h = _lib.vp()
+        gs, qs = geometry.struct(), quad.struct()
+        check(lib.ubolt_ctx_create(C.byref(gs), C.byref(qs), C.byref(h)))
+        self.handle = h
+        self.device = torch.device("cuda", torch.cuda.current_device())
+        rows, nodes, cells = C.c_int64(), C.c_int64(), C.c_int64()
+        nb, na = C.c_int32(), C.c_int32()
+        check(lib.ubolt_ctx_sizes(h, C.byref(rows), C.byref(nodes), C.byref(cells), C.byref(nb), C.byref(na)))
+        self.n_rows, self.n_nodes, self.n_cells = rows.value, nodes.value, cells.value
+        self.n_basis, self.n_angles = nb.value, na.value
+        self._group = None
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib.ubolt_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def vector(self, dtype=torch.float64, fill=None):
+        v = torch.empty(self.n_rows, dtype=dtype, device=self.device)
+        if fill is not None:
+            v.fill_(fill)
+        return v
+
+    def set_group(self, sigma_t, sigma_s_within, stream=None):
+        """Point the terms at a group's cross sections (device float64, per cell).
+        The tensors are referenced, not copied - keep them alive."""
+        self._group = (sigma_t, sigma_s_within)
+        check(lib.ubolt_set_group(self.handle, _p(sigma_t), _p(sigma_s_within), _stream(stream)))
+
+
+class TransportOperator:
+    """The shell operator A = L - S and its unscattered twin L."""
+
+    def __init__(self, ctx):
+        self.ctx = ctx
+
+    def _call(self, fn64, fn32, x, y, stream):
+        if y is None:
+            y = torch.empty_like(x)
+        fn = fn64 if x.dtype == torch.float64 else fn32
+        check(fn(self.ctx.handle, _p(x), _p(y), _stream(stream)))
+        return y
+
+    def mult(self, x, y=None, stream=None):
+        """y = (L - S) x (ShellMatMultApply)."""
+        return self._call(lib.ubolt_apply, lib.ubolt_apply_f32, x, y, stream)
+
+    def mult_unscattered(self, x, y=None, stream=None):
+        """y = L x (UnscatteredMatMultApply)."""
+        return self._call(lib.ubolt_apply_unscattered, lib.ubolt_apply_unscattered_f32, x, y, stream)
+
+    def mult_transpose(self, x, y=None, stream=None):
+        """y = (L - S)^T x."""
+        return self._call(lib.ubolt_apply_adjoint, lib.ubolt_apply_adjoint_f32, x, y, stream)
+
+    def diagonal(self, d=None, stream=None):
+        d = self.ctx.vector() if d is None else d
+        check(lib.ubolt_diagonal(self.ctx.handle, _p(d), _stream(stream)))
+        return d
+
+
+class ElementBlockInverse:
+    """D^{-1} for the (cell, angle) element blocks of streaming + removal."""
+
+    def __init__(self, ctx):
+        self.ctx = ctx
+
+    def setup(self, stream=None):
+        """Check every block is invertible; raises UBOLT_ERR_SINGULAR otherwise."""
+        n = C.c_int64()
+        check(lib.ubolt_block_setup(self.ctx.handle, C.byref(n), _stream(stream)))
+        return n.value
+
+    def apply(self, x, y=None, stream=None):
+        y = torch.empty_like(x) if y is None else y
+        fn = lib.ubolt_block_apply if x.dtype == torch.float64 else lib.ubolt_block_apply_f32
+        check(fn(self.ctx.handle, _p(x), _p(y), _stream(stream)))
+        return y
+
+    def apply_transpose(self, x, y=None, stream=None):
+        y = torch.empty_like(x) if y is None else y
+        check(lib.ubolt_block_apply_transpose(self.ctx.handle, _p(x), _p(y), _stream(stream)))
+        return y
+
+    def inverse(self, stream=None):
+        c = self.ctx
+        inv = torch.empty(c.n_cells * c.n_angles * c.n_basis * c.n_basis, dtype=torch.float64, device=c.device)
+        check(lib.ubolt_block_inverse(c.handle, _p(inv), _stream(stream)))
+        return inv
+
+
+def angular_integral(ctx, psi, phi=None, stream=None):
+    phi = torch.empty(ctx.n_nodes, dtype=psi.dtype, device=psi.device) if phi is None else phi
+    fn = lib.ubolt_scalar_flux if psi.dtype == torch.float64 else lib.ubolt_scalar_flux_f32
+    check(fn(ctx.handle, _p(psi), _p(phi), _stream(stream)))
+    return phi
+
+
+def fill_inflow(ctx, side_inflow, b, stream=None):
+    """b += the ghost-flux vacuum inflow (side_inflow: angle-integrated, per side)."""
+    s = np.zeros(6)
+    s[:len(side_inflow)] = side_inflow
+    check(lib.ubolt_add_ghost_inflow(ctx.handle, s.ctypes.data_as(_lib.dp), _p(b), _stream(stream)))
+    return b
+
+
+class GroupTransfer:
+    """External source and group-to-group transfer of the per-node backends."""
+
+    def __init__(self, ctx, sigma_s_table, source_table):
+        """sigma_s_table[g_from][g_to], source_table[g]: device float64 per-cell tensors."""
+        self.ctx = ctx
+        self.sigma_s = sigma_s_table
+        self.source = source_table
+        self.phi = [None] * len(source_table)
+
+    def add_external(self, g, b, stream=None):
+        check(lib.ubolt_add_source(self.ctx.handle, _p(self.source[g]), _p(b), _stream(stream)))
+        return b
+
+    def set_scalar_flux(self, g, psi, stream=None):
+        self.phi[g] = angular_integral(self.ctx, psi, self.phi[g], stream)
+        return self.phi[g]
+
+    def add_transfer(self, g_from, g_to, b, stream=None):
+        if self.phi[g_from] is None:
+            raise _lib.UboltError(4, f"no scalar flux cached for group {g_from}")
+        check(lib.ubolt_add_transfer(self.ctx.handle, _p(self.phi[g_from]), _p(self.sigma_s[g_from][g_to]), _p(b),
+                                     _stream(stream)))
+        return b
