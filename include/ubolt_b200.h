@@ -212,6 +212,102 @@ int ubolt_add_transfer(ubolt_ctx *ctx, const double *phi_from, const double *sig
  * values of src/unstructured_dgk.kokkos.cxx:476-494 built on the fly. */
 int ubolt_add_ghost_inflow(ubolt_ctx *ctx, const double *side_inflow, double *b, void *stream);
 
+/* ~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~
+ * The streaming stage: psi = L^{-1} q by an upwind sweep of every ordinate
+ * ~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~ */
+typedef struct {
+   int32_t patch_size;    /* cells per patch */
+   int32_t n_patches;
+   int64_t n_tasks;       /* patch pieces x ordinates */
+   int64_t n_lagged;      /* interior couplings lagged to break cycles */
+   int64_t n_split;       /* extra tasks where a patch is solved in pieces */
+   int32_t max_levels;    /* most levels in one patch-ordinate task */
+   int32_t grid;          /* blocks of the last launch */
+   int64_t total_levels;
+   uint32_t timeouts;     /* bounded waits that gave up since the last status */
+   uint32_t pad_;
+} ubolt_sweep_info;
+
+/* Build the sweep plan: patches of patch_size consecutive cells (0 picks 128
+ * in 2D, 64 in 3D; at most 256), per-ordinate upwind orders, task list. Host
+ * work plus one upload; independent of the group. Called by the first sweep
+ * if not before. The streaming stage of the preconditioner, in place of
+ * PCAIR (src/transport_solverk.kokkos.cxx:238-260, composite index 1). */
+int ubolt_sweep_setup(ubolt_ctx *ctx, int patch_size);
+/* psi = L^{-1} q for every ordinate: exact where the per-ordinate upwind
+ * graph is acyclic; reflective inflow and cycle-breaking couplings are lagged
+ * to zero. Every wait is bounded; check ubolt_sweep_status. */
+int ubolt_sweep(ubolt_ctx *ctx, const double *q, double *psi, void *stream);
+int ubolt_sweep_f32(ubolt_ctx *ctx, const float *q, float *psi, void *stream);
+/* Plan statistics and the sticky timeout flag (synchronises `stream`):
+ * returns UBOLT_ERR_TIMEOUT, and clears the flag, if a wait gave up. */
+int ubolt_sweep_status(ubolt_ctx *ctx, ubolt_sweep_info *info, void *stream);
+
+/* The plan on the host alone, for inspection. Tasks are numbered in launch
+ * order; task t solves cells of patch p for ordinate a, task_pa[t] = p * A + a,
+ * after its upstream tasks (all numbered below t). Arrays are owned by the
+ * returned handle. */
+typedef struct ubolt_sweep_plan_host ubolt_sweep_plan_host;
+typedef struct {
+   int32_t patch_size, n_patches;
+   int64_t n_tasks;
+   int64_t n_lagged;         /* couplings lagged to break upwind cycles */
+   int64_t n_split;          /* extra tasks where a patch is solved in pieces */
+   const int32_t *task_pa;   /* [n_tasks] */
+   const int32_t *dep_ptr;   /* [n_tasks + 1] */
+   const int32_t *deps;
+   const int64_t *cell_ptr;  /* [n_tasks + 1] */
+   const uint8_t *tcell;     /* local cell index, patch p covering cells [p P, p P + P) */
+   const uint16_t *tmask;    /* bit f: face f's upwind cell is in the same task; bit 8 + f: in an earlier task */
+   const int32_t *lvl_ptr;   /* [n_tasks + 1] */
+   const uint16_t *lvl;      /* level end positions within a task's cells */
+} ubolt_sweep_plan_view;
+int ubolt_sweep_plan_build(const ubolt_dg_geometry *geom, const ubolt_quadrature *quad, int patch_size,
+                           ubolt_sweep_plan_host **out, ubolt_sweep_plan_view *view);
+void ubolt_sweep_plan_free(ubolt_sweep_plan_host *plan);
+
+/* ~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~
+ * The solve
+ * ~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~ */
+enum { UBOLT_PC_NONE = 0, UBOLT_PC_BLOCK = 1, UBOLT_PC_SWEEP = 2, UBOLT_PC_SWEEP_DSA = 3 };
+enum { UBOLT_PRECISION_FP64 = 0, UBOLT_PRECISION_MIXED = 1 };
+
+typedef struct {
+   double rtol;        /* stop at ||b - A x|| <= rtol ||b|| (true residual, FP64) */
+   double inner_rtol;  /* mixed: each FP32 correction solve's relative tolerance */
+   int32_t max_it;     /* GMRES iterations in total */
+   int32_t restart;    /* GMRES(m) */
+   int32_t precision;  /* UBOLT_PRECISION_* */
+   int32_t pc;         /* UBOLT_PC_* */
+   int32_t max_outer;  /* mixed: refinement steps */
+   int32_t x_zero;     /* 1: start from zero, 0: from the x passed in */
+} ubolt_solve_options;
+
+typedef struct {
+   int32_t iterations; /* GMRES iterations (all refinement steps) */
+   int32_t outer;      /* refinement steps (1 for FP64) */
+   int32_t converged;
+   int32_t pad_;
+   double residual;    /* ||b - A x|| / ||b|| of the returned x, FP64 */
+   double rnorm0;      /* ||b|| */
+   double seconds;     /* host wall time of the call */
+} ubolt_solve_stats;
+
+/* rtol 1e-8, inner_rtol 1e-5, max_it 500, restart 30, FP64, sweep preconditioner. */
+void ubolt_solve_defaults(ubolt_solve_options *opts);
+/* Allocate the solver's workspace ((restart + 1) Krylov vectors, FP64, or
+ * FP32 in the mixed form) and the sweep plan its preconditioner needs.
+ * ubolt_solve calls it when the workspace is missing or of another shape. */
+int ubolt_solver_setup(ubolt_ctx *ctx, const ubolt_solve_options *opts);
+/* Solve (L - S) x = b for the current group. Right-preconditioned GMRES
+ * (KSPGMRES + PC_RIGHT, src/transport_solverk.kokkos.cxx:196-318; the solve
+ * TransportSolver::solve runs, :334-343), stopping on the true residual.
+ * Mixed form: FP32 operator, sweep and Krylov storage (FP64 accumulation)
+ * inside FP64 iterative refinement r = b - A x. Synchronises `stream`.
+ * Returns UBOLT_ERR_NOT_CONVERGED, with x and stats filled, at max_it. */
+int ubolt_solve(ubolt_ctx *ctx, const double *b, double *x, const ubolt_solve_options *opts,
+                ubolt_solve_stats *stats, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -89,3 +89,65 @@ def declared_symbols(header=None):
     text = open(header).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
     return sorted(set(re.findall(r"\b(ubolt_[a-z0-9_]+)\s*\(", text)))
+
+
+class SweepInfo(C.Structure):
+    _fields_ = [("patch_size", C.c_int32), ("n_patches", C.c_int32), ("n_tasks", C.c_int64),
+                ("n_lagged", C.c_int64), ("n_split", C.c_int64), ("max_levels", C.c_int32), ("grid", C.c_int32),
+                ("total_levels", C.c_int64), ("timeouts", C.c_uint32), ("pad_", C.c_uint32)]
+
+
+class SolveOptions(C.Structure):
+    _fields_ = [("rtol", C.c_double), ("inner_rtol", C.c_double), ("max_it", C.c_int32), ("restart", C.c_int32),
+                ("precision", C.c_int32), ("pc", C.c_int32), ("max_outer", C.c_int32), ("x_zero", C.c_int32)]
+
+
+class SolveStats(C.Structure):
+    _fields_ = [("iterations", C.c_int32), ("outer", C.c_int32), ("converged", C.c_int32), ("pad_", C.c_int32),
+                ("residual", C.c_double), ("rnorm0", C.c_double), ("seconds", C.c_double)]
+
+
+PC_NONE, PC_BLOCK, PC_SWEEP, PC_SWEEP_DSA = 0, 1, 2, 3
+PRECISION_FP64, PRECISION_MIXED = 0, 1
+
+_sig("ubolt_sweep_setup", C.c_int, vp, C.c_int)
+_sig("ubolt_sweep", C.c_int, vp, vp, vp, vp)
+_sig("ubolt_sweep_f32", C.c_int, vp, vp, vp, vp)
+_sig("ubolt_sweep_status", C.c_int, vp, C.POINTER(SweepInfo), vp)
+_sig("ubolt_solve_defaults", None, C.POINTER(SolveOptions))
+_sig("ubolt_solver_setup", C.c_int, vp, C.POINTER(SolveOptions))
+_sig("ubolt_solve", C.c_int, vp, vp, vp, C.POINTER(SolveOptions), C.POINTER(SolveStats), vp)
+
+
+class SweepPlanView(C.Structure):
+    _fields_ = [("patch_size", C.c_int32), ("n_patches", C.c_int32), ("n_tasks", C.c_int64),
+                ("n_lagged", C.c_int64), ("n_split", C.c_int64), ("task_pa", i32p), ("dep_ptr", i32p),
+                ("deps", i32p), ("cell_ptr", i64p), ("tcell", C.POINTER(C.c_uint8)),
+                ("tmask", C.POINTER(C.c_uint16)), ("lvl_ptr", i32p), ("lvl", C.POINTER(C.c_uint16))]
+
+
+_sig("ubolt_sweep_plan_build", C.c_int, C.POINTER(DGGeometry), C.POINTER(Quadrature), C.c_int, C.POINTER(vp),
+     C.POINTER(SweepPlanView))
+_sig("ubolt_sweep_plan_free", None, vp)
+
+
+def sweep_plan(geometry, quad, patch_size=0):
+    """The sweep plan built on the host, as NumPy arrays (for inspection and tests)."""
+    import numpy as np
+    h = vp()
+    view = SweepPlanView()
+    gs, qs = geometry.struct(), quad.struct()
+    check(lib.ubolt_sweep_plan_build(C.byref(gs), C.byref(qs), patch_size, C.byref(h), C.byref(view)))
+    try:
+        nt = view.n_tasks
+        arr = lambda p, n: np.ctypeslib.as_array(p, shape=(n,)).copy() if n > 0 else np.zeros(0)
+        out = {"patch_size": view.patch_size, "n_patches": view.n_patches, "n_tasks": nt, "n_lagged": view.n_lagged,
+               "n_split": view.n_split, "task_pa": arr(view.task_pa, nt), "dep_ptr": arr(view.dep_ptr, nt + 1),
+               "cell_ptr": arr(view.cell_ptr, nt + 1), "lvl_ptr": arr(view.lvl_ptr, nt + 1)}
+        out["deps"] = arr(view.deps, int(out["dep_ptr"][-1]))
+        out["tcell"] = arr(view.tcell, int(out["cell_ptr"][-1]))
+        out["tmask"] = arr(view.tmask, int(out["cell_ptr"][-1]))
+        out["lvl"] = arr(view.lvl, int(out["lvl_ptr"][-1]))
+        return out
+    finally:
+        lib.ubolt_sweep_plan_free(h)

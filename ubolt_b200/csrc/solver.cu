@@ -1,0 +1,470 @@
+// The solve: right-preconditioned restarted GMRES on the shell operator,
+// in a plain FP64 form and a mixed form (FP32 operator, preconditioner and
+// Krylov storage inside FP64 iterative refinement).
+//
+// Restates the reference's KSP set-up (src/transport_solverk.kokkos.cxx:
+// 196-318): GMRES with PC_RIGHT, so the stopping test is the true residual
+// ||b - A x|| against rtol ||b||, the preconditioner being the streaming
+// stage (here the exact sweep, ubolt_sweep), optionally followed by the DSA
+// correction formed on the operator's own residual, or the removal block
+// stage alone (ubolt_block_apply). Orthogonalisation is classical
+// Gram-Schmidt with one reorthogonalisation (PETSc's GMRES default refines),
+// as fused multi-vector dot and update kernels that read each basis vector
+// once and accumulate in FP64 whatever the storage precision. The Hessenberg
+// least-squares problem and its Givens rotations stay on the host.
+#include "ctx.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <vector>
+
+namespace ubolt {
+template <typename T>
+int Sweep(ubolt_ctx *ctx, const T *q, T *psi, void *stream);
+template <typename T>
+int BlockApply(ubolt_ctx *ctx, const T *x, T *y, bool trans, void *stream);
+template <typename T>
+int DsaCorrect(ubolt_ctx *ctx, const T *r, T *y, T *tmp, void *stream);
+}  // namespace ubolt
+
+struct ubolt_solver {
+   int restart = 0;
+   int64_t n = 0;
+   bool mixed = false;
+   // FP64 workspace: residual, preconditioned vector, spare
+   double *r = nullptr, *z = nullptr, *t = nullptr;
+   double *V = nullptr;  // (restart + 1) x n, plain form
+   // FP32 workspace, mixed form: basis, preconditioned vector, rhs, spare, correction
+   float *V32 = nullptr, *z32 = nullptr, *b32 = nullptr, *t32 = nullptr, *d32 = nullptr;
+   // Reductions: partial[red_blocks][restart + 2], h[3 * (restart + 2)]
+   double *partial = nullptr, *h = nullptr;
+   int red_blocks = 0;
+};
+
+namespace ubolt {
+
+constexpr int kRedThreads = 256;
+constexpr int kChunk = 8;
+
+// partial[blk][i0 + i] = this block's share of V_{i0+i} . w
+template <typename S>
+__global__ void __launch_bounds__(kRedThreads) MultiDotKernel(const S *__restrict__ V, int64_t n, int i0, int nc,
+                                                              const S *__restrict__ w, double *__restrict__ partial,
+                                                              int stride)
+{
+   double acc[kChunk];
+#pragma unroll
+   for (int i = 0; i < kChunk; i++) acc[i] = 0.0;
+   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+      const double wk = (double)w[k];
+#pragma unroll
+      for (int i = 0; i < kChunk; i++)
+         if (i < nc) acc[i] += (double)V[(int64_t)(i0 + i) * n + k] * wk;
+   }
+   __shared__ double red[kChunk][kRedThreads / 32];
+   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+   for (int i = 0; i < kChunk; i++) {
+      double v = acc[i];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (lane == 0) red[i][warp] = v;
+   }
+   __syncthreads();
+   if (threadIdx.x < nc) {
+      double s = 0.0;
+      for (int k = 0; k < kRedThreads / 32; k++) s += red[threadIdx.x][k];
+      partial[(int64_t)blockIdx.x * stride + i0 + threadIdx.x] = s;
+   }
+}
+
+// out[i] = sum over blocks of partial[blk][i]
+__global__ void ReducePartialKernel(const double *__restrict__ partial, int n_blocks, int stride,
+                                    double *__restrict__ out)
+{
+   const int i = blockIdx.x;
+   double s = 0.0;
+   for (int b = threadIdx.x; b < n_blocks; b += blockDim.x) s += partial[(int64_t)b * stride + i];
+   __shared__ double red[32];
+#pragma unroll
+   for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+   __syncthreads();
+   if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int k = 0; k < (int)(blockDim.x + 31) / 32; k++) t += red[k];
+      out[i] = t;
+   }
+}
+
+// w = sign * w + sum_i c[i] V_i, c on the device (sign 1: update, 0: assign)
+template <typename S>
+__global__ void MultiAxpyKernel(const S *__restrict__ V, int64_t n, int nv, const double *__restrict__ c,
+                                double scale_c, S *__restrict__ w, int keep_w)
+{
+   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+      double s = keep_w ? (double)w[k] : 0.0;
+      for (int i = 0; i < nv; i++) s += scale_c * c[i] * (double)V[(int64_t)i * n + k];
+      w[k] = (S)s;
+   }
+}
+
+// y = alpha * x (in place allowed), any precision pair
+template <typename A, typename B>
+__global__ void ScaleKernel(const A *__restrict__ x, B *__restrict__ y, double alpha, int64_t n)
+{
+   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+      y[k] = (B)(alpha * (double)x[k]);
+}
+
+// y += alpha * x
+template <typename A, typename B>
+__global__ void AxpyKernel(const A *__restrict__ x, B *__restrict__ y, double alpha, int64_t n)
+{
+   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+      y[k] = (B)((double)y[k] + alpha * (double)x[k]);
+}
+
+// r = b - r
+template <typename S>
+__global__ void ResidualKernel(const S *__restrict__ b, S *__restrict__ r, int64_t n)
+{
+   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+      r[k] = b[k] - r[k];
+}
+
+static int GridFor(int64_t n)
+{
+   int dev = 0, sms = 148;
+   cudaGetDevice(&dev);
+   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+   const int64_t want = (n + 255) / 256;
+   return (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)sms * 8));
+}
+
+// h[0..nv) = V^T w, computed on the device
+template <typename S>
+static void MultiDot(const ubolt_solver *ws, const S *V, int nv, const S *w, int64_t n, double *h, cudaStream_t s)
+{
+   const int stride = ws->restart + 2;
+   for (int i0 = 0; i0 < nv; i0 += kChunk)
+      MultiDotKernel<S><<<ws->red_blocks, kRedThreads, 0, s>>>(V, n, i0, std::min(kChunk, nv - i0), w, ws->partial,
+                                                                stride);
+   ReducePartialKernel<<<nv, 256, 0, s>>>(ws->partial, ws->red_blocks, stride, h);
+}
+
+template <typename S>
+static double Norm(const ubolt_solver *ws, const S *x, int64_t n, cudaStream_t s, int *rc)
+{
+   double *slot = ws->h + 3 * (ws->restart + 2) - 1;
+   MultiDot<S>(ws, x, 1, x, n, slot, s);
+   double v = 0.0;
+   cudaMemcpyAsync(&v, slot, sizeof v, cudaMemcpyDeviceToHost, s);
+   *rc = CudaCheck(cudaStreamSynchronize(s), "norm");
+   return std::sqrt(v);
+}
+
+template <typename T>
+int OperatorApply(ubolt_ctx *ctx, const T *x, T *y, void *stream);
+template <>
+int OperatorApply<double>(ubolt_ctx *ctx, const double *x, double *y, void *stream)
+{
+   return ubolt_apply(ctx, x, y, stream);
+}
+template <>
+int OperatorApply<float>(ubolt_ctx *ctx, const float *x, float *y, void *stream)
+{
+   return ubolt_apply_f32(ctx, x, y, stream);
+}
+
+// y = M^{-1} x. tmp is scratch of n values (the DSA stage's residual).
+template <typename T>
+static int Precondition(ubolt_ctx *ctx, int pc, const T *x, T *y, T *tmp, int64_t n, void *stream)
+{
+   switch (pc) {
+   case UBOLT_PC_NONE:
+      return CudaCheck(cudaMemcpyAsync(y, x, n * sizeof(T), cudaMemcpyDeviceToDevice, (cudaStream_t)stream),
+                       "pc copy");
+   case UBOLT_PC_BLOCK: return BlockApply<T>(ctx, x, y, false, stream);
+   case UBOLT_PC_SWEEP: return Sweep<T>(ctx, x, y, stream);
+   case UBOLT_PC_SWEEP_DSA: {
+      int rc = Sweep<T>(ctx, x, y, stream);
+      if (rc) return rc;
+      return DsaCorrect<T>(ctx, x, y, tmp, stream);
+   }
+   default: return SetError(UBOLT_ERR_ARG, "unknown preconditioner %d", pc);
+   }
+}
+
+struct GmresResult {
+   int iterations = 0;
+   double estimate = 1.0;  // last residual estimate / ||b||
+   bool converged = false;
+};
+
+// Right-preconditioned GMRES(m) for A x = b in storage precision S from the
+// guess in x (x_zero: it is zero). V: (m + 1) n basis, z, t: n each.
+template <typename S>
+static int Gmres(ubolt_ctx *ctx, const ubolt_solver *ws, S *V, S *z, S *t, const S *b, S *x, double bnorm,
+                 double rtol, int max_it, int pc, bool x_zero, GmresResult *out, void *stream)
+{
+   cudaStream_t s = (cudaStream_t)stream;
+   const int64_t n = ws->n;
+   const int m = ws->restart;
+   const int grid = GridFor(n);
+   std::vector<double> H((size_t)(m + 1) * m, 0.0), cs(m), sn(m), g(m + 1), y(m), h1(m + 1), h2(m + 2);
+   double *dh1 = ws->h, *dh2 = ws->h + (m + 2), *dy = ws->h + 2 * (m + 2);
+   int rc = 0;
+   out->iterations = 0;
+   out->converged = false;
+   while (out->iterations < max_it) {
+      if (x_zero) {
+         rc = CudaCheck(cudaMemcpyAsync(V, b, n * sizeof(S), cudaMemcpyDeviceToDevice, s), "gmres");
+         x_zero = false;
+      } else {
+         rc = OperatorApply<S>(ctx, x, V, stream);
+         ResidualKernel<S><<<grid, 256, 0, s>>>(b, V, n);
+      }
+      if (rc) return rc;
+      const double beta = Norm<S>(ws, V, n, s, &rc);
+      if (rc) return rc;
+      if (!std::isfinite(beta)) return SetError(UBOLT_ERR_NONFINITE, "GMRES residual is not finite");
+      out->estimate = bnorm > 0 ? beta / bnorm : 0.0;
+      if (beta <= rtol * bnorm || beta == 0.0) {
+         out->converged = true;
+         break;
+      }
+      ScaleKernel<S, S><<<grid, 256, 0, s>>>(V, V, 1.0 / beta, n);
+      std::fill(g.begin(), g.end(), 0.0);
+      g[0] = beta;
+      int j = 0;
+      for (; j < m && out->iterations < max_it; j++) {
+         S *vj = V + (int64_t)j * n, *vn = V + (int64_t)(j + 1) * n;
+         if ((rc = Precondition<S>(ctx, pc, vj, z, t, n, stream))) return rc;
+         if ((rc = OperatorApply<S>(ctx, z, vn, stream))) return rc;
+         MultiDot<S>(ws, V, j + 1, vn, n, dh1, s);
+         MultiAxpyKernel<S><<<grid, 256, 0, s>>>(V, n, j + 1, dh1, -1.0, vn, 1);
+         MultiDot<S>(ws, V, j + 1, vn, n, dh2, s);
+         MultiAxpyKernel<S><<<grid, 256, 0, s>>>(V, n, j + 1, dh2, -1.0, vn, 1);
+         MultiDot<S>(ws, vn, 1, vn, n, dh2 + j + 1, s);
+         cudaMemcpyAsync(h1.data(), dh1, (j + 1) * sizeof(double), cudaMemcpyDeviceToHost, s);
+         cudaMemcpyAsync(h2.data(), dh2, (j + 2) * sizeof(double), cudaMemcpyDeviceToHost, s);
+         if ((rc = CudaCheck(cudaStreamSynchronize(s), "gmres"))) return rc;
+         out->iterations++;
+         const double hn = std::sqrt(h2[j + 1]);
+         if (!std::isfinite(hn)) return SetError(UBOLT_ERR_NONFINITE, "GMRES Arnoldi vector is not finite");
+         for (int i = 0; i <= j; i++) H[i * m + j] = h1[i] + h2[i];
+         if (hn > 0.0) ScaleKernel<S, S><<<grid, 256, 0, s>>>(vn, vn, 1.0 / hn, n);
+         for (int i = 0; i < j; i++) {
+            const double tt = cs[i] * H[i * m + j] + sn[i] * H[(i + 1) * m + j];
+            H[(i + 1) * m + j] = -sn[i] * H[i * m + j] + cs[i] * H[(i + 1) * m + j];
+            H[i * m + j] = tt;
+         }
+         const double d = std::hypot(H[j * m + j], hn);
+         if (d == 0.0) return SetError(UBOLT_ERR_BREAKDOWN, "GMRES breakdown at iteration %d", out->iterations);
+         cs[j] = H[j * m + j] / d;
+         sn[j] = hn / d;
+         H[j * m + j] = d;
+         g[j + 1] = -sn[j] * g[j];
+         g[j] = cs[j] * g[j];
+         out->estimate = bnorm > 0 ? std::fabs(g[j + 1]) / bnorm : 0.0;
+         if (std::fabs(g[j + 1]) <= rtol * bnorm || hn == 0.0) {
+            j++;
+            out->converged = true;
+            break;
+         }
+      }
+      // x += M^{-1} (V y)
+      for (int i = j - 1; i >= 0; i--) {
+         double tt = g[i];
+         for (int k = i + 1; k < j; k++) tt -= H[i * m + k] * y[k];
+         y[i] = tt / H[i * m + i];
+      }
+      cudaMemcpyAsync(dy, y.data(), j * sizeof(double), cudaMemcpyHostToDevice, s);
+      // V_j is free scratch here: the next cycle rebuilds the basis
+      S *u = V + (int64_t)m * n;
+      MultiAxpyKernel<S><<<grid, 256, 0, s>>>(V, n, j, dy, 1.0, u, 0);
+      if ((rc = Precondition<S>(ctx, pc, u, z, t, n, stream))) return rc;
+      AxpyKernel<S, S><<<grid, 256, 0, s>>>(z, x, 1.0, n);
+      if (out->converged) break;
+   }
+   return CheckLaunch("gmres");
+}
+
+static int EnsureWorkspace(ubolt_ctx *ctx, const ubolt_solve_options *o)
+{
+   const bool mixed = o->precision == UBOLT_PRECISION_MIXED;
+   const int m = o->restart > 0 ? o->restart : 30;
+   ubolt_solver *ws = ctx->solver;
+   if (ws && ws->restart == m && ws->mixed == mixed) return UBOLT_OK;
+   // Workspace is re-made only when its shape changes
+   if (ws) {
+      cudaDeviceSynchronize();
+      for (void *p : {(void *)ws->r, (void *)ws->z, (void *)ws->t, (void *)ws->V, (void *)ws->V32, (void *)ws->z32,
+                      (void *)ws->b32, (void *)ws->t32, (void *)ws->d32, (void *)ws->partial, (void *)ws->h})
+         if (p) cudaFree(p);
+      delete ws;
+      ctx->solver = nullptr;
+   }
+   ws = new ubolt_solver();
+   ws->restart = m;
+   ws->n = ctx->n_rows;
+   ws->mixed = mixed;
+   ws->red_blocks = std::min(GridFor(ws->n), 1184);
+   const int64_t n = ws->n;
+   auto alloc = [&](void **p, size_t bytes) -> int {
+      const cudaError_t e = cudaMalloc(p, std::max<size_t>(bytes, 16));
+      if (e != cudaSuccess) {
+         cudaGetLastError();
+         *p = nullptr;
+         return SetError(UBOLT_ERR_NOMEM, "solver workspace: cudaMalloc of %zu bytes: %s", bytes,
+                         cudaGetErrorString(e));
+      }
+      return UBOLT_OK;
+   };
+   int rc = 0;
+   ctx->solver = ws;
+   if ((rc = alloc((void **)&ws->r, n * 8)) || (rc = alloc((void **)&ws->z, n * 8)) ||
+       (rc = alloc((void **)&ws->t, n * 8)) || (rc = alloc((void **)&ws->partial, (size_t)ws->red_blocks * (m + 2) * 8)) ||
+       (rc = alloc((void **)&ws->h, 3 * (size_t)(m + 2) * 8)))
+      return rc;
+   if (!mixed) {
+      if ((rc = alloc((void **)&ws->V, (size_t)(m + 1) * n * 8))) return rc;
+   } else {
+      if ((rc = alloc((void **)&ws->V32, (size_t)(m + 1) * n * 4)) || (rc = alloc((void **)&ws->z32, n * 4)) ||
+          (rc = alloc((void **)&ws->b32, n * 4)) || (rc = alloc((void **)&ws->t32, n * 4)) ||
+          (rc = alloc((void **)&ws->d32, n * 4)))
+         return rc;
+   }
+   return UBOLT_OK;
+}
+
+}  // namespace ubolt
+
+using namespace ubolt;
+
+void UboltSolverFree(ubolt_ctx *ctx)
+{
+   ubolt_solver *ws = ctx->solver;
+   if (!ws) return;
+   for (void *p : {(void *)ws->r, (void *)ws->z, (void *)ws->t, (void *)ws->V, (void *)ws->V32, (void *)ws->z32,
+                   (void *)ws->b32, (void *)ws->t32, (void *)ws->d32, (void *)ws->partial, (void *)ws->h})
+      if (p) cudaFree(p);
+   delete ws;
+   ctx->solver = nullptr;
+}
+
+extern "C" void ubolt_solve_defaults(ubolt_solve_options *o)
+{
+   if (!o) return;
+   o->rtol = 1e-8;
+   o->max_it = 500;
+   o->restart = 30;
+   o->precision = UBOLT_PRECISION_FP64;
+   o->pc = UBOLT_PC_SWEEP;
+   o->inner_rtol = 1e-5;
+   o->max_outer = 10;
+   o->x_zero = 1;
+}
+
+extern "C" int ubolt_solver_setup(ubolt_ctx *ctx, const ubolt_solve_options *opts)
+{
+   int rc = CheckReady(ctx, false);
+   if (rc) return rc;
+   ubolt_solve_options o;
+   ubolt_solve_defaults(&o);
+   if (opts) o = *opts;
+   if (o.restart < 1 || o.restart > 200) return SetError(UBOLT_ERR_ARG, "restart %d (1..200)", o.restart);
+   if ((rc = EnsureWorkspace(ctx, &o))) return rc;
+   if ((o.pc == UBOLT_PC_SWEEP || o.pc == UBOLT_PC_SWEEP_DSA) && !ctx->sweep) return ubolt_sweep_setup(ctx, 0);
+   return UBOLT_OK;
+}
+
+extern "C" int ubolt_solve(ubolt_ctx *ctx, const double *b, double *x, const ubolt_solve_options *opts,
+                           ubolt_solve_stats *stats, void *stream)
+{
+   int rc = CheckReady(ctx, true);
+   if (rc) return rc;
+   if (!b || !x || (const void *)b == (const void *)x) return SetError(UBOLT_ERR_ARG, "solve: b and x must be distinct");
+   ubolt_solve_options o;
+   ubolt_solve_defaults(&o);
+   if (opts) o = *opts;
+   if (!(o.rtol > 0.0) || o.max_it < 1) return SetError(UBOLT_ERR_ARG, "solve: rtol must be > 0 and max_it >= 1");
+   if ((rc = ubolt_solver_setup(ctx, &o))) return rc;
+   ubolt_solver *ws = ctx->solver;
+   cudaStream_t s = (cudaStream_t)stream;
+   const int64_t n = ws->n;
+   const int grid = GridFor(n);
+   const auto t0 = std::chrono::steady_clock::now();
+   if (o.x_zero) cudaMemsetAsync(x, 0, n * sizeof(double), s);
+   const double bnorm = Norm<double>(ws, b, n, s, &rc);
+   if (rc) return rc;
+   if (!std::isfinite(bnorm)) return SetError(UBOLT_ERR_NONFINITE, "the right-hand side is not finite");
+
+   ubolt_solve_stats st{};
+   bool converged = false;
+   if (bnorm == 0.0) {
+      cudaMemsetAsync(x, 0, n * sizeof(double), s);
+      converged = true;
+   } else if (o.precision == UBOLT_PRECISION_FP64) {
+      GmresResult res;
+      rc = Gmres<double>(ctx, ws, ws->V, ws->z, ws->t, b, x, bnorm, o.rtol, o.max_it, o.pc, o.x_zero != 0, &res,
+                         stream);
+      if (rc) return rc;
+      st.iterations = res.iterations;
+      st.outer = 1;
+      converged = res.converged;
+   } else {
+      // Iterative refinement: r = b - A x in FP64, A d = r in FP32, x += d
+      bool x_zero = o.x_zero != 0;
+      for (int outer = 0; outer < o.max_outer; outer++) {
+         if (x_zero) {
+            cudaMemcpyAsync(ws->r, b, n * sizeof(double), cudaMemcpyDeviceToDevice, s);
+         } else {
+            if ((rc = ubolt_apply(ctx, x, ws->r, stream))) return rc;
+            ResidualKernel<double><<<grid, 256, 0, s>>>(b, ws->r, n);
+         }
+         const double rnorm = Norm<double>(ws, ws->r, n, s, &rc);
+         if (rc) return rc;
+         if (!std::isfinite(rnorm)) return SetError(UBOLT_ERR_NONFINITE, "refinement residual is not finite");
+         st.residual = rnorm / bnorm;
+         if (rnorm <= o.rtol * bnorm) {
+            converged = true;
+            break;
+         }
+         st.outer = outer + 1;
+         // The correction equation, scaled to unit norm so FP32 has the range
+         ScaleKernel<double, float><<<grid, 256, 0, s>>>(ws->r, ws->b32, 1.0 / rnorm, n);
+         cudaMemsetAsync(ws->d32, 0, n * sizeof(float), s);
+         GmresResult res;
+         const double inner = std::max(o.inner_rtol, 0.5 * o.rtol * bnorm / rnorm);
+         rc = Gmres<float>(ctx, ws, ws->V32, ws->z32, ws->t32, ws->b32, ws->d32, 1.0, inner,
+                           o.max_it - st.iterations, o.pc, true, &res, stream);
+         if (rc) return rc;
+         st.iterations += res.iterations;
+         AxpyKernel<float, double><<<grid, 256, 0, s>>>(ws->d32, x, rnorm, n);
+         x_zero = false;
+         if (st.iterations >= o.max_it) break;
+      }
+   }
+   // The true residual of what is returned
+   if ((rc = ubolt_apply(ctx, x, ws->r, stream))) return rc;
+   ResidualKernel<double><<<grid, 256, 0, s>>>(b, ws->r, n);
+   const double rn = Norm<double>(ws, ws->r, n, s, &rc);
+   if (rc) return rc;
+   st.residual = bnorm > 0 ? rn / bnorm : 0.0;
+   st.rnorm0 = bnorm;
+   st.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+   if (ctx->sweep && (o.pc == UBOLT_PC_SWEEP || o.pc == UBOLT_PC_SWEEP_DSA)) {
+      ubolt_sweep_info si;
+      if ((rc = ubolt_sweep_status(ctx, &si, stream))) return rc;
+   }
+   converged = converged && st.residual <= o.rtol * 1.01;
+   st.converged = converged ? 1 : 0;
+   if (stats) *stats = st;
+   if (!converged)
+      return SetError(UBOLT_ERR_NOT_CONVERGED, "not converged: true residual %.3e after %d iterations", st.residual,
+                      st.iterations);
+   return UBOLT_OK;
+}

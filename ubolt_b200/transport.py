@@ -174,3 +174,45 @@ class GroupTransfer:
         check(lib.ubolt_add_transfer(self.ctx.handle, _p(self.phi[g_from]), _p(self.sigma_s[g_from][g_to]), _p(b),
                                      _stream(stream)))
         return b
+
+
+class Sweep:
+    """psi = L^{-1} q for every ordinate - the streaming stage (PCAIR's place)."""
+
+    def __init__(self, ctx, patch_size=0):
+        self.ctx = ctx
+        check(lib.ubolt_sweep_setup(ctx.handle, patch_size))
+
+    def apply(self, q, psi=None, stream=None):
+        psi = torch.empty_like(q) if psi is None else psi
+        fn = lib.ubolt_sweep if q.dtype == torch.float64 else lib.ubolt_sweep_f32
+        check(fn(self.ctx.handle, _p(q), _p(psi), _stream(stream)))
+        return psi
+
+    def status(self, stream=None):
+        info = _lib.SweepInfo()
+        check(lib.ubolt_sweep_status(self.ctx.handle, C.byref(info), _stream(stream)))
+        return {k: getattr(info, k) for k, _ in info._fields_ if k != "pad_"}
+
+
+class TransportSolver:
+    """GMRES (right-preconditioned) on the current group: TransportSolver::solve."""
+
+    def __init__(self, ctx, rtol=1e-8, precision="fp64", pc="sweep", restart=30, max_it=500, inner_rtol=1e-5,
+                 max_outer=10):
+        self.ctx = ctx
+        o = _lib.SolveOptions()
+        lib.ubolt_solve_defaults(C.byref(o))
+        o.rtol, o.inner_rtol, o.max_it, o.restart, o.max_outer = rtol, inner_rtol, max_it, restart, max_outer
+        o.precision = {"fp64": _lib.PRECISION_FP64, "mixed": _lib.PRECISION_MIXED}[precision]
+        o.pc = {"none": _lib.PC_NONE, "block": _lib.PC_BLOCK, "sweep": _lib.PC_SWEEP,
+                "sweep+dsa": _lib.PC_SWEEP_DSA}[pc]
+        self.opts = o
+        check(lib.ubolt_solver_setup(ctx.handle, C.byref(o)))
+
+    def solve(self, b, x=None, stream=None, x_zero=True):
+        x = torch.zeros_like(b) if x is None else x
+        self.opts.x_zero = 1 if x_zero else 0
+        st = _lib.SolveStats()
+        check(lib.ubolt_solve(self.ctx.handle, _p(b), _p(x), C.byref(self.opts), C.byref(st), _stream(stream)))
+        return x, {k: getattr(st, k) for k, _ in st._fields_ if k != "pad_"}
