@@ -49,6 +49,8 @@ enum { UBOLT_BC_VACUUM = 0, UBOLT_BC_REFLECT = 1 };
 
 const char *ubolt_last_error(void);
 const char *ubolt_version(void);
+/* Kernels this library has launched in this process (all contexts). */
+uint64_t ubolt_launch_count(void);
 
 /* ~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~
  * Angular quadrature (host)
@@ -307,6 +309,29 @@ int ubolt_solver_setup(ubolt_ctx *ctx, const ubolt_solve_options *opts);
  * Returns UBOLT_ERR_NOT_CONVERGED, with x and stats filled, at max_it. */
 int ubolt_solve(ubolt_ctx *ctx, const double *b, double *x, const ubolt_solve_options *opts,
                 ubolt_solve_stats *stats, void *stream);
+
+/* ~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~
+ * Adjoint and gradients. No reference counterpart (the reference has no
+ * adjoint, docs/architecture.md:493-494; it tests the identity the adjoint
+ * rests on, (V A)^T = P (V A) P, docs/architecture.md:284-304).
+ * ~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~ */
+
+/* Solve (L - S)^T lambda = g: GMRES on ubolt_apply_adjoint, preconditioned
+ * with the transposed stage - the sweep of the reversed ordinates,
+ * L^{-T} = V P L^{-1} P V^{-1} (P swaps each ordinate with its opposite, V is
+ * the cell volume per row), or the transposed element blocks. Options and
+ * returns as ubolt_solve. */
+int ubolt_solve_adjoint(ubolt_ctx *ctx, const double *g, double *lambda, const ubolt_solve_options *opts,
+                        ubolt_solve_stats *stats, void *stream);
+/* g(c, 0, a) += detector(c) V_c w_a: the adjoint source of the response
+ * J = sum_c detector(c) V_c phi(c, 0) = g^T psi (detector: device, n_cells). */
+int ubolt_add_response_source(ubolt_ctx *ctx, const double *detector, double *g, void *stream);
+/* dJ/dsigma_t(c) = -sum_{rows of c} lambda psi and
+ * dJ/dsigma_s(c) = sum_i (sum_a lambda(c,i,a)) (sum_b w_b psi(c,i,b)) / W,
+ * for J = g^T psi with A psi = b and A^T lambda = g (device, n_cells each;
+ * either output may be NULL). */
+int ubolt_gradient(ubolt_ctx *ctx, const double *psi, const double *lambda, double *grad_sigma_t,
+                   double *grad_sigma_s, void *stream);
 
 #ifdef __cplusplus
 }

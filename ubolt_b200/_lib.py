@@ -151,3 +151,8 @@ def sweep_plan(geometry, quad, patch_size=0):
         return out
     finally:
         lib.ubolt_sweep_plan_free(h)
+
+_sig("ubolt_launch_count", C.c_uint64)
+_sig("ubolt_solve_adjoint", C.c_int, vp, vp, vp, C.POINTER(SolveOptions), C.POINTER(SolveStats), vp)
+_sig("ubolt_add_response_source", C.c_int, vp, vp, vp, vp)
+_sig("ubolt_gradient", C.c_int, vp, vp, vp, vp, vp, vp)

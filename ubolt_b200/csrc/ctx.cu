@@ -2,6 +2,7 @@
 // FP32 mirror, and the per-group cross-section pointers.
 #include "ctx.h"
 
+#include <atomic>
 #include <cstring>
 #include <unordered_map>
 
@@ -13,7 +14,16 @@ int CudaCheck(cudaError_t e, const char *what)
    return SetError(UBOLT_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
 }
 
-int CheckLaunch(const char *what) { return CudaCheck(cudaGetLastError(), what); }
+static std::atomic<uint64_t> g_launches{0};
+
+void CountLaunch(int n) { g_launches.fetch_add((uint64_t)n, std::memory_order_relaxed); }
+
+// Every launch wrapper calls this once per kernel it launched
+int CheckLaunch(const char *what)
+{
+   CountLaunch(1);
+   return CudaCheck(cudaGetLastError(), what);
+}
 
 int CheckReady(const ubolt_ctx *ctx, bool need_group)
 {
@@ -257,6 +267,21 @@ extern "C" int ubolt_ctx_create(const ubolt_dg_geometry *geom, const ubolt_quadr
    h.sigma_t = ctx->sigma_t32;
    h.sigma_s = ctx->sigma_s32;
    if ((rc = Upload(ctx, ctx->h_volume, &ctx->d_volume))) return fail(rc);
+   {
+      // The opposite ordinate (every cosine negated), by exact search
+      std::vector<int32_t> opp(A, -1);
+      for (int a = 0; a < A; a++)
+         for (int b = 0; b < A; b++)
+            if (ctx->h_omega[3 * b] == -ctx->h_omega[3 * a] && ctx->h_omega[3 * b + 1] == -ctx->h_omega[3 * a + 1] &&
+                ctx->h_omega[3 * b + 2] == -ctx->h_omega[3 * a + 2]) {
+               opp[a] = b;
+               break;
+            }
+      for (int a = 0; a < A; a++)
+         if (opp[a] < 0 || ctx->h_w[opp[a]] != ctx->h_w[a])
+            return fail(SetError(UBOLT_ERR_ARG, "ordinate %d has no opposite of equal weight", a));
+      if ((rc = Upload(ctx, opp, &ctx->d_opp))) return fail(rc);
+   }
    if ((rc = CtxAlloc(ctx, 64 * sizeof(unsigned long long), &p))) return fail(rc);
    ctx->d_counters = static_cast<unsigned long long *>(p);
    if ((rc = CudaCheck(cudaDeviceSynchronize(), "ctx_create"))) return fail(rc);
@@ -267,6 +292,8 @@ extern "C" int ubolt_ctx_create(const ubolt_dg_geometry *geom, const ubolt_quadr
 void UboltSweepFree(ubolt_ctx *ctx);
 void UboltDsaFree(ubolt_ctx *ctx);
 void UboltSolverFree(ubolt_ctx *ctx);
+
+extern "C" uint64_t ubolt_launch_count(void) { return g_launches.load(); }
 
 extern "C" int ubolt_ctx_destroy(ubolt_ctx *ctx)
 {
@@ -304,6 +331,7 @@ extern "C" int ubolt_set_group(ubolt_ctx *ctx, const double *sigma_t, const doub
    cudaStream_t s = (cudaStream_t)stream;
    ToFloatKernel<double><<<(n + 255) / 256, 256, 0, s>>>(sigma_t, ctx->sigma_t32, n);
    ToFloatKernel<double><<<(n + 255) / 256, 256, 0, s>>>(sigma_s_within, ctx->sigma_s32, n);
+   CountLaunch(1);
    rc = CheckLaunch("set_group");
    if (rc) return rc;
    ctx->group_set = true;

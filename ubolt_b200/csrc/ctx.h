@@ -32,6 +32,7 @@ struct ubolt_ctx {
    ubolt::DevGeom<float> g32{};
    float *sigma_t32 = nullptr, *sigma_s32 = nullptr;
    const double *d_volume = nullptr;           // [n_cells] FP64 cell volumes
+   const int32_t *d_opp = nullptr;             // [A] the ordinate opposite each ordinate
    unsigned long long *d_counters = nullptr;   // 64 counters/flags for set-up calls
    bool group_set = false;
 
@@ -57,6 +58,8 @@ inline const ubolt::DevGeom<float> &ubolt_ctx::geom<float>() const
 namespace ubolt {
 
 int CheckLaunch(const char *what);
+// Count kernels launched by the library (ubolt_launch_count)
+void CountLaunch(int n = 1);
 int CudaCheck(cudaError_t e, const char *what);
 // Context exists (and, with need_group, has cross sections) and its device is current
 int CheckReady(const ubolt_ctx *ctx, bool need_group);

@@ -152,6 +152,7 @@ static void MultiDot(const ubolt_solver *ws, const S *V, int nv, const S *w, int
       MultiDotKernel<S><<<ws->red_blocks, kRedThreads, 0, s>>>(V, n, i0, std::min(kChunk, nv - i0), w, ws->partial,
                                                                 stride);
    ReducePartialKernel<<<nv, 256, 0, s>>>(ws->partial, ws->red_blocks, stride, h);
+   CountLaunch((nv + kChunk - 1) / kChunk + 1);
 }
 
 template <typename S>
@@ -165,28 +166,57 @@ static double Norm(const ubolt_solver *ws, const S *x, int64_t n, cudaStream_t s
    return std::sqrt(v);
 }
 
-template <typename T>
-int OperatorApply(ubolt_ctx *ctx, const T *x, T *y, void *stream);
-template <>
-int OperatorApply<double>(ubolt_ctx *ctx, const double *x, double *y, void *stream)
+// y(c, i, a) = scale(c) x(c, i, opp(a)): P (the swap of each ordinate with
+// its opposite) times V^{-1} (inverse = 1) or V (inverse = 0), V the cell volume
+template <typename S>
+__global__ void OppositeScaleKernel(const S *__restrict__ x, S *__restrict__ y, const int32_t *__restrict__ opp,
+                                    const double *__restrict__ volume, int nb, int A, int64_t n, int inverse)
 {
-   return ubolt_apply(ctx, x, y, stream);
-}
-template <>
-int OperatorApply<float>(ubolt_ctx *ctx, const float *x, float *y, void *stream)
-{
-   return ubolt_apply_f32(ctx, x, y, stream);
+   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+      const int64_t node = r / A;
+      const int a = (int)(r - node * A);
+      const double v = volume[node / nb];
+      y[r] = (S)((double)x[node * A + opp[a]] * (inverse ? 1.0 / v : v));
+   }
 }
 
-// y = M^{-1} x. tmp is scratch of n values (the DSA stage's residual).
+// The system GMRES iterates on: A = L - S, or its transpose for the adjoint
 template <typename T>
-static int Precondition(ubolt_ctx *ctx, int pc, const T *x, T *y, T *tmp, int64_t n, void *stream)
+int OperatorApply(ubolt_ctx *ctx, bool adjoint, const T *x, T *y, void *stream);
+template <>
+int OperatorApply<double>(ubolt_ctx *ctx, bool adjoint, const double *x, double *y, void *stream)
 {
+   return adjoint ? ubolt_apply_adjoint(ctx, x, y, stream) : ubolt_apply(ctx, x, y, stream);
+}
+template <>
+int OperatorApply<float>(ubolt_ctx *ctx, bool adjoint, const float *x, float *y, void *stream)
+{
+   return adjoint ? ubolt_apply_adjoint_f32(ctx, x, y, stream) : ubolt_apply_f32(ctx, x, y, stream);
+}
+
+// y = M^{-1} x. tmp is scratch of n values. For the adjoint system the
+// transposed preconditioner: the transposed blocks, or the sweep of the
+// reversed ordinates, L^{-T} = V P L^{-1} P V^{-1} - from (V L)^T = P (V L) P
+// (docs/architecture.md:284-304 of the reference; P swaps each ordinate with
+// its opposite, V is the cell volume per row).
+template <typename T>
+static int Precondition(ubolt_ctx *ctx, int pc, bool adjoint, const T *x, T *y, T *tmp, int64_t n, void *stream)
+{
+   cudaStream_t s = (cudaStream_t)stream;
+   if (adjoint && (pc == UBOLT_PC_SWEEP || pc == UBOLT_PC_SWEEP_DSA)) {
+      const int grid = (int)std::min<int64_t>((n + 255) / 256, 148 * 8);
+      OppositeScaleKernel<T><<<grid, 256, 0, s>>>(x, tmp, ctx->d_opp, ctx->d_volume, ctx->nb, ctx->A, n, 1);
+      CountLaunch();
+      int rc = Sweep<T>(ctx, tmp, y, stream);
+      if (rc) return rc;
+      OppositeScaleKernel<T><<<grid, 256, 0, s>>>(y, tmp, ctx->d_opp, ctx->d_volume, ctx->nb, ctx->A, n, 0);
+      CountLaunch();
+      return CudaCheck(cudaMemcpyAsync(y, tmp, n * sizeof(T), cudaMemcpyDeviceToDevice, s), "adjoint pc");
+   }
    switch (pc) {
    case UBOLT_PC_NONE:
-      return CudaCheck(cudaMemcpyAsync(y, x, n * sizeof(T), cudaMemcpyDeviceToDevice, (cudaStream_t)stream),
-                       "pc copy");
-   case UBOLT_PC_BLOCK: return BlockApply<T>(ctx, x, y, false, stream);
+      return CudaCheck(cudaMemcpyAsync(y, x, n * sizeof(T), cudaMemcpyDeviceToDevice, s), "pc copy");
+   case UBOLT_PC_BLOCK: return BlockApply<T>(ctx, x, y, adjoint, stream);
    case UBOLT_PC_SWEEP: return Sweep<T>(ctx, x, y, stream);
    case UBOLT_PC_SWEEP_DSA: {
       int rc = Sweep<T>(ctx, x, y, stream);
@@ -207,7 +237,7 @@ struct GmresResult {
 // guess in x (x_zero: it is zero). V: (m + 1) n basis, z, t: n each.
 template <typename S>
 static int Gmres(ubolt_ctx *ctx, const ubolt_solver *ws, S *V, S *z, S *t, const S *b, S *x, double bnorm,
-                 double rtol, int max_it, int pc, bool x_zero, GmresResult *out, void *stream)
+                 double rtol, int max_it, int pc, bool adjoint, bool x_zero, GmresResult *out, void *stream)
 {
    cudaStream_t s = (cudaStream_t)stream;
    const int64_t n = ws->n;
@@ -223,8 +253,9 @@ static int Gmres(ubolt_ctx *ctx, const ubolt_solver *ws, S *V, S *z, S *t, const
          rc = CudaCheck(cudaMemcpyAsync(V, b, n * sizeof(S), cudaMemcpyDeviceToDevice, s), "gmres");
          x_zero = false;
       } else {
-         rc = OperatorApply<S>(ctx, x, V, stream);
+         rc = OperatorApply<S>(ctx, adjoint, x, V, stream);
          ResidualKernel<S><<<grid, 256, 0, s>>>(b, V, n);
+         CountLaunch();
       }
       if (rc) return rc;
       const double beta = Norm<S>(ws, V, n, s, &rc);
@@ -236,17 +267,20 @@ static int Gmres(ubolt_ctx *ctx, const ubolt_solver *ws, S *V, S *z, S *t, const
          break;
       }
       ScaleKernel<S, S><<<grid, 256, 0, s>>>(V, V, 1.0 / beta, n);
+      CountLaunch();
       std::fill(g.begin(), g.end(), 0.0);
       g[0] = beta;
       int j = 0;
       for (; j < m && out->iterations < max_it; j++) {
          S *vj = V + (int64_t)j * n, *vn = V + (int64_t)(j + 1) * n;
-         if ((rc = Precondition<S>(ctx, pc, vj, z, t, n, stream))) return rc;
-         if ((rc = OperatorApply<S>(ctx, z, vn, stream))) return rc;
+         if ((rc = Precondition<S>(ctx, pc, adjoint, vj, z, t, n, stream))) return rc;
+         if ((rc = OperatorApply<S>(ctx, adjoint, z, vn, stream))) return rc;
          MultiDot<S>(ws, V, j + 1, vn, n, dh1, s);
          MultiAxpyKernel<S><<<grid, 256, 0, s>>>(V, n, j + 1, dh1, -1.0, vn, 1);
+         CountLaunch();
          MultiDot<S>(ws, V, j + 1, vn, n, dh2, s);
          MultiAxpyKernel<S><<<grid, 256, 0, s>>>(V, n, j + 1, dh2, -1.0, vn, 1);
+         CountLaunch();
          MultiDot<S>(ws, vn, 1, vn, n, dh2 + j + 1, s);
          cudaMemcpyAsync(h1.data(), dh1, (j + 1) * sizeof(double), cudaMemcpyDeviceToHost, s);
          cudaMemcpyAsync(h2.data(), dh2, (j + 2) * sizeof(double), cudaMemcpyDeviceToHost, s);
@@ -255,7 +289,10 @@ static int Gmres(ubolt_ctx *ctx, const ubolt_solver *ws, S *V, S *z, S *t, const
          const double hn = std::sqrt(h2[j + 1]);
          if (!std::isfinite(hn)) return SetError(UBOLT_ERR_NONFINITE, "GMRES Arnoldi vector is not finite");
          for (int i = 0; i <= j; i++) H[i * m + j] = h1[i] + h2[i];
-         if (hn > 0.0) ScaleKernel<S, S><<<grid, 256, 0, s>>>(vn, vn, 1.0 / hn, n);
+         if (hn > 0.0) {
+            ScaleKernel<S, S><<<grid, 256, 0, s>>>(vn, vn, 1.0 / hn, n);
+            CountLaunch();
+         }
          for (int i = 0; i < j; i++) {
             const double tt = cs[i] * H[i * m + j] + sn[i] * H[(i + 1) * m + j];
             H[(i + 1) * m + j] = -sn[i] * H[i * m + j] + cs[i] * H[(i + 1) * m + j];
@@ -285,8 +322,10 @@ static int Gmres(ubolt_ctx *ctx, const ubolt_solver *ws, S *V, S *z, S *t, const
       // V_j is free scratch here: the next cycle rebuilds the basis
       S *u = V + (int64_t)m * n;
       MultiAxpyKernel<S><<<grid, 256, 0, s>>>(V, n, j, dy, 1.0, u, 0);
-      if ((rc = Precondition<S>(ctx, pc, u, z, t, n, stream))) return rc;
+      CountLaunch();
+      if ((rc = Precondition<S>(ctx, pc, adjoint, u, z, t, n, stream))) return rc;
       AxpyKernel<S, S><<<grid, 256, 0, s>>>(z, x, 1.0, n);
+      CountLaunch();
       if (out->converged) break;
    }
    return CheckLaunch("gmres");
@@ -381,8 +420,8 @@ extern "C" int ubolt_solver_setup(ubolt_ctx *ctx, const ubolt_solve_options *opt
    return UBOLT_OK;
 }
 
-extern "C" int ubolt_solve(ubolt_ctx *ctx, const double *b, double *x, const ubolt_solve_options *opts,
-                           ubolt_solve_stats *stats, void *stream)
+static int SolveSystem(ubolt_ctx *ctx, bool adjoint, const double *b, double *x, const ubolt_solve_options *opts,
+                       ubolt_solve_stats *stats, void *stream)
 {
    int rc = CheckReady(ctx, true);
    if (rc) return rc;
@@ -409,7 +448,7 @@ extern "C" int ubolt_solve(ubolt_ctx *ctx, const double *b, double *x, const ubo
       converged = true;
    } else if (o.precision == UBOLT_PRECISION_FP64) {
       GmresResult res;
-      rc = Gmres<double>(ctx, ws, ws->V, ws->z, ws->t, b, x, bnorm, o.rtol, o.max_it, o.pc, o.x_zero != 0, &res,
+      rc = Gmres<double>(ctx, ws, ws->V, ws->z, ws->t, b, x, bnorm, o.rtol, o.max_it, o.pc, adjoint, o.x_zero != 0, &res,
                          stream);
       if (rc) return rc;
       st.iterations = res.iterations;
@@ -422,8 +461,9 @@ extern "C" int ubolt_solve(ubolt_ctx *ctx, const double *b, double *x, const ubo
          if (x_zero) {
             cudaMemcpyAsync(ws->r, b, n * sizeof(double), cudaMemcpyDeviceToDevice, s);
          } else {
-            if ((rc = ubolt_apply(ctx, x, ws->r, stream))) return rc;
+            if ((rc = OperatorApply<double>(ctx, adjoint, x, ws->r, stream))) return rc;
             ResidualKernel<double><<<grid, 256, 0, s>>>(b, ws->r, n);
+            CountLaunch();
          }
          const double rnorm = Norm<double>(ws, ws->r, n, s, &rc);
          if (rc) return rc;
@@ -436,21 +476,24 @@ extern "C" int ubolt_solve(ubolt_ctx *ctx, const double *b, double *x, const ubo
          st.outer = outer + 1;
          // The correction equation, scaled to unit norm so FP32 has the range
          ScaleKernel<double, float><<<grid, 256, 0, s>>>(ws->r, ws->b32, 1.0 / rnorm, n);
+         CountLaunch();
          cudaMemsetAsync(ws->d32, 0, n * sizeof(float), s);
          GmresResult res;
          const double inner = std::max(o.inner_rtol, 0.5 * o.rtol * bnorm / rnorm);
          rc = Gmres<float>(ctx, ws, ws->V32, ws->z32, ws->t32, ws->b32, ws->d32, 1.0, inner,
-                           o.max_it - st.iterations, o.pc, true, &res, stream);
+                           o.max_it - st.iterations, o.pc, adjoint, true, &res, stream);
          if (rc) return rc;
          st.iterations += res.iterations;
          AxpyKernel<float, double><<<grid, 256, 0, s>>>(ws->d32, x, rnorm, n);
+         CountLaunch();
          x_zero = false;
          if (st.iterations >= o.max_it) break;
       }
    }
    // The true residual of what is returned
-   if ((rc = ubolt_apply(ctx, x, ws->r, stream))) return rc;
+   if ((rc = OperatorApply<double>(ctx, adjoint, x, ws->r, stream))) return rc;
    ResidualKernel<double><<<grid, 256, 0, s>>>(b, ws->r, n);
+   CountLaunch();
    const double rn = Norm<double>(ws, ws->r, n, s, &rc);
    if (rc) return rc;
    st.residual = bnorm > 0 ? rn / bnorm : 0.0;
@@ -467,4 +510,16 @@ extern "C" int ubolt_solve(ubolt_ctx *ctx, const double *b, double *x, const ubo
       return SetError(UBOLT_ERR_NOT_CONVERGED, "not converged: true residual %.3e after %d iterations", st.residual,
                       st.iterations);
    return UBOLT_OK;
+}
+
+extern "C" int ubolt_solve(ubolt_ctx *ctx, const double *b, double *x, const ubolt_solve_options *opts,
+                           ubolt_solve_stats *stats, void *stream)
+{
+   return SolveSystem(ctx, false, b, x, opts, stats, stream);
+}
+
+extern "C" int ubolt_solve_adjoint(ubolt_ctx *ctx, const double *g, double *lambda, const ubolt_solve_options *opts,
+                                   ubolt_solve_stats *stats, void *stream)
+{
+   return SolveSystem(ctx, true, g, lambda, opts, stats, stream);
 }

@@ -216,3 +216,73 @@ class TransportSolver:
         st = _lib.SolveStats()
         check(lib.ubolt_solve(self.ctx.handle, _p(b), _p(x), C.byref(self.opts), C.byref(st), _stream(stream)))
         return x, {k: getattr(st, k) for k, _ in st._fields_ if k != "pad_"}
+
+    def solve_adjoint(self, g, lam=None, stream=None, x_zero=True):
+        """(L - S)^T lambda = g with the hand-written transpose operator."""
+        lam = torch.zeros_like(g) if lam is None else lam
+        self.opts.x_zero = 1 if x_zero else 0
+        st = _lib.SolveStats()
+        check(lib.ubolt_solve_adjoint(self.ctx.handle, _p(g), _p(lam), C.byref(self.opts), C.byref(st),
+                                      _stream(stream)))
+        return lam, {k: getattr(st, k) for k, _ in st._fields_ if k != "pad_"}
+
+
+def response_source(ctx, detector, g=None, stream=None):
+    """g += the adjoint source of J = sum_c detector(c) V_c phi(c, basis 0)."""
+    g = ctx.vector(fill=0.0) if g is None else g
+    check(lib.ubolt_add_response_source(ctx.handle, _p(detector), _p(g), _stream(stream)))
+    return g
+
+
+def gradient(ctx, psi, lam, stream=None):
+    """(dJ/dsigma_t, dJ/dsigma_s) per cell from the forward and adjoint fluxes."""
+    gt = torch.empty(ctx.n_cells, dtype=torch.float64, device=psi.device)
+    gs = torch.empty_like(gt)
+    check(lib.ubolt_gradient(ctx.handle, _p(psi), _p(lam), _p(gt), _p(gs), _stream(stream)))
+    return gt, gs
+
+
+class _Response(torch.autograd.Function):
+    @staticmethod
+    def forward(fctx, sigma_t, sigma_s, model):
+        st = sigma_t.detach().contiguous().double()
+        ss = sigma_s.detach().contiguous().double()
+        model.ctx.set_group(st, ss)
+        psi, stats = model.solver.solve(model.b)
+        model.last_forward = stats
+        J = torch.dot(model.g, psi)
+        fctx.model = model
+        fctx.keep = (st, ss)
+        fctx.save_for_backward(psi)
+        return J
+
+    @staticmethod
+    def backward(fctx, grad_J):
+        (psi,) = fctx.saved_tensors
+        model = fctx.model
+        model.ctx.set_group(*fctx.keep)
+        lam, stats = model.solver.solve_adjoint(model.g)
+        model.last_adjoint = stats
+        gt, gs = gradient(model.ctx, psi, lam)
+        return grad_J * gt, grad_J * gs, None
+
+
+class DetectorResponse:
+    """J(sigma_t, sigma_s) = sum_c detector(c) V_c phi(c, 0) of the fixed-source
+    solution, differentiable with respect to both per-cell cross sections
+    through the adjoint solve (a torch.autograd.Function over the C ABI)."""
+
+    def __init__(self, ctx, source_cell, detector_cell, side_inflow=None, **solver_opts):
+        self.ctx = ctx
+        dev = ctx.device
+        self.source = torch.as_tensor(source_cell, dtype=torch.float64, device=dev)
+        self.detector = torch.as_tensor(detector_cell, dtype=torch.float64, device=dev)
+        self.b = ctx.vector(fill=0.0)
+        if side_inflow is not None:
+            fill_inflow(ctx, side_inflow, self.b)
+        check(lib.ubolt_add_source(ctx.handle, _p(self.source), _p(self.b), _stream()))
+        self.g = response_source(ctx, self.detector)
+        self.solver = TransportSolver(ctx, **solver_opts)
+
+    def __call__(self, sigma_t, sigma_s):
+        return _Response.apply(sigma_t, sigma_s, self)
