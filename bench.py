@@ -1,0 +1,385 @@
+"""Benchmark: the fixed-source DG1 SN solve on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step is one full solve, from zero, of the 256 x 256 jittered-triangle DG1
+S8 one-group problem (15.7M unknowns) to a true relative residual of 1e-8,
+plain FP64, with the right-hand side resident in HBM: the reference's plain
+FP64 drop-in configuration. `value` is seconds per solve (lower is better).
+Beside it the line carries the mixed FP32+FP64-refinement solve, the adjoint
+gradient of the detector response (same mesh), the operator apply in GB/s,
+the roofline of the dominant kernel, the CPU restatement timed on this host's
+cores, the end-to-end solve through the public API with host buffers, the SM
+clocks seen during the timed region and the library's kernel launch count.
+
+Multi-GPU: replicas only - each rank solves its own copy (the solve is not
+sharded); value aggregates the solves of all ranks per second of the slowest
+rank's time, reported as seconds per solve per replica set.
+
+--impl reference times the reference path's CPU restatement (the oracle port:
+the reference build needs PETSc + Kokkos + PFLARE, which are not installed) on
+all host cores, on the same workload; other ranks exit without work.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "solve s to 1e-8 resid, FP32+refine vs FP64 on 1 B200; adjoint grad s; apply GB/s"
+WORKLOAD = "tri256_dg1_s8: 2D DG1, 256x256 jittered quads split into 131072 triangles, S8 (40 ordinates), 1 group"
+
+
+def _args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--scale", type=float, default=1.0, help="mesh scale (1.0 = the named workload)")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--quick", action="store_true", help="skip the secondary measurements")
+    return p.parse_args()
+
+
+def _peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampled every 200 ms while the timed region runs."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 7:
+                self.samples.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def _dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_reference(args):
+    """The CPU restatement of the reference path on every host core."""
+    world, rank, _ = _dist()
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from ubolt_b200 import problem as P
+    prob = P.config_tri256(scale=args.scale)
+    g, q = prob.geometry, prob.quad
+    op = O.Operator(g, q, prob.sigma_t[0], prob.sigma_s[0, 0])
+    b = O.rhs(g, q, prob.source[0])
+    for _ in range(args.warmup):
+        op.solve(b, rtol=1e-8)
+    times, its = [], []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        x, it, res = op.solve(b, rtol=1e-8)
+        times.append(time.perf_counter() - t0)
+        its.append(it)
+    v = float(np.mean(times))
+    cores = O.threads()
+    line = {"metric": METRIC, "value": v, "unit": "s/solve", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "impl": "reference",
+            "config": {"workload": WORKLOAD, "rtol": 1e-8, "rows": int(op.n), "iterations": int(np.median(its)),
+                       "parallelism": f"replicas{args.gpus}"},
+            "cpu_baseline": {"value": v, "unit": "s/solve", "cores": cores, "kind": "port",
+                             "sample": "the full workload: one FP64 GMRES solve to 1e-8 with an upwind-sweep "
+                                       "preconditioner per step, OpenMP on every host core"},
+            "e2e": {"value": v, "unit": "s/solve", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline(args):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from ubolt_b200 import problem as P
+    prob = P.config_tri256(scale=args.scale)
+    g, q = prob.geometry, prob.quad
+    op = O.Operator(g, q, prob.sigma_t[0], prob.sigma_s[0, 0])
+    b = O.rhs(g, q, prob.source[0])
+    op.solve(b, rtol=1e-8)
+    t0 = time.perf_counter()
+    n = 2
+    for _ in range(n):
+        x, it, res = op.solve(b, rtol=1e-8)
+    v = (time.perf_counter() - t0) / n
+    return {"value": v, "unit": "s/solve", "cores": O.threads(), "kind": "port",
+            "sample": f"the full workload, {n} FP64 solves to 1e-8 ({it} iterations each), GMRES + CPU upwind "
+                      "sweep, OpenMP"}, x
+
+
+def main():
+    args = _args()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    import torch.distributed as dist
+    from ubolt_b200 import _lib
+    from ubolt_b200 import problem as P
+    from ubolt_b200 import transport as T
+
+    world, rank, local = _dist()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    prob = P.config_tri256(scale=args.scale)
+    g, q = prob.geometry, prob.quad
+    ctx = T.Context(g, q)
+    st = torch.tensor(prob.sigma_t[0], device="cuda")
+    ss = torch.tensor(prob.sigma_s[0, 0], device="cuda")
+    ctx.set_group(st, ss)
+    src = torch.tensor(prob.source[0], device="cuda")
+    b = ctx.vector(fill=0.0)
+    T.GroupTransfer(ctx, [[ss]], [src]).add_external(0, b)
+    n = ctx.n_rows
+    t_setup = time.perf_counter()
+    solver = T.TransportSolver(ctx, rtol=1e-8, precision="fp64", pc="sweep", restart=30, max_it=500)
+    setup_s = time.perf_counter() - t_setup
+    stream = torch.cuda.current_stream()
+    x = ctx.vector(fill=0.0)
+
+    # ~~~ Headline: plain FP64 solve, inputs resident
+    for _ in range(args.warmup):
+        solver.solve(b, x)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    launches0 = _lib.lib.ubolt_launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stats = []
+    with Clocks(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            x, st_ = solver.solve(b, x)
+            stats.append(st_)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    launches = (_lib.lib.ubolt_launch_count() - launches0)
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+    value = ms / 1e3 / world if world > 1 else ms / 1e3
+    its = int(np.median([s["iterations"] for s in stats]))
+    res = float(max(s["residual"] for s in stats))
+
+    extra = {}
+    if not args.quick:
+        # ~~~ Kernel timings: apply (FP64, FP32), sweep (FP64, FP32)
+        A = T.TransportOperator(ctx)
+        sw = T.Sweep.__new__(T.Sweep)
+        sw.ctx = ctx
+        def timed(fn, reps=20):
+            for _ in range(3):
+                fn()
+            torch.cuda.synchronize()
+            a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a0.record(stream)
+            for _ in range(reps):
+                fn()
+            a1.record(stream)
+            torch.cuda.synchronize()
+            return a0.elapsed_time(a1) / reps
+        xr = torch.randn(n, dtype=torch.float64, device="cuda")
+        yr = torch.empty_like(xr)
+        xf, yf = xr.float(), torch.empty(n, dtype=torch.float32, device="cuda")
+        t_apply64 = timed(lambda: A.mult(xr, yr))
+        t_apply32 = timed(lambda: A.mult(xf, yf))
+        t_sweep64 = timed(lambda: sw.apply(xr, yr))
+        t_sweep32 = timed(lambda: sw.apply(xf, yf))
+        apply_bytes64 = 2 * n * 8 + 2 * ctx.n_cells * 8
+        apply_bytes32 = 2 * n * 4 + 2 * ctx.n_cells * 4
+        sweep_bytes64 = 2 * n * 8 + ctx.n_cells * 8
+        extra["apply_gbs"] = {"fp64": apply_bytes64 / t_apply64 / 1e6, "fp32": apply_bytes32 / t_apply32 / 1e6,
+                              "fp64_us": t_apply64 * 1e3, "fp32_us": t_apply32 * 1e3}
+        extra["sweep_us"] = {"fp64": t_sweep64 * 1e3, "fp32": t_sweep32 * 1e3}
+        # Dominant kernel of the solve: one sweep and one apply per iteration
+        sweeps = its + 1
+        dom_sweep = t_sweep64 * sweeps >= t_apply64 * (its + 1)
+        peak, peak_kind = _peaks()
+        if dom_sweep:
+            ach = sweep_bytes64 / t_sweep64 / 1e6
+            kernel, traffic_key = "SweepKernel<double,3,3>", "sweep_fp64"
+        else:
+            ach = apply_bytes64 / t_apply64 / 1e6
+            kernel, traffic_key = "ApplyKernel<double,3,3,0>", "apply_fp64"
+        traffic = None
+        tpath = os.path.join(ROOT, "profiles", "traffic.json")
+        if os.path.exists(tpath):
+            try:
+                traffic = json.load(open(tpath)).get(traffic_key)
+            except Exception:
+                traffic = None
+        extra["roofline"] = {"bound": "hbm", "kernel": kernel, "achieved": ach, "peak": peak, "unit": "GB/s",
+                             "frac": ach / peak, "peak_source": peak_kind, "traffic": traffic,
+                             "share_of_solve": (t_sweep64 * sweeps if dom_sweep else t_apply64 * (its + 1)) / ms}
+
+        # ~~~ Mixed precision: FP32 operator / sweep / Krylov storage + FP64 refinement
+        mixed = T.TransportSolver(ctx, rtol=1e-8, precision="mixed", pc="sweep", restart=30, max_it=500,
+                                  inner_rtol=1e-5)
+        xm = ctx.vector(fill=0.0)
+        for _ in range(2):
+            mixed.solve(b, xm)
+        torch.cuda.synchronize()
+        m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        m0.record(stream)
+        for _ in range(args.steps):
+            xm, stm = mixed.solve(b, xm)
+        m1.record(stream)
+        torch.cuda.synchronize()
+        mixed_ms = m0.elapsed_time(m1) / args.steps
+        phi64 = T.angular_integral(ctx, x)
+        phim = T.angular_integral(ctx, xm)
+        extra["mixed"] = {"s_per_solve": mixed_ms / 1e3, "speedup_vs_fp64": ms / mixed_ms,
+                          "iterations": stm["iterations"], "outer": stm["outer"], "residual": stm["residual"],
+                          "phi_rel_err_vs_fp64": float((phim - phi64).norm() / phi64.norm())}
+        # FP64 solve back on its own workspace
+        solver = T.TransportSolver(ctx, rtol=1e-8, precision="fp64", pc="sweep", restart=30, max_it=500)
+
+        # ~~~ Adjoint gradient of the detector response over a seeded 16 x 16-cell patch
+        det = torch.tensor(P.detector_patch(prob).astype(np.float64), device="cuda")
+        model = T.DetectorResponse(ctx, prob.source[0], det.cpu().numpy(), rtol=1e-8, max_it=500)
+        sig_t = st.clone().requires_grad_(True)
+        sig_s = ss.clone().requires_grad_(True)
+        for _ in range(2):
+            J = model(sig_t, sig_s)
+            torch.autograd.grad(J, (sig_t, sig_s))
+        torch.cuda.synchronize()
+        g0, g1, g2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        g0.record(stream)
+        J = model(sig_t, sig_s)
+        g1.record(stream)
+        gt, gs = torch.autograd.grad(J, (sig_t, sig_s))
+        g2.record(stream)
+        torch.cuda.synchronize()
+        fwd_ms, tot_ms = g0.elapsed_time(g1), g0.elapsed_time(g2)
+        extra["adjoint"] = {"grad_s": tot_ms / 1e3, "forward_s": fwd_ms / 1e3,
+                            "adjoint_over_forward": (tot_ms - fwd_ms) / fwd_ms,
+                            "parameters": 2 * ctx.n_cells, "J": float(J.item()),
+                            "adjoint_iterations": model.last_adjoint["iterations"]}
+        ctx.set_group(st, ss)
+
+    # ~~~ End to end: pinned host b -> device, solve, x -> pinned host
+    hb = b.cpu().pin_memory()
+    hx = torch.empty(n, dtype=torch.float64).pin_memory()
+    db = torch.empty_like(b)
+    for _ in range(2):
+        db.copy_(hb, non_blocking=True)
+        x, _s = solver.solve(db, x)
+        hx.copy_(x, non_blocking=True)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(args.steps):
+        db.copy_(hb, non_blocking=True)
+        x, _s = solver.solve(db, x)
+        hx.copy_(x, non_blocking=True)
+    f1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(f0.elapsed_time(f1) / args.steps)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu, xcpu = cpu_baseline(args)
+        phi_c = np.asarray(T.angular_integral(ctx, x).cpu())
+        import oracle as O
+        phi_o = O.angular_integral(xcpu, ctx.n_nodes, q)
+        cpu["phi_rel_diff_gpu_vs_cpu"] = float(np.linalg.norm(phi_c - phi_o) / np.linalg.norm(phi_o))
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "s/solve", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, PCG64 20261203+1)",
+                "config": {"workload": WORKLOAD, "rows": n, "rtol": 1e-8, "iterations": its,
+                           "true_residual": res, "preconditioner": "exact upwind sweep (patch tasks)",
+                           "restart": 30, "parallelism": f"replicas{world}", "setup_s": setup_s,
+                           "l2": "each step (a full solve) streams >4 GB of Krylov vectors, far above the 126 MB L2"},
+                "gpu_launches": int(launches), "clocks": clk.summary(),
+                "e2e": {"value": e2e_ms / 1e3, "unit": "s/solve", "h2d_bytes_per_step": n * 8,
+                        "d2h_bytes_per_step": n * 8}}
+        line.update({k: v for k, v in extra.items() if k != "roofline"})
+        if "roofline" in extra:
+            line["roofline"] = extra["roofline"]
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

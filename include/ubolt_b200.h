@@ -269,6 +269,41 @@ int ubolt_sweep_plan_build(const ubolt_dg_geometry *geom, const ubolt_quadrature
 void ubolt_sweep_plan_free(ubolt_sweep_plan_host *plan);
 
 /* ~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~
+ * DSA: the diffusion correction y = P D^{-1} R x (DSAPrecon, include/ubolt/dsa.hpp)
+ * ~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~ */
+typedef struct {
+   double penalty;           /* MIP penalty C (-dsa_mip_penalty, default 4) */
+   double consistent_power;  /* DG0 consistent-D blend power p (default 1.5) */
+   int32_t consistent_d;     /* DG0: blend the upwind numerical diffusion in (default 1) */
+   int32_t inner_iterations; /* block-Jacobi PCG iterations of the inner solve (default 30) */
+} ubolt_dsa_options;
+
+void ubolt_dsa_defaults(ubolt_dsa_options *opts);
+/* Keep the host geometry the diffusion operator is built from and allocate
+ * its device storage (DSAPrecon::create on an UnstructuredDG,
+ * src/dsak.kokkos.cxx:113-121, src/dsa_plexk.kokkos.cxx:68-209). The
+ * geometry must be the context's. No voids: every sigma_t must be > 0. */
+int ubolt_dsa_setup(ubolt_ctx *ctx, const ubolt_dg_geometry *geom, const ubolt_dsa_options *opts);
+/* Refill the diffusion matrix for the context's current group - host
+ * assembly, then upload (DSAPrecon::set_group, src/dsak.kokkos.cxx:216-226:
+ * MIP at DG1, dsa_plexk.kokkos.cxx:365-475; two-point flux with the
+ * consistent-D blend at DG0, :288-348). Synchronises `stream`. */
+int ubolt_dsa_set_group(ubolt_ctx *ctx, void *stream);
+/* y = P D^{-1} R x (DSAPrecon::apply, src/dsak.kokkos.cxx:350-391), the
+ * inner solve a fixed count of FP64 block-Jacobi PCG iterations on device. */
+int ubolt_dsa_apply(ubolt_ctx *ctx, const double *x, double *y, void *stream);
+/* v = D u over the nodes (n_cells * n_basis): the diffusion SpMV. */
+int ubolt_dsa_spmv(ubolt_ctx *ctx, const double *u, double *v, void *stream);
+/* rhs(node) = V_c sum_a w_a x(node, a) (RestrictKernel, src/dsak.kokkos.cxx:20-44). */
+int ubolt_dsa_restrict(ubolt_ctx *ctx, const double *x, double *rhs, void *stream);
+/* y(node, a) = u(node) / W (ProlongKernel, src/dsak.kokkos.cxx:51-62). */
+int ubolt_dsa_prolong(ubolt_ctx *ctx, const double *u, double *y, void *stream);
+/* The assembled blocks, host array [n_cells][F + 1][nb][nb]: per cell its
+ * neighbour blocks in face-slot order (zero without a neighbour), then its
+ * own block. */
+int ubolt_dsa_matrix(ubolt_ctx *ctx, double *blocks);
+
+/* ~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~
  * The solve
  * ~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~ */
 enum { UBOLT_PC_NONE = 0, UBOLT_PC_BLOCK = 1, UBOLT_PC_SWEEP = 2, UBOLT_PC_SWEEP_DSA = 3 };

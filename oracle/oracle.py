@@ -182,3 +182,45 @@ def fd2d(nx, ny, quad, sigma_t, side_bc=(0, 0, 0, 0), lx=1.0, ly=1.0):
 
 def threads():
     return _lib.oracle_threads()
+
+
+_sig("oracle_dsa_mip", C.c_int64, C.c_int, C.c_int, C.c_int64, dp, i64p, i32p, dp, dp, dp, dp, dp, dp, dp, dp,
+     C.c_double, i64p, i64p, dp)
+_sig("oracle_dsa_dg0", C.c_int64, C.c_int, C.c_int64, C.c_int, dp, i64p, i32p, dp, dp, dp, dp, C.c_double, dp, dp,
+     C.c_int, C.c_double, i64p, i64p, dp)
+_sig("oracle_dsa_restrict", None, C.c_int64, C.c_int, C.c_int, dp, dp, dp, dp)
+_sig("oracle_dsa_prolong", None, C.c_int64, C.c_int, C.c_int, C.c_double, dp, dp)
+
+
+def dsa_matrix(geometry, quad, sigma_t, sigma_s, penalty=4.0, consistent=True, power=1.5):
+    """The DSA diffusion matrix (MIP at DG1, two-point flux at DG0) as SciPy CSR."""
+    g = geometry
+    nc, F, nb = g.n_cells, g.faces_per_cell, g.n_basis
+    cap = nc * (F + 1) * nb * nb
+    ri, ci, v = np.zeros(cap, dtype=np.int64), np.zeros(cap, dtype=np.int64), np.zeros(cap)
+    st = np.ascontiguousarray(sigma_t, dtype=np.float64)
+    ss = np.ascontiguousarray(sigma_s, dtype=np.float64)
+    if nb > 1:
+        e = _lib.oracle_dsa_mip(nb, F, nc, g.face_nA, g.face_neighbour, g.face_bc, g.face_distance, g.volume,
+                                g.face_own, g.face_up, g.basis_grad, g.face_neighbour_grad, st, ss, penalty, ri, ci, v)
+    else:
+        e = _lib.oracle_dsa_dg0(F, nc, quad.n_angles, g.face_nA, g.face_neighbour, g.face_bc, g.face_distance,
+                                g.volume, quad.omega.ravel(), quad.w, quad.sum_weights, st, ss, int(consistent), power,
+                                ri, ci, v)
+    return sp.csr_matrix((v[:e], (ri[:e], ci[:e])), shape=(nc * nb, nc * nb))
+
+
+def dsa_restrict(x, geometry, quad):
+    g = geometry
+    rhs = np.empty(g.n_cells * g.n_basis)
+    _lib.oracle_dsa_restrict(g.n_cells, g.n_basis, quad.n_angles, quad.w, g.volume,
+                             np.ascontiguousarray(x, dtype=np.float64), rhs)
+    return rhs
+
+
+def dsa_prolong(u, geometry, quad):
+    g = geometry
+    y = np.empty(g.n_cells * g.n_basis * quad.n_angles)
+    _lib.oracle_dsa_prolong(g.n_cells, g.n_basis, quad.n_angles, quad.sum_weights,
+                            np.ascontiguousarray(u, dtype=np.float64), y)
+    return y

@@ -653,3 +653,165 @@ int oracle_threads(void)
    return 1;
 #endif
 }
+
+/* ~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~
+ * DSA diffusion operators (DSAPlex, src/dsa_plexk.kokkos.cxx), no voids:
+ * D = 1/(3 sigma_t), sigma_a = sigma_t - sigma_s, VOLUME-weighted rows.
+ * Output as COO (row, col, val) with the reference's entry order per row.
+ * ~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~ */
+
+/* The MIP interior-penalty form at DG1 (assemble_dg1, :365-475); penalty C.
+ * Returns the number of entries written. */
+int64_t oracle_dsa_mip(int nb, int F, int64_t n_cells, const double *face_nA, const int64_t *face_nbr,
+                       const int32_t *face_bc, const double *face_distance, const double *volume,
+                       const double *face_own, const double *face_up, const double *basis_grad,
+                       const double *face_nb_grad, const double *sigma_t, const double *sigma_s, double penalty,
+                       int64_t *ri, int64_t *ci, double *v)
+{
+   int64_t e = 0;
+   for (int64_t c = 0; c < n_cells; c++) {
+      const double vol = volume[c];
+      const double d_c = 1.0 / (3.0 * sigma_t[c]);
+      const double sigma_a = sigma_t[c] - sigma_s[c];
+      double own[MAXB][MAXB];
+      for (int i = 0; i < nb; i++)
+         for (int j = 0; j < nb; j++) {
+            double gd = 0.0;
+            for (int d = 0; d < 3; d++) gd += basis_grad[(c * nb + i) * 3 + d] * basis_grad[(c * nb + j) * 3 + d];
+            own[i][j] = vol * (d_c * gd + (i == j ? sigma_a : 0.0));
+         }
+      for (int k = 0; k < F; k++) {
+         const int64_t kf = c * F + k;
+         const int interior = face_nbr[kf] >= 0;
+         if (!interior && face_bc[kf] != BC_VACUUM) continue;
+         double area = 0.0, nrm[3];
+         for (int d = 0; d < 3; d++) area += face_nA[3 * kf + d] * face_nA[3 * kf + d];
+         area = sqrt(area);
+         for (int d = 0; d < 3; d++) nrm[d] = face_nA[3 * kf + d] / area;
+         const double scale = vol * area;
+         const double *fo = face_own + kf * nb * nb, *fu = face_up + kf * nb * nb;
+         double gc[MAXB], gn[MAXB];
+         for (int j = 0; j < nb; j++) {
+            gc[j] = 0.0;
+            gn[j] = 0.0;
+            for (int d = 0; d < 3; d++) {
+               gc[j] += basis_grad[(c * nb + j) * 3 + d] * nrm[d];
+               gn[j] += face_nb_grad[(kf * nb + j) * 3 + d] * nrm[d];
+            }
+         }
+         const double h_c = 2.0 * face_distance[2 * kf];
+         if (interior) {
+            const int64_t n = face_nbr[kf];
+            const double d_n = 1.0 / (3.0 * sigma_t[n]);
+            const double h_n = 2.0 * face_distance[2 * kf + 1];
+            double kappa = 0.5 * penalty * (d_c / h_c + d_n / h_n);
+            if (kappa < 0.25) kappa = 0.25;
+            for (int i = 0; i < nb; i++) {
+               const double m_i = scale * fo[i * nb];
+               for (int j = 0; j < nb; j++) {
+                  own[i][j] += kappa * scale * fo[i * nb + j] - 0.5 * d_c * gc[j] * m_i - 0.5 * d_c * gc[i] * scale * fo[j];
+                  ri[e] = c * nb + i;
+                  ci[e] = n * nb + j;
+                  v[e++] = -kappa * scale * fu[i * nb + j] - 0.5 * d_n * gn[j] * m_i + 0.5 * d_c * gc[i] * scale * fu[j];
+               }
+            }
+         } else {
+            double kappa = penalty * d_c / h_c;
+            if (kappa < 0.25) kappa = 0.25;
+            for (int i = 0; i < nb; i++) {
+               const double m_i = scale * fo[i * nb];
+               for (int j = 0; j < nb; j++)
+                  own[i][j] += kappa * scale * fo[i * nb + j] - 0.5 * d_c * gc[j] * m_i - 0.5 * d_c * gc[i] * scale * fo[j];
+            }
+         }
+      }
+      for (int i = 0; i < nb; i++)
+         for (int j = 0; j < nb; j++) {
+            ri[e] = c * nb + i;
+            ci[e] = c * nb + j;
+            v[e++] = own[i][j];
+         }
+   }
+   return e;
+}
+
+/* The half-range current of an isotropic unit flux through a face,
+ * sum_{Omega . n > 0} w (Omega . n) / W (HalfRangeCurrent, dsa_operatork.hpp:110-118) */
+static double half_range(int A, const double *omega, const double *w, double sum_weights, const double *nA, int64_t k,
+                         double area)
+{
+   double s = 0.0;
+   for (int a = 0; a < A; a++) {
+      double dot = 0.0;
+      for (int d = 0; d < 3; d++) dot += omega[3 * a + d] * nA[3 * k + d];
+      dot /= area;
+      if (dot > 0.0) s += w[a] * dot;
+   }
+   return s / sum_weights;
+}
+
+static double blend_d(double d, double m, double p)
+{
+   if (p == 1.0) return d + m;
+   return pow(pow(d, p) + pow(m, p), 1.0 / p);
+}
+
+/* The DG0 two-point flux with the consistent-D blend (assemble_dg0, :288-348;
+ * BlendD, dsa_operatork.hpp:122-126); consistent = 0 switches the blend off. */
+int64_t oracle_dsa_dg0(int F, int64_t n_cells, int A, const double *face_nA, const int64_t *face_nbr,
+                       const int32_t *face_bc, const double *face_distance, const double *volume,
+                       const double *omega, const double *w, double sum_weights, const double *sigma_t,
+                       const double *sigma_s, int consistent, double power, int64_t *ri, int64_t *ci, double *v)
+{
+   int64_t e = 0;
+   for (int64_t c = 0; c < n_cells; c++) {
+      const double d_c = 1.0 / (3.0 * sigma_t[c]);
+      double diag = volume[c] * (sigma_t[c] - sigma_s[c]);
+      for (int k = 0; k < F; k++) {
+         const int64_t kf = c * F + k;
+         double area = 0.0;
+         for (int d = 0; d < 3; d++) area += face_nA[3 * kf + d] * face_nA[3 * kf + d];
+         area = sqrt(area);
+         const double hr = half_range(A, omega, w, sum_weights, face_nA, kf, area);
+         const double d_own = face_distance[2 * kf];
+         if (face_nbr[kf] >= 0) {
+            const int64_t n = face_nbr[kf];
+            const double d_n = 1.0 / (3.0 * sigma_t[n]);
+            double t_f = area / (d_own / d_c + face_distance[2 * kf + 1] / d_n);
+            if (consistent) {
+               const double len = d_own + face_distance[2 * kf + 1];
+               t_f = area / len * blend_d(t_f * len / area, hr * len, power);
+            }
+            ri[e] = c;
+            ci[e] = n;
+            v[e++] = -t_f;
+            diag += t_f;
+         } else if (face_bc[kf] == BC_VACUUM) {
+            const double d_b = consistent ? blend_d(d_c, 2.0 * d_own * hr, power) : d_c;
+            diag += area / (2.0 + d_own / d_b);
+         }
+      }
+      ri[e] = c;
+      ci[e] = c;
+      v[e++] = diag;
+   }
+   return e;
+}
+
+/* R: rhs(node) = V_c sum_a w_a x(node, a); P: y(node, a) = u(node) / W
+ * (RestrictKernel / ProlongKernel, src/dsak.kokkos.cxx:20-62, no BC rows) */
+void oracle_dsa_restrict(int64_t n_cells, int nb, int A, const double *w, const double *volume, const double *x,
+                         double *rhs)
+{
+   for (int64_t n = 0; n < n_cells * nb; n++) {
+      double s = 0.0;
+      for (int a = 0; a < A; a++) s += w[a] * x[n * A + a];
+      rhs[n] = s * volume[n / nb];
+   }
+}
+
+void oracle_dsa_prolong(int64_t n_cells, int nb, int A, double sum_weights, const double *u, double *y)
+{
+   for (int64_t n = 0; n < n_cells * nb; n++)
+      for (int a = 0; a < A; a++) y[n * A + a] = u[n] / sum_weights;
+}

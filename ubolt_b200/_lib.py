@@ -156,3 +156,18 @@ _sig("ubolt_launch_count", C.c_uint64)
 _sig("ubolt_solve_adjoint", C.c_int, vp, vp, vp, C.POINTER(SolveOptions), C.POINTER(SolveStats), vp)
 _sig("ubolt_add_response_source", C.c_int, vp, vp, vp, vp)
 _sig("ubolt_gradient", C.c_int, vp, vp, vp, vp, vp, vp)
+
+
+class DsaOptions(C.Structure):
+    _fields_ = [("penalty", C.c_double), ("consistent_power", C.c_double), ("consistent_d", C.c_int32),
+                ("inner_iterations", C.c_int32)]
+
+
+_sig("ubolt_dsa_defaults", None, C.POINTER(DsaOptions))
+_sig("ubolt_dsa_setup", C.c_int, vp, C.POINTER(DGGeometry), C.POINTER(DsaOptions))
+_sig("ubolt_dsa_set_group", C.c_int, vp, vp)
+_sig("ubolt_dsa_apply", C.c_int, vp, vp, vp, vp)
+_sig("ubolt_dsa_spmv", C.c_int, vp, vp, vp, vp)
+_sig("ubolt_dsa_restrict", C.c_int, vp, vp, vp, vp)
+_sig("ubolt_dsa_prolong", C.c_int, vp, vp, vp, vp)
+_sig("ubolt_dsa_matrix", C.c_int, vp, dp)

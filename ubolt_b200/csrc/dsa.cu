@@ -1,0 +1,546 @@
+// Diffusion synthetic acceleration, the scattering half of the preconditioner
+// (DSAPrecon, include/ubolt/dsa.hpp; src/dsak.kokkos.cxx, src/dsa_plexk.kokkos.cxx):
+//
+//    y = P D^{-1} R x,  R: rhs(node) = V_c sum_a w_a x(node, a),
+//                       P: y(node, a) = u(node) / W,
+//    D the VOLUME-weighted diffusion operator on the cell nodes,
+//    D_c = 1 / (3 sigma_t), sigma_a = sigma_t - sigma_s:
+//      DG1: the MIP interior-penalty form on the modal basis, penalty C (4),
+//           floor 1/4 (DSAPlex::assemble_dg1, dsa_plexk.kokkos.cxx:365-475);
+//      DG0: the two-point flux with the consistent-D blend
+//           (D^p + (m h)^p)^(1/p), p = 1.5 (assemble_dg0, :288-348).
+// Voids (sigma_t <= 0) are refused: none of the workloads has one, and the
+// bridge/mask policy of DSAPrecon::assemble (dsak.kokkos.cxx:233-345) is
+// not restated.
+//
+// As in the reference the matrix is refilled on the host per group (a host
+// loop) and uploaded; here into a block-ELL layout - per cell its F neighbour
+// blocks (slot order, zero where a face has no neighbour) then its own block,
+// nb x nb each - so the SpMV is one gather per face, coalesced over nodes.
+// The inner solve replaces the reference's one GAMG V-cycle (PCGAMG,
+// dsak.kokkos.cxx:197-212) with a fixed number of block-Jacobi PCG
+// iterations run entirely on the device (scalars stay in device memory, no
+// host round trip), in FP64 whatever the outer precision.
+#include "ctx.h"
+
+#include <cmath>
+#include <vector>
+
+struct ubolt_dsa {
+   int nb = 1, F = 0;
+   int64_t nc = 0, n_nodes = 0;
+   double penalty = 4.0, power = 1.5;
+   int consistent = 1, inner_its = 30;
+   bool assembled = false;
+   // Host geometry (the backend data DSAPlex::create keeps)
+   std::vector<double> area, nrm, dist, volume, fown, fup, bgrad, nbgrad, half_range;
+   std::vector<int64_t> nbr;
+   std::vector<int32_t> bc;
+   std::vector<double> h_val, h_jinv;
+   // Device
+   double *val = nullptr, *jinv = nullptr;          // [nc][F+1][nb][nb], [nc][nb][nb]
+   double *rhs = nullptr, *u = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *q = nullptr;
+   double *scal = nullptr;                         // [0] rho, [1] rho_new, [2] pq
+};
+
+namespace ubolt {
+
+// v = D u over the block-ELL rows, one thread per node
+__global__ void DsaSpmvKernel(int64_t n_nodes, int nb, int F, const int32_t *__restrict__ code,
+                              const double *__restrict__ val, const double *__restrict__ u, double *__restrict__ v,
+                              const double *__restrict__ dotw, double *dot_out)
+{
+   const int64_t node = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+   double d = 0.0;
+   if (node < n_nodes) {
+      const int64_t c = node / nb;
+      const int i = (int)(node - c * nb);
+      const double *blk = val + (c * (F + 1)) * nb * nb;
+      double s = 0.0;
+      for (int f = 0; f < F; f++) {
+         const int32_t n = code[c * F + f];
+         if (n < 0) continue;
+         for (int j = 0; j < nb; j++) s += blk[(f * nb + i) * nb + j] * u[(int64_t)n * nb + j];
+      }
+      for (int j = 0; j < nb; j++) s += blk[(F * nb + i) * nb + j] * u[c * nb + j];
+      v[node] = s;
+      if (dotw) d = dotw[node] * s;
+   }
+   if (dot_out) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
+      if ((threadIdx.x & 31) == 0 && d != 0.0) atomicAdd(dot_out, d);
+   }
+}
+
+// rhs(node) = V_c sum_a w_a (x(node, a) - ax(node, a)); ax may be NULL. Warp per node.
+template <typename T>
+__global__ void DsaRestrictKernel(int64_t n_nodes, int nb, int A, const double *__restrict__ w,
+                                  const double *__restrict__ volume, const T *__restrict__ x,
+                                  const T *__restrict__ ax, double *__restrict__ rhs)
+{
+   const int64_t node = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+   const int lane = threadIdx.x & 31;
+   if (node >= n_nodes) return;
+   double s = 0.0;
+   for (int a = lane; a < A; a += 32) {
+      double v = (double)x[node * A + a];
+      if (ax) v -= (double)ax[node * A + a];
+      s += w[a] * v;
+   }
+#pragma unroll
+   for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+   if (lane == 0) rhs[node] = s * volume[node / nb];
+}
+
+// y(node, a) (+)= u(node) / W
+template <typename T>
+__global__ void DsaProlongKernel(int64_t n_rows, int A, double inv_w, const double *__restrict__ u, T *__restrict__ y,
+                                 int add)
+{
+   const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+   if (r >= n_rows) return;
+   const double v = u[r / A] * inv_w;
+   y[r] = add ? (T)((double)y[r] + v) : (T)v;
+}
+
+// ~~~ Block-Jacobi PCG on the device, a fixed number of iterations from u = 0
+
+// r = rhs, u = 0, z = J r, p = z, scal[0] = (r, z)
+__global__ void CgStartKernel(int64_t n_nodes, int nb, const double *__restrict__ jinv, const double *__restrict__ rhs,
+                              double *__restrict__ u, double *__restrict__ r, double *__restrict__ z,
+                              double *__restrict__ p, double *scal)
+{
+   const int64_t node = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+   double d = 0.0;
+   if (node < n_nodes) {
+      const int64_t c = node / nb;
+      const int i = (int)(node - c * nb);
+      double zz = 0.0;
+      for (int j = 0; j < nb; j++) zz += jinv[(c * nb + i) * nb + j] * rhs[c * nb + j];
+      r[node] = rhs[node];
+      u[node] = 0.0;
+      z[node] = zz;
+      p[node] = zz;
+      d = rhs[node] * zz;
+   }
+#pragma unroll
+   for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
+   if ((threadIdx.x & 31) == 0 && d != 0.0) atomicAdd(&scal[0], d);
+}
+
+// alpha = rho / pq; u += alpha p; r -= alpha q
+__global__ void CgUpdateKernel(int64_t n_nodes, const double *__restrict__ p, const double *__restrict__ q,
+                               double *__restrict__ u, double *__restrict__ r, const double *scal)
+{
+   const int64_t node = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+   if (node >= n_nodes) return;
+   const double pq = scal[2];
+   const double alpha = pq != 0.0 ? scal[0] / pq : 0.0;
+   u[node] += alpha * p[node];
+   r[node] -= alpha * q[node];
+}
+
+// z = J r; scal[1] += (r, z)
+__global__ void CgPrecondKernel(int64_t n_nodes, int nb, const double *__restrict__ jinv, const double *__restrict__ r,
+                                double *__restrict__ z, double *scal)
+{
+   const int64_t node = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+   double d = 0.0;
+   if (node < n_nodes) {
+      const int64_t c = node / nb;
+      const int i = (int)(node - c * nb);
+      double zz = 0.0;
+      for (int j = 0; j < nb; j++) zz += jinv[(c * nb + i) * nb + j] * r[c * nb + j];
+      z[node] = zz;
+      d = r[node] * zz;
+   }
+#pragma unroll
+   for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
+   if ((threadIdx.x & 31) == 0 && d != 0.0) atomicAdd(&scal[1], d);
+}
+
+// beta = rho_new / rho; p = z + beta p; rho = rho_new; clear rho_new and pq (one thread does the scalars)
+__global__ void CgDirectionKernel(int64_t n_nodes, const double *__restrict__ z, double *__restrict__ p, double *scal)
+{
+   const int64_t node = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+   const double rho = scal[0], rho_new = scal[1];
+   const double beta = rho != 0.0 ? rho_new / rho : 0.0;
+   if (node < n_nodes) p[node] = z[node] + beta * p[node];
+}
+
+__global__ void CgRotateScalars(double *scal)
+{
+   scal[0] = scal[1];
+   scal[1] = 0.0;
+   scal[2] = 0.0;
+}
+
+// ~~~ Host assembly
+
+static void InvertSmall(int nb, const double *m_in, double *inv)
+{
+   double m[4][4], w[4][4];
+   for (int i = 0; i < nb; i++)
+      for (int j = 0; j < nb; j++) {
+         m[i][j] = m_in[i * nb + j];
+         w[i][j] = (i == j) ? 1.0 : 0.0;
+      }
+   for (int k = 0; k < nb; k++) {
+      int piv = k;
+      for (int i = k + 1; i < nb; i++)
+         if (std::fabs(m[i][k]) > std::fabs(m[piv][k])) piv = i;
+      if (m[piv][k] == 0.0) {
+         for (int i = 0; i < nb * nb; i++) inv[i] = 0.0;
+         return;
+      }
+      if (piv != k)
+         for (int j = 0; j < nb; j++) {
+            std::swap(m[k][j], m[piv][j]);
+            std::swap(w[k][j], w[piv][j]);
+         }
+      const double ip = 1.0 / m[k][k];
+      for (int j = 0; j < nb; j++) { m[k][j] *= ip; w[k][j] *= ip; }
+      for (int i = 0; i < nb; i++) {
+         if (i == k) continue;
+         const double f = m[i][k];
+         for (int j = 0; j < nb; j++) { m[i][j] -= f * m[k][j]; w[i][j] -= f * w[k][j]; }
+      }
+   }
+   for (int i = 0; i < nb; i++)
+      for (int j = 0; j < nb; j++) inv[i * nb + j] = w[i][j];
+}
+
+static double BlendD(double d, double m, double p)
+{
+   if (p == 1.0) return d + m;
+   return std::pow(std::pow(d, p) + std::pow(m, p), 1.0 / p);
+}
+
+// Fill the block-ELL values and the block-Jacobi inverses for one group.
+static int Assemble(ubolt_dsa *ds, const double *st, const double *ss)
+{
+   const int nb = ds->nb, F = ds->F;
+   const int64_t nc = ds->nc;
+   const size_t bs = (size_t)nb * nb;
+   ds->h_val.assign(nc * (F + 1) * bs, 0.0);
+   ds->h_jinv.assign(nc * bs, 0.0);
+   int bad = 0;
+#pragma omp parallel for schedule(static)
+   for (int64_t c = 0; c < nc; c++) {
+      if (!(st[c] > 0.0)) {
+         bad = 1;
+         continue;
+      }
+      double *blk = &ds->h_val[c * (F + 1) * bs];
+      double *own = blk + F * bs;
+      const double vol = ds->volume[c];
+      const double d_c = 1.0 / (3.0 * st[c]);
+      if (nb == 1) {
+         double diag = vol * (st[c] - ss[c]);
+         for (int f = 0; f < F; f++) {
+            const int64_t k = c * F + f;
+            const double d_own = ds->dist[2 * k];
+            if (ds->nbr[k] >= 0) {
+               const int64_t n = ds->nbr[k];
+               const double d_n = 1.0 / (3.0 * st[n]);
+               double t_f = ds->area[k] / (d_own / d_c + ds->dist[2 * k + 1] / d_n);
+               if (ds->consistent) {
+                  const double len = d_own + ds->dist[2 * k + 1];
+                  t_f = ds->area[k] / len * BlendD(t_f * len / ds->area[k], ds->half_range[k] * len, ds->power);
+               }
+               blk[f] = -t_f;
+               diag += t_f;
+            } else if (ds->bc[k] == UBOLT_BC_VACUUM) {
+               const double d_b = ds->consistent ? BlendD(d_c, 2.0 * d_own * ds->half_range[k], ds->power) : d_c;
+               diag += ds->area[k] / (2.0 + d_own / d_b);
+            }
+         }
+         own[0] = diag;
+      } else {
+         const double sigma_a = st[c] - ss[c];
+         for (int i = 0; i < nb; i++)
+            for (int j = 0; j < nb; j++) {
+               double gd = 0.0;
+               for (int d = 0; d < 3; d++) gd += ds->bgrad[(c * nb + i) * 3 + d] * ds->bgrad[(c * nb + j) * 3 + d];
+               own[i * nb + j] = vol * (d_c * gd + (i == j ? sigma_a : 0.0));
+            }
+         for (int f = 0; f < F; f++) {
+            const int64_t k = c * F + f;
+            const bool interior = ds->nbr[k] >= 0;
+            if (!interior && ds->bc[k] != UBOLT_BC_VACUUM) continue;
+            const double scale = vol * ds->area[k];
+            const double *fo = &ds->fown[k * bs], *fu = &ds->fup[k * bs];
+            double gc[4], gn[4];
+            for (int j = 0; j < nb; j++) {
+               gc[j] = gn[j] = 0.0;
+               for (int d = 0; d < 3; d++) {
+                  gc[j] += ds->bgrad[(c * nb + j) * 3 + d] * ds->nrm[3 * k + d];
+                  gn[j] += ds->nbgrad[(k * nb + j) * 3 + d] * ds->nrm[3 * k + d];
+               }
+            }
+            const double h_c = 2.0 * ds->dist[2 * k];
+            if (interior) {
+               const double d_n = 1.0 / (3.0 * st[ds->nbr[k]]);
+               const double h_n = 2.0 * ds->dist[2 * k + 1];
+               const double kappa = std::max(0.5 * ds->penalty * (d_c / h_c + d_n / h_n), 0.25);
+               double *nbb = blk + f * bs;
+               for (int i = 0; i < nb; i++) {
+                  const double m_i = scale * fo[i * nb];
+                  for (int j = 0; j < nb; j++) {
+                     own[i * nb + j] += kappa * scale * fo[i * nb + j] - 0.5 * d_c * gc[j] * m_i -
+                                        0.5 * d_c * gc[i] * scale * fo[j];
+                     nbb[i * nb + j] = -kappa * scale * fu[i * nb + j] - 0.5 * d_n * gn[j] * m_i +
+                                       0.5 * d_c * gc[i] * scale * fu[j];
+                  }
+               }
+            } else {
+               const double kappa = std::max(ds->penalty * d_c / h_c, 0.25);
+               for (int i = 0; i < nb; i++) {
+                  const double m_i = scale * fo[i * nb];
+                  for (int j = 0; j < nb; j++)
+                     own[i * nb + j] += kappa * scale * fo[i * nb + j] - 0.5 * d_c * gc[j] * m_i -
+                                        0.5 * d_c * gc[i] * scale * fo[j];
+               }
+            }
+         }
+      }
+      InvertSmall(nb, own, &ds->h_jinv[c * bs]);
+   }
+   if (bad) return SetError(UBOLT_ERR_ARG, "DSA: a cell has sigma_t <= 0 (voids are not supported)");
+   return UBOLT_OK;
+}
+
+int DsaSolveOnDevice(ubolt_ctx *ctx, cudaStream_t s)
+{
+   ubolt_dsa *ds = ctx->dsa;
+   const int64_t nn = ds->n_nodes;
+   const int bl = 256;
+   const int64_t grid = (nn + bl - 1) / bl;
+   cudaMemsetAsync(ds->scal, 0, 4 * sizeof(double), s);
+   CgStartKernel<<<grid, bl, 0, s>>>(nn, ds->nb, ds->jinv, ds->rhs, ds->u, ds->r, ds->z, ds->p, ds->scal);
+   CountLaunch();
+   for (int it = 0; it < ds->inner_its; it++) {
+      DsaSpmvKernel<<<grid, bl, 0, s>>>(nn, ds->nb, ds->F, ctx->g64.code, ds->val, ds->p, ds->q, ds->p, &ds->scal[2]);
+      CgUpdateKernel<<<grid, bl, 0, s>>>(nn, ds->p, ds->q, ds->u, ds->r, ds->scal);
+      CgPrecondKernel<<<grid, bl, 0, s>>>(nn, ds->nb, ds->jinv, ds->r, ds->z, ds->scal);
+      CgDirectionKernel<<<grid, bl, 0, s>>>(nn, ds->z, ds->p, ds->scal);
+      CgRotateScalars<<<1, 1, 0, s>>>(ds->scal);
+      CountLaunch(5);
+   }
+   return CheckLaunch("dsa solve");
+}
+
+static int CheckDsa(ubolt_ctx *ctx)
+{
+   if (!ctx->dsa) return SetError(UBOLT_ERR_STATE, "no DSA - call ubolt_dsa_setup first");
+   if (!ctx->dsa->assembled) return SetError(UBOLT_ERR_STATE, "DSA not filled for a group - call ubolt_dsa_set_group");
+   return UBOLT_OK;
+}
+
+template <typename T>
+int OperatorApply(ubolt_ctx *ctx, bool adjoint, const T *x, T *y, void *stream);
+
+// The multiplicative DSA stage after the sweep, its residual formed with the
+// operator itself (PCSetUseAmat, transport_solverk.kokkos.cxx:280-289):
+// y += P D^{-1} R (r - A y)
+template <typename T>
+int DsaCorrect(ubolt_ctx *ctx, const T *r, T *y, T *tmp, void *stream)
+{
+   int rc = CheckDsa(ctx);
+   if (rc) return rc;
+   cudaStream_t s = (cudaStream_t)stream;
+   ubolt_dsa *ds = ctx->dsa;
+   if ((rc = OperatorApply<T>(ctx, false, y, tmp, stream))) return rc;
+   const int64_t threads = ds->n_nodes * 32;
+   DsaRestrictKernel<T><<<(threads + 255) / 256, 256, 0, s>>>(ds->n_nodes, ds->nb, ctx->A, ctx->g64.w, ctx->d_volume,
+                                                              r, tmp, ds->rhs);
+   CountLaunch();
+   if ((rc = DsaSolveOnDevice(ctx, s))) return rc;
+   DsaProlongKernel<T><<<(ctx->n_rows + 255) / 256, 256, 0, s>>>(ctx->n_rows, ctx->A, 1.0 / ctx->sum_weights, ds->u,
+                                                                  y, 1);
+   return CheckLaunch("dsa correct");
+}
+template int DsaCorrect<double>(ubolt_ctx *, const double *, double *, double *, void *);
+template int DsaCorrect<float>(ubolt_ctx *, const float *, float *, float *, void *);
+
+}  // namespace ubolt
+
+using namespace ubolt;
+
+void UboltDsaFree(ubolt_ctx *ctx)
+{
+   ubolt_dsa *ds = ctx->dsa;
+   if (!ds) return;
+   for (void *p : {(void *)ds->val, (void *)ds->jinv, (void *)ds->rhs, (void *)ds->u, (void *)ds->r, (void *)ds->z,
+                   (void *)ds->p, (void *)ds->q, (void *)ds->scal})
+      if (p) cudaFree(p);
+   delete ds;
+   ctx->dsa = nullptr;
+}
+
+extern "C" void ubolt_dsa_defaults(ubolt_dsa_options *o)
+{
+   if (!o) return;
+   o->penalty = 4.0;
+   o->consistent_power = 1.5;
+   o->consistent_d = 1;
+   o->inner_iterations = 30;
+}
+
+extern "C" int ubolt_dsa_setup(ubolt_ctx *ctx, const ubolt_dg_geometry *g, const ubolt_dsa_options *opts)
+{
+   int rc = CheckReady(ctx, false);
+   if (rc) return rc;
+   if (!g) return SetError(UBOLT_ERR_ARG, "dsa_setup: NULL geometry");
+   if (g->n_cells != ctx->n_cells || g->n_basis != ctx->nb || g->faces_per_cell != ctx->F)
+      return SetError(UBOLT_ERR_ARG, "dsa_setup: the geometry is not the context's");
+   if (ctx->nb > 1 && (!g->face_own || !g->face_up || !g->basis_grad || !g->face_neighbour_grad))
+      return SetError(UBOLT_ERR_ARG, "dsa_setup: DG1 needs face matrices and basis gradients");
+   if (!g->face_distance) return SetError(UBOLT_ERR_ARG, "dsa_setup: face distances missing");
+   ubolt_dsa_options o;
+   ubolt_dsa_defaults(&o);
+   if (opts) o = *opts;
+   if (!(o.penalty > 0.0)) return SetError(UBOLT_ERR_ARG, "dsa penalty must be positive, got %g", o.penalty);
+   if (!(o.consistent_power >= 1.0)) return SetError(UBOLT_ERR_ARG, "consistent-D power must be >= 1");
+   if (o.inner_iterations < 1 || o.inner_iterations > 10000) return SetError(UBOLT_ERR_ARG, "inner iterations");
+   UboltDsaFree(ctx);
+   auto ds = new ubolt_dsa();
+   ctx->dsa = ds;
+   const int nb = ctx->nb, F = ctx->F, A = ctx->A;
+   const int64_t nc = ctx->n_cells, ns = nc * F;
+   ds->nb = nb;
+   ds->F = F;
+   ds->nc = nc;
+   ds->n_nodes = nc * nb;
+   ds->penalty = o.penalty;
+   ds->consistent = o.consistent_d;
+   ds->power = o.consistent_power;
+   ds->inner_its = o.inner_iterations;
+   ds->volume.assign(g->volume, g->volume + nc);
+   ds->nbr.assign(g->face_neighbour, g->face_neighbour + ns);
+   ds->bc.assign(g->face_bc, g->face_bc + ns);
+   ds->dist.assign(g->face_distance, g->face_distance + 2 * ns);
+   ds->area.resize(ns);
+   ds->nrm.resize(3 * ns);
+   for (int64_t k = 0; k < ns; k++) {
+      double a = 0.0;
+      for (int d = 0; d < 3; d++) a += g->face_nA[3 * k + d] * g->face_nA[3 * k + d];
+      ds->area[k] = std::sqrt(a);
+      for (int d = 0; d < 3; d++) ds->nrm[3 * k + d] = g->face_nA[3 * k + d] / ds->area[k];
+   }
+   if (nb > 1) {
+      ds->fown.assign(g->face_own, g->face_own + ns * nb * nb);
+      ds->fup.assign(g->face_up, g->face_up + ns * nb * nb);
+      ds->bgrad.assign(g->basis_grad, g->basis_grad + nc * nb * 3);
+      ds->nbgrad.assign(g->face_neighbour_grad, g->face_neighbour_grad + ns * nb * 3);
+   } else {
+      // The consistent D's half-range current per face slot, off the same ordinates
+      ds->half_range.resize(ns);
+      for (int64_t k = 0; k < ns; k++) {
+         double sum = 0.0;
+         for (int a = 0; a < A; a++) {
+            double dot = 0.0;
+            for (int d = 0; d < 3; d++) dot += ctx->h_omega[3 * a + d] * g->face_nA[3 * k + d];
+            dot /= ds->area[k];
+            if (dot > 0.0) sum += ctx->h_w[a] * dot;
+         }
+         ds->half_range[k] = sum / ctx->sum_weights;
+      }
+   }
+   auto alloc = [&](double **p, size_t n) -> int {
+      const cudaError_t e = cudaMalloc((void **)p, std::max<size_t>(n, 1) * sizeof(double));
+      if (e != cudaSuccess) {
+         cudaGetLastError();
+         return SetError(UBOLT_ERR_NOMEM, "DSA workspace: %s", cudaGetErrorString(e));
+      }
+      return UBOLT_OK;
+   };
+   const size_t bs = (size_t)nb * nb, nn = (size_t)ds->n_nodes;
+   if ((rc = alloc(&ds->val, nc * (F + 1) * bs)) || (rc = alloc(&ds->jinv, nc * bs)) || (rc = alloc(&ds->rhs, nn)) ||
+       (rc = alloc(&ds->u, nn)) || (rc = alloc(&ds->r, nn)) || (rc = alloc(&ds->z, nn)) || (rc = alloc(&ds->p, nn)) ||
+       (rc = alloc(&ds->q, nn)) || (rc = alloc(&ds->scal, 4))) {
+      UboltDsaFree(ctx);
+      return rc;
+   }
+   return UBOLT_OK;
+}
+
+extern "C" int ubolt_dsa_set_group(ubolt_ctx *ctx, void *stream)
+{
+   int rc = CheckReady(ctx, true);
+   if (rc) return rc;
+   if (!ctx->dsa) return SetError(UBOLT_ERR_STATE, "no DSA - call ubolt_dsa_setup first");
+   ubolt_dsa *ds = ctx->dsa;
+   cudaStream_t s = (cudaStream_t)stream;
+   // The assembly is a host loop (DSAHostCopy then DSAPlex::assemble in the reference)
+   std::vector<double> st(ds->nc), ss(ds->nc);
+   cudaMemcpyAsync(st.data(), ctx->g64.sigma_t, ds->nc * 8, cudaMemcpyDeviceToHost, s);
+   cudaMemcpyAsync(ss.data(), ctx->g64.sigma_s, ds->nc * 8, cudaMemcpyDeviceToHost, s);
+   if ((rc = CudaCheck(cudaStreamSynchronize(s), "dsa_set_group"))) return rc;
+   if ((rc = Assemble(ds, st.data(), ss.data()))) return rc;
+   cudaMemcpyAsync(ds->val, ds->h_val.data(), ds->h_val.size() * 8, cudaMemcpyHostToDevice, s);
+   cudaMemcpyAsync(ds->jinv, ds->h_jinv.data(), ds->h_jinv.size() * 8, cudaMemcpyHostToDevice, s);
+   if ((rc = CudaCheck(cudaStreamSynchronize(s), "dsa upload"))) return rc;
+   ds->assembled = true;
+   return UBOLT_OK;
+}
+
+extern "C" int ubolt_dsa_spmv(ubolt_ctx *ctx, const double *u, double *v, void *stream)
+{
+   int rc = CheckReady(ctx, false);
+   if (rc || (rc = CheckDsa(ctx))) return rc;
+   if (!u || !v || u == v) return SetError(UBOLT_ERR_ARG, "dsa_spmv: u and v must be distinct device arrays");
+   ubolt_dsa *ds = ctx->dsa;
+   DsaSpmvKernel<<<(ds->n_nodes + 255) / 256, 256, 0, (cudaStream_t)stream>>>(ds->n_nodes, ds->nb, ds->F,
+                                                                              ctx->g64.code, ds->val, u, v, nullptr,
+                                                                              nullptr);
+   return CheckLaunch("dsa_spmv");
+}
+
+extern "C" int ubolt_dsa_restrict(ubolt_ctx *ctx, const double *x, double *rhs, void *stream)
+{
+   int rc = CheckReady(ctx, false);
+   if (rc) return rc;
+   if (!x || !rhs) return SetError(UBOLT_ERR_ARG, "dsa_restrict: NULL array");
+   const int64_t threads = ctx->n_nodes * 32;
+   DsaRestrictKernel<double><<<(threads + 255) / 256, 256, 0, (cudaStream_t)stream>>>(
+      ctx->n_nodes, ctx->nb, ctx->A, ctx->g64.w, ctx->d_volume, x, nullptr, rhs);
+   return CheckLaunch("dsa_restrict");
+}
+
+extern "C" int ubolt_dsa_prolong(ubolt_ctx *ctx, const double *u, double *y, void *stream)
+{
+   int rc = CheckReady(ctx, false);
+   if (rc) return rc;
+   if (!u || !y) return SetError(UBOLT_ERR_ARG, "dsa_prolong: NULL array");
+   DsaProlongKernel<double><<<(ctx->n_rows + 255) / 256, 256, 0, (cudaStream_t)stream>>>(
+      ctx->n_rows, ctx->A, 1.0 / ctx->sum_weights, u, y, 0);
+   return CheckLaunch("dsa_prolong");
+}
+
+extern "C" int ubolt_dsa_apply(ubolt_ctx *ctx, const double *x, double *y, void *stream)
+{
+   int rc = CheckReady(ctx, false);
+   if (rc || (rc = CheckDsa(ctx))) return rc;
+   if (!x || !y || x == y) return SetError(UBOLT_ERR_ARG, "dsa_apply: x and y must be distinct device arrays");
+   cudaStream_t s = (cudaStream_t)stream;
+   ubolt_dsa *ds = ctx->dsa;
+   const int64_t threads = ds->n_nodes * 32;
+   DsaRestrictKernel<double><<<(threads + 255) / 256, 256, 0, s>>>(ds->n_nodes, ds->nb, ctx->A, ctx->g64.w,
+                                                                   ctx->d_volume, x, nullptr, ds->rhs);
+   CountLaunch();
+   if ((rc = DsaSolveOnDevice(ctx, s))) return rc;
+   DsaProlongKernel<double><<<(ctx->n_rows + 255) / 256, 256, 0, s>>>(ctx->n_rows, ctx->A, 1.0 / ctx->sum_weights,
+                                                                      ds->u, y, 0);
+   return CheckLaunch("dsa_apply");
+}
+
+extern "C" int ubolt_dsa_matrix(ubolt_ctx *ctx, double *blocks)
+{
+   int rc = CheckReady(ctx, false);
+   if (rc || (rc = CheckDsa(ctx))) return rc;
+   if (!blocks) return SetError(UBOLT_ERR_ARG, "dsa_matrix: NULL output");
+   std::copy(ctx->dsa->h_val.begin(), ctx->dsa->h_val.end(), blocks);
+   return UBOLT_OK;
+}

@@ -37,6 +37,11 @@ struct ubolt_solver {
    double *V = nullptr;  // (restart + 1) x n, plain form
    // FP32 workspace, mixed form: basis, preconditioned vector, rhs, spare, correction
    float *V32 = nullptr, *z32 = nullptr, *b32 = nullptr, *t32 = nullptr, *d32 = nullptr;
+   // Flexible GMRES (a preconditioner that varies, the DSA's inner PCG): the
+   // preconditioned basis, restart x n, FP64 (Z) or FP32 (Z32)
+   bool flexible = false;
+   double *Z = nullptr;
+   float *Z32 = nullptr;
    // Reductions: partial[red_blocks][restart + 2], h[3 * (restart + 2)]
    double *partial = nullptr, *h = nullptr;
    int red_blocks = 0;
@@ -236,7 +241,7 @@ struct GmresResult {
 // Right-preconditioned GMRES(m) for A x = b in storage precision S from the
 // guess in x (x_zero: it is zero). V: (m + 1) n basis, z, t: n each.
 template <typename S>
-static int Gmres(ubolt_ctx *ctx, const ubolt_solver *ws, S *V, S *z, S *t, const S *b, S *x, double bnorm,
+static int Gmres(ubolt_ctx *ctx, const ubolt_solver *ws, S *V, S *Zb, S *z, S *t, const S *b, S *x, double bnorm,
                  double rtol, int max_it, int pc, bool adjoint, bool x_zero, GmresResult *out, void *stream)
 {
    cudaStream_t s = (cudaStream_t)stream;
@@ -273,8 +278,9 @@ static int Gmres(ubolt_ctx *ctx, const ubolt_solver *ws, S *V, S *z, S *t, const
       int j = 0;
       for (; j < m && out->iterations < max_it; j++) {
          S *vj = V + (int64_t)j * n, *vn = V + (int64_t)(j + 1) * n;
-         if ((rc = Precondition<S>(ctx, pc, adjoint, vj, z, t, n, stream))) return rc;
-         if ((rc = OperatorApply<S>(ctx, adjoint, z, vn, stream))) return rc;
+         S *zj = Zb ? Zb + (int64_t)j * n : z;
+         if ((rc = Precondition<S>(ctx, pc, adjoint, vj, zj, t, n, stream))) return rc;
+         if ((rc = OperatorApply<S>(ctx, adjoint, zj, vn, stream))) return rc;
          MultiDot<S>(ws, V, j + 1, vn, n, dh1, s);
          MultiAxpyKernel<S><<<grid, 256, 0, s>>>(V, n, j + 1, dh1, -1.0, vn, 1);
          CountLaunch();
@@ -319,37 +325,51 @@ static int Gmres(ubolt_ctx *ctx, const ubolt_solver *ws, S *V, S *z, S *t, const
          y[i] = tt / H[i * m + i];
       }
       cudaMemcpyAsync(dy, y.data(), j * sizeof(double), cudaMemcpyHostToDevice, s);
-      // V_j is free scratch here: the next cycle rebuilds the basis
-      S *u = V + (int64_t)m * n;
-      MultiAxpyKernel<S><<<grid, 256, 0, s>>>(V, n, j, dy, 1.0, u, 0);
-      CountLaunch();
-      if ((rc = Precondition<S>(ctx, pc, adjoint, u, z, t, n, stream))) return rc;
-      AxpyKernel<S, S><<<grid, 256, 0, s>>>(z, x, 1.0, n);
-      CountLaunch();
+      if (Zb) {
+         // Flexible: x += Z y, the preconditioned vectors kept
+         MultiAxpyKernel<S><<<grid, 256, 0, s>>>(Zb, n, j, dy, 1.0, x, 1);
+         CountLaunch();
+      } else {
+         // V_m is free scratch here: the next cycle rebuilds the basis
+         S *u = V + (int64_t)m * n;
+         MultiAxpyKernel<S><<<grid, 256, 0, s>>>(V, n, j, dy, 1.0, u, 0);
+         CountLaunch();
+         if ((rc = Precondition<S>(ctx, pc, adjoint, u, z, t, n, stream))) return rc;
+         AxpyKernel<S, S><<<grid, 256, 0, s>>>(z, x, 1.0, n);
+         CountLaunch();
+      }
       if (out->converged) break;
    }
    return CheckLaunch("gmres");
 }
 
+static void FreeWorkspace(ubolt_ctx *ctx)
+{
+   ubolt_solver *ws = ctx->solver;
+   if (!ws) return;
+   cudaDeviceSynchronize();
+   for (void *p : {(void *)ws->r, (void *)ws->z, (void *)ws->t, (void *)ws->V, (void *)ws->V32, (void *)ws->z32,
+                   (void *)ws->b32, (void *)ws->t32, (void *)ws->d32, (void *)ws->Z, (void *)ws->Z32,
+                   (void *)ws->partial, (void *)ws->h})
+      if (p) cudaFree(p);
+   delete ws;
+   ctx->solver = nullptr;
+}
+
 static int EnsureWorkspace(ubolt_ctx *ctx, const ubolt_solve_options *o)
 {
    const bool mixed = o->precision == UBOLT_PRECISION_MIXED;
+   const bool flexible = o->pc == UBOLT_PC_SWEEP_DSA;
    const int m = o->restart > 0 ? o->restart : 30;
    ubolt_solver *ws = ctx->solver;
-   if (ws && ws->restart == m && ws->mixed == mixed) return UBOLT_OK;
+   if (ws && ws->restart == m && ws->mixed == mixed && ws->flexible == flexible) return UBOLT_OK;
    // Workspace is re-made only when its shape changes
-   if (ws) {
-      cudaDeviceSynchronize();
-      for (void *p : {(void *)ws->r, (void *)ws->z, (void *)ws->t, (void *)ws->V, (void *)ws->V32, (void *)ws->z32,
-                      (void *)ws->b32, (void *)ws->t32, (void *)ws->d32, (void *)ws->partial, (void *)ws->h})
-         if (p) cudaFree(p);
-      delete ws;
-      ctx->solver = nullptr;
-   }
+   FreeWorkspace(ctx);
    ws = new ubolt_solver();
    ws->restart = m;
    ws->n = ctx->n_rows;
    ws->mixed = mixed;
+   ws->flexible = flexible;
    ws->red_blocks = std::min(GridFor(ws->n), 1184);
    const int64_t n = ws->n;
    auto alloc = [&](void **p, size_t bytes) -> int {
@@ -370,11 +390,13 @@ static int EnsureWorkspace(ubolt_ctx *ctx, const ubolt_solve_options *o)
       return rc;
    if (!mixed) {
       if ((rc = alloc((void **)&ws->V, (size_t)(m + 1) * n * 8))) return rc;
+      if (flexible && (rc = alloc((void **)&ws->Z, (size_t)m * n * 8))) return rc;
    } else {
       if ((rc = alloc((void **)&ws->V32, (size_t)(m + 1) * n * 4)) || (rc = alloc((void **)&ws->z32, n * 4)) ||
           (rc = alloc((void **)&ws->b32, n * 4)) || (rc = alloc((void **)&ws->t32, n * 4)) ||
           (rc = alloc((void **)&ws->d32, n * 4)))
          return rc;
+      if (flexible && (rc = alloc((void **)&ws->Z32, (size_t)m * n * 4))) return rc;
    }
    return UBOLT_OK;
 }
@@ -383,16 +405,7 @@ static int EnsureWorkspace(ubolt_ctx *ctx, const ubolt_solve_options *o)
 
 using namespace ubolt;
 
-void UboltSolverFree(ubolt_ctx *ctx)
-{
-   ubolt_solver *ws = ctx->solver;
-   if (!ws) return;
-   for (void *p : {(void *)ws->r, (void *)ws->z, (void *)ws->t, (void *)ws->V, (void *)ws->V32, (void *)ws->z32,
-                   (void *)ws->b32, (void *)ws->t32, (void *)ws->d32, (void *)ws->partial, (void *)ws->h})
-      if (p) cudaFree(p);
-   delete ws;
-   ctx->solver = nullptr;
-}
+void UboltSolverFree(ubolt_ctx *ctx) { FreeWorkspace(ctx); }
 
 extern "C" void ubolt_solve_defaults(ubolt_solve_options *o)
 {
@@ -448,7 +461,7 @@ static int SolveSystem(ubolt_ctx *ctx, bool adjoint, const double *b, double *x,
       converged = true;
    } else if (o.precision == UBOLT_PRECISION_FP64) {
       GmresResult res;
-      rc = Gmres<double>(ctx, ws, ws->V, ws->z, ws->t, b, x, bnorm, o.rtol, o.max_it, o.pc, adjoint, o.x_zero != 0, &res,
+      rc = Gmres<double>(ctx, ws, ws->V, ws->Z, ws->z, ws->t, b, x, bnorm, o.rtol, o.max_it, o.pc, adjoint, o.x_zero != 0, &res,
                          stream);
       if (rc) return rc;
       st.iterations = res.iterations;
@@ -480,7 +493,7 @@ static int SolveSystem(ubolt_ctx *ctx, bool adjoint, const double *b, double *x,
          cudaMemsetAsync(ws->d32, 0, n * sizeof(float), s);
          GmresResult res;
          const double inner = std::max(o.inner_rtol, 0.5 * o.rtol * bnorm / rnorm);
-         rc = Gmres<float>(ctx, ws, ws->V32, ws->z32, ws->t32, ws->b32, ws->d32, 1.0, inner,
+         rc = Gmres<float>(ctx, ws, ws->V32, ws->Z32, ws->z32, ws->t32, ws->b32, ws->d32, 1.0, inner,
                            o.max_it - st.iterations, o.pc, adjoint, true, &res, stream);
          if (rc) return rc;
          st.iterations += res.iterations;

@@ -286,3 +286,55 @@ class DetectorResponse:
 
     def __call__(self, sigma_t, sigma_s):
         return _Response.apply(sigma_t, sigma_s, self)
+
+
+class DSAPrecon:
+    """The diffusion correction y = P D^{-1} R x (include/ubolt/dsa.hpp)."""
+
+    def __init__(self, ctx, penalty=4.0, consistent_d=True, consistent_power=1.5, inner_iterations=30):
+        self.ctx = ctx
+        o = _lib.DsaOptions()
+        lib.ubolt_dsa_defaults(C.byref(o))
+        o.penalty, o.consistent_d, o.consistent_power = penalty, int(consistent_d), consistent_power
+        o.inner_iterations = inner_iterations
+        gs = ctx.geometry.struct()
+        check(lib.ubolt_dsa_setup(ctx.handle, C.byref(gs), C.byref(o)))
+
+    def set_group(self, stream=None):
+        """Refill D for the context's current group (call after Context.set_group)."""
+        check(lib.ubolt_dsa_set_group(self.ctx.handle, _stream(stream)))
+
+    def apply(self, x, y=None, stream=None):
+        y = torch.empty_like(x) if y is None else y
+        check(lib.ubolt_dsa_apply(self.ctx.handle, _p(x), _p(y), _stream(stream)))
+        return y
+
+    def spmv(self, u, v=None, stream=None):
+        v = torch.empty_like(u) if v is None else v
+        check(lib.ubolt_dsa_spmv(self.ctx.handle, _p(u), _p(v), _stream(stream)))
+        return v
+
+    def restrict(self, x, stream=None):
+        rhs = torch.empty(self.ctx.n_nodes, dtype=torch.float64, device=x.device)
+        check(lib.ubolt_dsa_restrict(self.ctx.handle, _p(x), _p(rhs), _stream(stream)))
+        return rhs
+
+    def prolong(self, u, stream=None):
+        y = self.ctx.vector()
+        check(lib.ubolt_dsa_prolong(self.ctx.handle, _p(u), _p(y), _stream(stream)))
+        return y
+
+    def matrix(self):
+        """D as a SciPy CSR matrix over the nodes, from the assembled blocks."""
+        import scipy.sparse as sp
+        g = self.ctx.geometry
+        nc, F, nb = g.n_cells, g.faces_per_cell, g.n_basis
+        blocks = np.zeros(nc * (F + 1) * nb * nb)
+        check(lib.ubolt_dsa_matrix(self.ctx.handle, blocks.ctypes.data_as(_lib.dp)))
+        blocks = blocks.reshape(nc, F + 1, nb, nb)
+        nbr = np.concatenate([g.face_neighbour.reshape(nc, F), np.arange(nc)[:, None]], axis=1)
+        c = np.repeat(np.arange(nc), F + 1).reshape(nc, F + 1)
+        rows = (c[:, :, None, None] * nb + np.arange(nb)[None, None, :, None]).repeat(nb, axis=3)
+        cols = (nbr[:, :, None, None] * nb + np.arange(nb)[None, None, None, :]).repeat(nb, axis=2)
+        keep = np.broadcast_to((nbr >= 0)[:, :, None, None], rows.shape)
+        return sp.csr_matrix((blocks[keep], (rows[keep], cols[keep])), shape=(nc * nb, nc * nb))
