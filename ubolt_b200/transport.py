@@ -288,6 +288,53 @@ class DetectorResponse:
         return _Response.apply(sigma_t, sigma_s, self)
 
 
+def solve_groups(ctx, sigma_t, sigma_s, source, side_inflow=None, dsa=None, keep_psi=False, **solver_opts):
+    """The downscatter group sweep of the reference driver
+    (tests/transportk.kokkos.cxx:1036-1157, one forward pass - exact for
+    downscatter only, docs/architecture.md:362-364): per group g, point the
+    operator (and the DSA) at g's cross sections, build b = inflow + source
+    + sum_{g' < g} transfer(g' -> g) from the cached scalar fluxes, solve,
+    and cache phi_g.
+
+    sigma_t: (G, n_cells), sigma_s: (G, G, n_cells) [from, to], source:
+    (G, n_cells) - NumPy or device tensors. Returns (phi per group, stats per
+    group[, psi per group])."""
+    dev = ctx.device
+    as_dev = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float64, device=dev)
+    G = len(sigma_t)
+    st = [as_dev(sigma_t[g]) for g in range(G)]
+    ss = [[as_dev(sigma_s[g][h]) for h in range(G)] for g in range(G)]
+    src = [as_dev(source[g]) for g in range(G)]
+    for g in range(G):
+        for h in range(g):
+            if torch.count_nonzero(ss[g][h]).item():
+                raise _lib.UboltError(1, f"upscatter {g} -> {h}: the group sweep is downscatter only")
+    transfer = GroupTransfer(ctx, ss, src)
+    solver = TransportSolver(ctx, **solver_opts)
+    b = ctx.vector()
+    psi = ctx.vector(fill=0.0)
+    phis, stats, psis = [], [], []
+    for g in range(G):
+        ctx.set_group(st[g], ss[g][g])
+        if dsa is not None:
+            dsa.set_group()
+        b.zero_()
+        if side_inflow is not None:
+            fill_inflow(ctx, side_inflow, b)
+        transfer.add_external(g, b)
+        for h in range(g):
+            if torch.count_nonzero(ss[h][g]).item():
+                transfer.add_transfer(h, g, b)
+        psi, s = solver.solve(b, psi)
+        transfer.set_scalar_flux(g, psi)
+        transfer.phi[g] = transfer.phi[g].clone()
+        phis.append(transfer.phi[g])
+        stats.append(s)
+        if keep_psi:
+            psis.append(psi.clone())
+    return (phis, stats, psis) if keep_psi else (phis, stats)
+
+
 class DSAPrecon:
     """The diffusion correction y = P D^{-1} R x (include/ubolt/dsa.hpp)."""
 
