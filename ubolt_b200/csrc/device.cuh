@@ -146,6 +146,70 @@ __device__ __forceinline__ bool SolveBlock(T B[NB][NB], T r[NB])
    }
 }
 
+// LU factorisation with partial pivoting in place (unit lower L below the
+// diagonal, U on and above it); perm records the row swaps. False on a zero pivot.
+template <typename T, int NB>
+__device__ __forceinline__ bool LuFactor(T B[NB][NB], int perm[NB])
+{
+#pragma unroll
+   for (int k = 0; k < NB; k++) perm[k] = k;
+#pragma unroll
+   for (int k = 0; k < NB; k++) {
+      int piv = k;
+      T best = fabs(B[k][k]);
+#pragma unroll
+      for (int i = k + 1; i < NB; i++) {
+         const T v = fabs(B[i][k]);
+         if (v > best) { best = v; piv = i; }
+      }
+      if (best == T(0)) return false;
+      if (piv != k) {
+#pragma unroll
+         for (int i = k + 1; i < NB; i++)
+            if (i == piv) {
+#pragma unroll
+               for (int j = 0; j < NB; j++) { const T t = B[k][j]; B[k][j] = B[i][j]; B[i][j] = t; }
+               const int t = perm[k]; perm[k] = perm[i]; perm[i] = t;
+            }
+      }
+      const T inv = T(1) / B[k][k];
+#pragma unroll
+      for (int i = k + 1; i < NB; i++) {
+         B[i][k] *= inv;
+#pragma unroll
+         for (int j = k + 1; j < NB; j++) B[i][j] -= B[i][k] * B[k][j];
+      }
+   }
+   return true;
+}
+
+// x = B^{-1} r from LuFactor's output (r is overwritten with x)
+template <typename T, int NB>
+__device__ __forceinline__ void LuSolve(const T B[NB][NB], const int perm[NB], T r[NB])
+{
+   T y[NB];
+#pragma unroll
+   for (int i = 0; i < NB; i++) {
+      T s = T(0);
+#pragma unroll
+      for (int j = 0; j < NB; j++)
+         if (j == perm[i]) s = r[j];
+      y[i] = s;
+   }
+#pragma unroll
+   for (int i = 0; i < NB; i++)
+#pragma unroll
+      for (int j = 0; j < i; j++) y[i] -= B[i][j] * y[j];
+#pragma unroll
+   for (int i = NB - 1; i >= 0; i--) {
+#pragma unroll
+      for (int j = i + 1; j < NB; j++) y[i] -= B[i][j] * y[j];
+      y[i] /= B[i][i];
+   }
+#pragma unroll
+   for (int i = 0; i < NB; i++) r[i] = y[i];
+}
+
 template <typename T, int NB>
 __device__ __forceinline__ void Transpose(T B[NB][NB])
 {

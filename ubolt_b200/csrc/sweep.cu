@@ -11,15 +11,17 @@
 // before it. Reflective inflow couples ordinates and is lagged (read as zero),
 // as are the couplings a cycle break releases.
 //
-// Kernel: persistent, one warp per task. A warp takes the next task number,
-// waits with a bounded spin on the epoch flags of its upstream tasks, then
-// walks the task level by level with its lanes across a level's cells. An
-// upwind value solved in the same task comes from the warp's shared-memory
-// slice, one from an earlier task from L2 (ld.global.cg). Each cell's nb x nb
-// block is rebuilt from geometry and sigma_t and solved in registers. The
-// warp publishes its flag with a release store after a device-scope fence.
-// Deadlock-free: a task waits only on lower-numbered tasks, which were taken
-// by warps already running.
+// Kernel: persistent, one warp per task, tasks taken in number order. The
+// critical path of a sweep is the chain of upwind dependencies, so everything
+// off that chain is moved ahead of the wait: in a prologue the lanes build and
+// LU-factorise every cell's nb x nb block from geometry and sigma_t, and keep
+// y0 = B^{-1} q and G_f = B^{-1} s_f face_up_f (one per gathered face) in the
+// warp's shared-memory slice. Then the warp waits, with a bounded spin, on the
+// epoch flags of its upstream tasks, folds their values in once
+// (y0 -= G_f psi(up), read from L2 with ld.global.cg), and walks its levels
+// touching only shared memory: psi_c = y0 - sum G_f psi(up). It publishes its
+// flag with a release store after a device-scope fence. Deadlock-free: a task
+// waits only on lower-numbered tasks, which were taken by warps already running.
 #include "ctx.h"
 #include "sweep_plan.h"
 
@@ -29,7 +31,7 @@
 struct ubolt_sweep_plan {
    int32_t P = 0, n_patches = 0, A = 0;
    int64_t n_tasks = 0, n_lagged = 0, n_split = 0, total_levels = 0;
-   int32_t max_levels = 0;
+   int32_t max_levels = 0, max_inflow = 0;
    // Device arrays (owned by the context's allocation list)
    const int32_t *task_pa = nullptr;    // [n_tasks] patch * A + ordinate
    const int32_t *dep_ptr = nullptr;    // [n_tasks + 1]
@@ -43,6 +45,7 @@ struct ubolt_sweep_plan {
    uint32_t *ctrl = nullptr;            // [0] task counter, [1] error flag, [2] timeout count
    uint32_t epoch = 0;
    int grid = 0, warps_per_block = 4;
+   uint32_t spin_limit = 1u << 22;
 };
 
 namespace ubolt {
@@ -86,6 +89,7 @@ struct SweepDev {
    uint32_t *flags, *ctrl;
    uint32_t epoch;
    uint32_t spin_limit;
+   int32_t slots;
 };
 
 template <typename T, int NB, int F>
@@ -95,7 +99,11 @@ __global__ void __launch_bounds__(128) SweepKernel(const DevGeom<T> g, const Swe
    extern __shared__ __align__(16) unsigned char smem_raw[];
    const int lane = threadIdx.x & 31;
    const int warp = threadIdx.x >> 5;
-   T *loc = reinterpret_cast<T *>(smem_raw) + (size_t)warp * s.P * NB;
+   const int S = s.slots;  // coupling matrices kept per cell
+   // Per warp: loc[P][NB] (the right-hand side, then the solution) and
+   // G[P][S][NB][NB], G_f = B^{-1} s_f face_up_f for each gathered face
+   T *loc = reinterpret_cast<T *>(smem_raw) + (size_t)warp * s.P * (NB + S * NB * NB);
+   T *G = loc + (size_t)s.P * NB;
    const int A = s.A;
 
    for (;;) {
@@ -106,6 +114,52 @@ __global__ void __launch_bounds__(128) SweepKernel(const DevGeom<T> g, const Swe
       const int32_t pa = s.task_pa[t];
       const int32_t p = pa / A;
       const int a = pa - p * A;
+      const int64_t base = (int64_t)p * s.P;
+      const int64_t off = s.cell_ptr[t];
+      const int ncell = (int)(s.cell_ptr[t + 1] - off);
+      const T om[3] = {g.omega[3 * a], g.omega[3 * a + 1], g.omega[3 * a + 2]};
+
+      // Prologue, before the wait - nothing here depends on upstream values:
+      // every cell's block B factorised once, y0 = B^{-1} q into loc, and
+      // G_f = B^{-1} (s_f face_up_f) for every gathered face into G
+      for (int i = lane; i < ncell; i += 32) {
+         const int local = s.tcell[off + i];
+         const uint32_t mask = s.tmask[off + i];
+         const int64_t c = base + local;
+         const int32_t cl = g.cls[c];
+         T B[NB][NB];
+         int perm[NB];
+         BuildBlock<T, NB, F>(g, cl, om, g.sigma_t[c], B);
+         const bool ok = LuFactor<T, NB>(B, perm);
+         T r[NB];
+#pragma unroll
+         for (int j = 0; j < NB; j++) r[j] = ok ? q[(c * NB + j) * A + a] : T(0);
+         if (ok) LuSolve<T, NB>(B, perm, r);
+#pragma unroll
+         for (int j = 0; j < NB; j++) loc[local * NB + j] = r[j];
+         int slot = 0;
+#pragma unroll
+         for (int f = 0; f < F; f++) {
+            if (!(((mask >> f) | (mask >> (8 + f))) & 1u)) continue;
+            const T sf = Dot3(om, g.nA + ((int64_t)cl * F + f) * 3);
+            T *Gf = G + ((size_t)local * S + slot) * NB * NB;
+            if constexpr (NB == 1) {
+               Gf[0] = ok ? sf * g.inv_vol[cl] / B[0][0] : T(0);
+            } else {
+               const T *M = g.fup + ((int64_t)cl * F + f) * NB * NB;
+#pragma unroll
+               for (int j = 0; j < NB; j++) {
+                  T col[NB];
+#pragma unroll
+                  for (int ii = 0; ii < NB; ii++) col[ii] = sf * M[ii * NB + j];
+                  if (ok) LuSolve<T, NB>(B, perm, col);
+#pragma unroll
+                  for (int ii = 0; ii < NB; ii++) Gf[ii * NB + j] = ok ? col[ii] : T(0);
+               }
+            }
+            slot++;
+         }
+      }
 
       // Wait for the upstream tasks: bounded, and a timeout is reported
       for (int d = s.dep_ptr[t] + lane; d < s.dep_ptr[t + 1]; d += 32) {
@@ -123,9 +177,42 @@ __global__ void __launch_bounds__(128) SweepKernel(const DevGeom<T> g, const Swe
       __syncwarp();
       __threadfence();
 
-      const int64_t base = (int64_t)p * s.P;
-      const int64_t off = s.cell_ptr[t];
-      const T om[3] = {g.omega[3 * a], g.omega[3 * a + 1], g.omega[3 * a + 2]};
+      // Fold the upwind values from earlier tasks in: y0 -= G_f psi(up)
+      for (int i = lane; i < ncell; i += 32) {
+         const uint32_t mask = s.tmask[off + i];
+         if (!(mask >> 8)) continue;
+         const int local = s.tcell[off + i];
+         const int64_t c = base + local;
+         T y[NB];
+#pragma unroll
+         for (int j = 0; j < NB; j++) y[j] = loc[local * NB + j];
+         int slot = 0;
+#pragma unroll
+         for (int f = 0; f < F; f++) {
+            const bool here = (mask >> f) & 1u, earlier = (mask >> (8 + f)) & 1u;
+            if (!(here || earlier)) continue;
+            if (earlier) {
+               const int64_t up = g.code[c * F + f];
+               const T *Gf = G + ((size_t)local * S + slot) * NB * NB;
+               T xn[NB];
+#pragma unroll
+               for (int j = 0; j < NB; j++) xn[j] = __ldcg(&psi[(up * NB + j) * A + a]);
+#pragma unroll
+               for (int ii = 0; ii < NB; ii++) {
+                  T u = T(0);
+#pragma unroll
+                  for (int j = 0; j < NB; j++) u += Gf[ii * NB + j] * xn[j];
+                  y[ii] -= u;
+               }
+            }
+            slot++;
+         }
+#pragma unroll
+         for (int j = 0; j < NB; j++) loc[local * NB + j] = y[j];
+      }
+      __syncwarp();
+
+      // Level by level, shared memory only: psi_c = y0 - sum_{in-task f} G_f psi(up)
       int lo = 0;
       for (int l = s.lvl_ptr[t]; l < s.lvl_ptr[t + 1]; l++) {
          const int hi = s.lvl[l];
@@ -133,47 +220,33 @@ __global__ void __launch_bounds__(128) SweepKernel(const DevGeom<T> g, const Swe
             const int local = s.tcell[off + i];
             const uint32_t mask = s.tmask[off + i];
             const int64_t c = base + local;
-            const int32_t cl = g.cls[c];
-            T r[NB];
+            T y[NB];
 #pragma unroll
-            for (int j = 0; j < NB; j++) r[j] = q[(c * NB + j) * A + a];
+            for (int j = 0; j < NB; j++) y[j] = loc[local * NB + j];
+            if (mask & 0xffu) {
+               int slot = 0;
 #pragma unroll
-            for (int f = 0; f < F; f++) {
-               const bool here = (mask >> f) & 1u, earlier = (mask >> (8 + f)) & 1u;
-               if (!here && !earlier) continue;
-               const int64_t up = g.code[c * F + f];
-               const T sf = Dot3(om, g.nA + ((int64_t)cl * F + f) * 3);
-               T xn[NB];
-               if (here) {
+               for (int f = 0; f < F; f++) {
+                  const bool here = (mask >> f) & 1u, earlier = (mask >> (8 + f)) & 1u;
+                  if (!(here || earlier)) continue;
+                  if (here) {
+                     const int ul = (int)(g.code[c * F + f] - base);
+                     const T *Gf = G + ((size_t)local * S + slot) * NB * NB;
 #pragma unroll
-                  for (int j = 0; j < NB; j++) xn[j] = loc[(up - base) * NB + j];
-               } else {
+                     for (int ii = 0; ii < NB; ii++) {
+                        T u = T(0);
 #pragma unroll
-                  for (int j = 0; j < NB; j++) xn[j] = __ldcg(&psi[(up * NB + j) * A + a]);
-               }
-               if constexpr (NB == 1) {
-                  r[0] -= sf * g.inv_vol[cl] * xn[0];
-               } else {
-                  const T *M = g.fup + ((int64_t)cl * F + f) * NB * NB;
-#pragma unroll
-                  for (int ii = 0; ii < NB; ii++) {
-                     T u = T(0);
-#pragma unroll
-                     for (int j = 0; j < NB; j++) u += M[ii * NB + j] * xn[j];
-                     r[ii] -= sf * u;
+                        for (int j = 0; j < NB; j++) u += Gf[ii * NB + j] * loc[ul * NB + j];
+                        y[ii] -= u;
+                     }
                   }
+                  slot++;
                }
-            }
-            T B[NB][NB];
-            BuildBlock<T, NB, F>(g, cl, om, g.sigma_t[c], B);
-            if (!SolveBlock<T, NB>(B, r))
 #pragma unroll
-               for (int j = 0; j < NB; j++) r[j] = T(0);
-#pragma unroll
-            for (int j = 0; j < NB; j++) {
-               loc[local * NB + j] = r[j];
-               psi[(c * NB + j) * A + a] = r[j];
+               for (int j = 0; j < NB; j++) loc[local * NB + j] = y[j];
             }
+#pragma unroll
+            for (int j = 0; j < NB; j++) psi[(c * NB + j) * A + a] = y[j];
          }
          lo = hi;
          __syncwarp();
@@ -189,7 +262,7 @@ __global__ void __launch_bounds__(128) SweepKernel(const DevGeom<T> g, const Swe
 int BuildSweepPlan(ubolt_ctx *ctx, int patch_size)
 {
    const int64_t nc = ctx->n_cells;
-   int P = patch_size > 0 ? patch_size : (ctx->dim == 2 ? 128 : 64);
+   int P = patch_size > 0 ? patch_size : 64;
    if (P > 256) P = 256;
    if (P > nc) P = (int)nc;
    if (((nc + P - 1) / P) * (int64_t)ctx->A * 4 >= INT32_MAX) return SetError(UBOLT_ERR_ARG, "too many sweep tasks");
@@ -204,6 +277,7 @@ int BuildSweepPlan(ubolt_ctx *ctx, int patch_size)
    plan->n_lagged = h.n_lagged;
    plan->n_split = h.n_split;
    plan->max_levels = h.max_levels;
+   plan->max_inflow = h.max_inflow;
    plan->total_levels = (int64_t)h.lvl.size();
    int rc = 0;
    if ((rc = UploadVec(ctx, h.task_pa, &plan->task_pa)) || (rc = UploadVec(ctx, h.dep_ptr, &plan->dep_ptr)) ||
@@ -230,7 +304,8 @@ static int LaunchSweep(ubolt_ctx *ctx, const T *q, T *psi, cudaStream_t st)
 {
    ubolt_sweep_plan *pl = ctx->sweep;
    const int threads = 32 * pl->warps_per_block;
-   const size_t smem = sizeof(T) * (size_t)pl->warps_per_block * pl->P * NB;
+   const int slots = std::max(1, std::min(F - 1, (int)pl->max_inflow));
+   const size_t smem = sizeof(T) * (size_t)pl->warps_per_block * pl->P * (NB + slots * NB * NB);
    auto kern = SweepKernel<T, NB, F>;
    if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
    int per_sm = 0, n_sm = 0, dev = 0;
@@ -257,7 +332,8 @@ static int LaunchSweep(ubolt_ctx *ctx, const T *q, T *psi, cudaStream_t st)
    s.flags = pl->flags;
    s.ctrl = pl->ctrl;
    s.epoch = pl->epoch;
-   s.spin_limit = 1u << 22;
+   s.spin_limit = pl->spin_limit;
+   s.slots = slots;
    cudaMemsetAsync(pl->ctrl, 0, sizeof(uint32_t), st);  // task counter; the error flag stays sticky
    kern<<<grid, threads, smem, st>>>(ctx->geom<T>(), s, q, psi);
    return CheckLaunch("sweep");

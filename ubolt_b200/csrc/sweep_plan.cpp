@@ -199,6 +199,9 @@ void BuildHostSweepPlan(int64_t nc, int F, int A, int P, const double *om, const
       plan.lvl_ptr[i + 1] = (int32_t)plan.lvl.size();
       plan.max_levels = std::max<int32_t>(plan.max_levels, (int32_t)T.lvl.size());
    }
+   plan.max_inflow = 0;
+   for (const uint16_t m : plan.tmask)
+      plan.max_inflow = std::max(plan.max_inflow, __builtin_popcount((unsigned)(m & 0xff) | (unsigned)(m >> 8)));
    plan.n_lagged = 0;
    plan.n_split = 0;
    for (int a = 0; a < A; a++) {
@@ -224,7 +227,7 @@ extern "C" int ubolt_sweep_plan_build(const ubolt_dg_geometry *g, const ubolt_qu
    const int64_t nc = g->n_cells;
    if (patch_size < 0 || patch_size > 256) return SetError(UBOLT_ERR_ARG, "patch size %d (0..256)", patch_size);
    if (F > 8) return SetError(UBOLT_ERR_ARG, "at most 8 faces per cell");
-   int P = patch_size > 0 ? patch_size : (g->dim == 2 ? 128 : 64);
+   int P = patch_size > 0 ? patch_size : 64;
    if (P > nc) P = (int)nc;
    std::vector<int32_t> code(nc * F);
    for (int64_t k = 0; k < nc * F; k++)

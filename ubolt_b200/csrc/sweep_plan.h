@@ -12,6 +12,7 @@ struct HostSweepPlan {
    int32_t P = 0, n_patches = 0, A = 0;
    int64_t n_tasks = 0, n_lagged = 0, n_split = 0;
    int32_t max_levels = 0;
+   int32_t max_inflow = 0;          // most gathered upwind faces of one (cell, ordinate)
    std::vector<int32_t> task_pa;    // [n_tasks]
    std::vector<int32_t> dep_ptr;    // [n_tasks + 1]
    std::vector<int32_t> deps;       // upstream task ids, all < t
