@@ -244,6 +244,13 @@ int ubolt_sweep_f32(ubolt_ctx *ctx, const float *q, float *psi, void *stream);
 /* Plan statistics and the sticky timeout flag (synchronises `stream`):
  * returns UBOLT_ERR_TIMEOUT, and clears the flag, if a wait gave up. */
 int ubolt_sweep_status(ubolt_ctx *ctx, ubolt_sweep_info *info, void *stream);
+/* Failure-path check of the sweep's bounded waits (no reference
+ * counterpart): set the wait limit in polls (default 2^22), and with
+ * make_one_wait_unmet make one task of the NEXT sweep wait for a flag no task
+ * publishes, so that wait runs out: that sweep completes, its result is
+ * invalid, ubolt_sweep_status reports UBOLT_ERR_TIMEOUT, and later sweeps
+ * are normal again. */
+int ubolt_sweep_test_wait(ubolt_ctx *ctx, uint32_t spin_limit, int make_one_wait_unmet);
 
 /* The plan on the host alone, for inspection. Tasks are numbered in launch
  * order; task t solves cells of patch p for ordinate a, task_pa[t] = p * A + a,

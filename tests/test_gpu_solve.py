@@ -193,3 +193,26 @@ def test_multigroup_downscatter_sweep_matches_oracle():
         got = phis[gg].cpu().numpy()
         assert np.linalg.norm(got - phi_ref[gg]) <= 1e-10 * np.linalg.norm(phi_ref[gg]), gg
     ctx.close()
+
+
+def test_sweep_wait_that_runs_out_is_reported_and_recovers():
+    """A sweep whose one wait can never be met (a flag nothing sets) with a
+    short limit: the sweep still completes, the host reads UBOLT_ERR_TIMEOUT,
+    and the next sweep on the same context is exact again."""
+    from ubolt_b200 import _lib
+    mesh, g, q, st, ss = build(CASES[0])
+    ctx, keep = ctx_for(g, q, st, ss)
+    sw = T.Sweep(ctx, 16)
+    op = O.Operator(g, q, st, ss)
+    qv = np.random.default_rng(1).standard_normal(op.n)
+    _lib.check(_lib.lib.ubolt_sweep_test_wait(ctx.handle, 2000, 1))
+    sw.apply(dev(qv))
+    with pytest.raises(_lib.UboltError) as e:
+        sw.status()
+    assert e.value.status == 6  # UBOLT_ERR_TIMEOUT
+    _lib.check(_lib.lib.ubolt_sweep_test_wait(ctx.handle, 1 << 22, 0))
+    psi = sw.apply(dev(qv)).cpu().numpy()
+    assert sw.status()["timeouts"] == 0
+    ref = op.sweep(qv)
+    assert np.abs(psi - ref).max() <= 1e-12 * np.abs(ref).max()
+    ctx.close()

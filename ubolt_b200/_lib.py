@@ -114,6 +114,7 @@ _sig("ubolt_sweep_setup", C.c_int, vp, C.c_int)
 _sig("ubolt_sweep", C.c_int, vp, vp, vp, vp)
 _sig("ubolt_sweep_f32", C.c_int, vp, vp, vp, vp)
 _sig("ubolt_sweep_status", C.c_int, vp, C.POINTER(SweepInfo), vp)
+_sig("ubolt_sweep_test_wait", C.c_int, vp, C.c_uint32, C.c_int)
 _sig("ubolt_solve_defaults", None, C.POINTER(SolveOptions))
 _sig("ubolt_solver_setup", C.c_int, vp, C.POINTER(SolveOptions))
 _sig("ubolt_solve", C.c_int, vp, vp, vp, C.POINTER(SolveOptions), C.POINTER(SolveStats), vp)

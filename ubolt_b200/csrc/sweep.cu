@@ -46,6 +46,7 @@ struct ubolt_sweep_plan {
    uint32_t epoch = 0;
    int grid = 0, warps_per_block = 4;
    uint32_t spin_limit = 1u << 22;
+   int64_t unmet_task = -1;  // ubolt_sweep_test_wait: one task waits on a flag nothing sets
 };
 
 namespace ubolt {
@@ -90,6 +91,7 @@ struct SweepDev {
    uint32_t epoch;
    uint32_t spin_limit;
    int32_t slots;
+   int64_t unmet_task;
 };
 
 template <typename T, int NB, int F>
@@ -165,7 +167,8 @@ __global__ void __launch_bounds__(128) SweepKernel(const DevGeom<T> g, const Swe
       for (int d = s.dep_ptr[t] + lane; d < s.dep_ptr[t + 1]; d += 32) {
          const uint32_t *f = &s.flags[s.deps[d]];
          uint32_t spins = 0;
-         while (LoadAcquire(f) != s.epoch) {
+         const uint32_t want = (t == s.unmet_task) ? s.epoch + 1u : s.epoch;
+         while (LoadAcquire(f) != want) {
             if (++spins > s.spin_limit || *(volatile uint32_t *)&s.ctrl[1]) {
                atomicOr(&s.ctrl[1], 1u);
                atomicAdd(&s.ctrl[2], 1u);
@@ -333,6 +336,8 @@ static int LaunchSweep(ubolt_ctx *ctx, const T *q, T *psi, cudaStream_t st)
    s.ctrl = pl->ctrl;
    s.epoch = pl->epoch;
    s.spin_limit = pl->spin_limit;
+   s.unmet_task = pl->unmet_task;
+   pl->unmet_task = -1;
    s.slots = slots;
    cudaMemsetAsync(pl->ctrl, 0, sizeof(uint32_t), st);  // task counter; the error flag stays sticky
    kern<<<grid, threads, smem, st>>>(ctx->geom<T>(), s, q, psi);
@@ -407,6 +412,27 @@ extern "C" int ubolt_sweep_status(ubolt_ctx *ctx, ubolt_sweep_info *info, void *
       cudaMemsetAsync(pl->ctrl + 1, 0, 2 * sizeof(uint32_t), s);
       cudaStreamSynchronize(s);
       return SetError(UBOLT_ERR_TIMEOUT, "a sweep wait gave up (%u timeouts); its result is not valid", h[2]);
+   }
+   return UBOLT_OK;
+}
+
+extern "C" int ubolt_sweep_test_wait(ubolt_ctx *ctx, uint32_t spin_limit, int make_one_wait_unmet)
+{
+   int rc = CheckReady(ctx, false);
+   if (rc) return rc;
+   if (!ctx->sweep && (rc = BuildSweepPlan(ctx, 0))) return rc;
+   ubolt_sweep_plan *pl = ctx->sweep;
+   if (spin_limit < 16) return SetError(UBOLT_ERR_ARG, "spin limit %u too small", spin_limit);
+   pl->spin_limit = spin_limit;
+   pl->unmet_task = -1;
+   if (make_one_wait_unmet) {
+      // The first task that has an upstream task waits for an epoch that no
+      // task of this sweep publishes
+      std::vector<int32_t> dp(pl->n_tasks + 1);
+      cudaMemcpy(dp.data(), pl->dep_ptr, dp.size() * sizeof(int32_t), cudaMemcpyDeviceToHost);
+      for (int64_t t = 0; t < pl->n_tasks; t++)
+         if (dp[t + 1] > dp[t]) { pl->unmet_task = t; break; }
+      if (pl->unmet_task < 0) return SetError(UBOLT_ERR_STATE, "no task of this plan waits on another");
    }
    return UBOLT_OK;
 }
