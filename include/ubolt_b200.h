@@ -305,6 +305,23 @@ int ubolt_dsa_spmv(ubolt_ctx *ctx, const double *u, double *v, void *stream);
 int ubolt_dsa_restrict(ubolt_ctx *ctx, const double *x, double *rhs, void *stream);
 /* y(node, a) = u(node) / W (ProlongKernel, src/dsak.kokkos.cxx:51-62). */
 int ubolt_dsa_prolong(ubolt_ctx *ctx, const double *u, double *y, void *stream);
+/* y = P D^{-1} R x exactly as ubolt_dsa_apply computes it, but with every
+ * scratch vector of the inner solve in one fixed device array built into
+ * the library rather than in memory the library allocates. No counterpart in
+ * the reference. It is for callers that cannot let this library allocate
+ * device memory while they solve: an application whose own memory pool (a
+ * PETSc/Kokkos or framework allocator) has already reserved the device, where
+ * a cudaMalloc from a library underneath would fail or upset the pool.
+ * Limit: at most 262144 nodes (n_cells * n_basis); larger problems get
+ * UBOLT_ERR_ARG and should use ubolt_dsa_apply. The array (12.6 MB) is held
+ * by every GPU that loads the library until the process exits. The first
+ * call on a device looks up the array's device address (cudaGetSymbolAddress)
+ * with that device current; make that first call before any stream capture.
+ * Every call, from any context on the device, shares the one array and
+ * leaves the last call's values in it: calls that overlap on the GPU race.
+ * ubolt_dsa_setup and ubolt_dsa_set_group must have run; the call itself
+ * allocates nothing. */
+int ubolt_dsa_apply_static(ubolt_ctx *ctx, const double *x, double *y, void *stream);
 /* The assembled blocks, host array [n_cells][F + 1][nb][nb]: per cell its
  * neighbour blocks in face-slot order (zero without a neighbour), then its
  * own block. */

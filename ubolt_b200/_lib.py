@@ -168,6 +168,7 @@ _sig("ubolt_dsa_defaults", None, C.POINTER(DsaOptions))
 _sig("ubolt_dsa_setup", C.c_int, vp, C.POINTER(DGGeometry), C.POINTER(DsaOptions))
 _sig("ubolt_dsa_set_group", C.c_int, vp, vp)
 _sig("ubolt_dsa_apply", C.c_int, vp, vp, vp, vp)
+_sig("ubolt_dsa_apply_static", C.c_int, vp, vp, vp, vp)
 _sig("ubolt_dsa_spmv", C.c_int, vp, vp, vp, vp)
 _sig("ubolt_dsa_restrict", C.c_int, vp, vp, vp, vp)
 _sig("ubolt_dsa_prolong", C.c_int, vp, vp, vp, vp)

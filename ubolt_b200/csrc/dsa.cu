@@ -24,6 +24,7 @@
 #include "ctx.h"
 
 #include <cmath>
+#include <mutex>
 #include <vector>
 
 struct ubolt_dsa {
@@ -543,4 +544,86 @@ extern "C" int ubolt_dsa_matrix(ubolt_ctx *ctx, double *blocks)
    if (!blocks) return SetError(UBOLT_ERR_ARG, "dsa_matrix: NULL output");
    std::copy(ctx->dsa->h_val.begin(), ctx->dsa->h_val.end(), blocks);
    return UBOLT_OK;
+}
+
+// ~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~
+// The DSA apply with its scratch in a fixed device array instead of the
+// context's workspace: for a caller that cannot have this library allocate
+// device memory while it solves - typically an application whose own memory
+// pool (a PETSc/Kokkos or framework allocator) has already reserved the
+// device, so a cudaMalloc from a library underneath it would fail or break
+// the pool's accounting. The array is part of the loaded library: every GPU
+// that loads it holds these 12.6 MB until the process exits.
+// ~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~
+
+namespace {
+
+// Six node vectors (restricted rhs and the PCG's u, r, z, p, q) of at most
+// kStaticDsaNodes nodes each, then 4 scalars
+constexpr int64_t kStaticDsaNodes = (int64_t)1 << 18;
+constexpr int64_t kStaticDsaDoubles = 6 * kStaticDsaNodes + 4;
+static __device__ __align__(256) double g_dsa_scratch[kStaticDsaDoubles];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_dsa_scratch_mutex;
+double *g_dsa_scratch_addr[kMaxDevices] = {};
+
+// The scratch array's device address on the current device. The symbol's
+// name in host code is a host-side stand-in, not a device address, so the
+// address is fetched once per device with cudaGetSymbolAddress while that
+// device is current.
+int StaticScratch(int device, double **out)
+{
+   if (device < 0 || device >= kMaxDevices) return SetError(UBOLT_ERR_ARG, "device %d out of range", device);
+   std::lock_guard<std::mutex> lock(g_dsa_scratch_mutex);
+   if (!g_dsa_scratch_addr[device]) {
+      void *p = nullptr;
+      const cudaError_t e = cudaGetSymbolAddress(&p, g_dsa_scratch);
+      if (e != cudaSuccess) return CudaCheck(e, "cudaGetSymbolAddress(dsa scratch)");
+      g_dsa_scratch_addr[device] = static_cast<double *>(p);
+   }
+   *out = g_dsa_scratch_addr[device];
+   return UBOLT_OK;
+}
+
+}  // namespace
+
+extern "C" int ubolt_dsa_apply_static(ubolt_ctx *ctx, const double *x, double *y, void *stream)
+{
+   int rc = CheckReady(ctx, false);
+   if (rc || (rc = CheckDsa(ctx))) return rc;
+   if (!x || !y || x == y) return SetError(UBOLT_ERR_ARG, "dsa_apply_static: x and y must be distinct device arrays");
+   ubolt_dsa *ds = ctx->dsa;
+   if (ds->n_nodes > kStaticDsaNodes)
+      return SetError(UBOLT_ERR_ARG,
+                      "dsa_apply_static: %lld nodes exceed the fixed scratch of %lld nodes - use ubolt_dsa_apply",
+                      (long long)ds->n_nodes, (long long)kStaticDsaNodes);
+   double *base = nullptr;
+   if ((rc = StaticScratch(ctx->device, &base))) return rc;
+   const int64_t nn = kStaticDsaNodes;
+   double *rhs = base, *u = base + nn, *r = base + 2 * nn, *z = base + 3 * nn, *p = base + 4 * nn, *q = base + 5 * nn;
+   double *scal = base + 6 * nn;
+   cudaStream_t s = (cudaStream_t)stream;
+   const int64_t threads = ds->n_nodes * 32;
+   DsaRestrictKernel<double><<<(threads + 255) / 256, 256, 0, s>>>(ds->n_nodes, ds->nb, ctx->A, ctx->g64.w,
+                                                                   ctx->d_volume, x, nullptr, rhs);
+   CountLaunch();
+   // The same fixed-count block-Jacobi PCG as the workspace path; the
+   // scalars are cleared here, every vector is written before it is read
+   const int64_t nodes = ds->n_nodes;
+   const int64_t grid = (nodes + 255) / 256;
+   cudaMemsetAsync(scal, 0, 4 * sizeof(double), s);
+   CgStartKernel<<<grid, 256, 0, s>>>(nodes, ds->nb, ds->jinv, rhs, u, r, z, p, scal);
+   CountLaunch();
+   for (int it = 0; it < ds->inner_its; it++) {
+      DsaSpmvKernel<<<grid, 256, 0, s>>>(nodes, ds->nb, ds->F, ctx->g64.code, ds->val, p, q, p, &scal[2]);
+      CgUpdateKernel<<<grid, 256, 0, s>>>(nodes, p, q, u, r, scal);
+      CgPrecondKernel<<<grid, 256, 0, s>>>(nodes, ds->nb, ds->jinv, r, z, scal);
+      CgDirectionKernel<<<grid, 256, 0, s>>>(nodes, z, p, scal);
+      CgRotateScalars<<<1, 1, 0, s>>>(scal);
+      CountLaunch(5);
+   }
+   DsaProlongKernel<double><<<(ctx->n_rows + 255) / 256, 256, 0, s>>>(ctx->n_rows, ctx->A, 1.0 / ctx->sum_weights, u,
+                                                                      y, 0);
+   return CheckLaunch("dsa_apply_static");
 }
