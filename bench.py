@@ -46,6 +46,8 @@ def _args():
     p.add_argument("--scale", type=float, default=1.0, help="mesh scale (1.0 = the named workload)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--quick", action="store_true", help="skip the secondary measurements")
+    p.add_argument("--profile", default="", choices=["", "apply", "apply32", "sweep", "sweep32", "adjoint"],
+                   help="run only this kernel, --warmup + --steps launches on the workload, for a profiler")
     return p.parse_args()
 
 
@@ -166,6 +168,33 @@ def cpu_baseline(args):
                       "sweep, OpenMP"}, x
 
 
+def profile_kernel(args, ctx, T, stream):
+    """--profile: one kernel alone on the workload, timed with CUDA events."""
+    import torch
+    dt = torch.float32 if args.profile.endswith("32") else torch.float64
+    g = torch.Generator(device="cuda").manual_seed(7)
+    xr = torch.rand(ctx.n_rows, dtype=torch.float64, device="cuda", generator=g).to(dt)
+    yr = torch.empty_like(xr)
+    kind = args.profile.rstrip("32")
+    if kind == "sweep":
+        sw = T.Sweep(ctx, 0)
+        fn = lambda: sw.apply(xr, yr)
+    else:
+        A = T.TransportOperator(ctx)
+        fn = (lambda: A.mult(xr, yr)) if kind == "apply" else (lambda: A.mult_transpose(xr, yr))
+    for _ in range(args.warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    print(json.dumps({"profile": args.profile, "workload": WORKLOAD, "launches": args.steps,
+                      "us_per_launch": e0.elapsed_time(e1) / args.steps * 1e3}), flush=True)
+
+
 def main():
     args = _args()
     if args.impl == "reference":
@@ -204,6 +233,10 @@ def main():
     b = ctx.vector(fill=0.0)
     T.GroupTransfer(ctx, [[ss]], [src]).add_external(0, b)
     n = ctx.n_rows
+    if args.profile:
+        profile_kernel(args, ctx, T, stream=torch.cuda.current_stream())
+        ctx.close()
+        return
     t_setup = time.perf_counter()
     solver = T.TransportSolver(ctx, rtol=1e-8, precision="fp64", pc="sweep", restart=30, max_it=500)
     setup_s = time.perf_counter() - t_setup
@@ -304,6 +337,19 @@ def main():
         extra["mixed"] = {"s_per_solve": mixed_ms / 1e3, "speedup_vs_fp64": ms / mixed_ms,
                           "iterations": stm["iterations"], "outer": stm["outer"], "residual": stm["residual"],
                           "phi_rel_err_vs_fp64": float((phim - phi64).norm() / phi64.norm())}
+        # The same FP64 solve with every basis vector held in full (no compressed form)
+        full = T.TransportSolver(ctx, rtol=1e-8, precision="fp64", pc="sweep", restart=30, max_it=500, krylov="full")
+        xf = ctx.vector(fill=0.0)
+        for _ in range(2):
+            full.solve(b, xf)
+        torch.cuda.synchronize()
+        k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        k0.record(stream)
+        for _ in range(args.steps):
+            xf, stf = full.solve(b, xf)
+        k1.record(stream)
+        torch.cuda.synchronize()
+        extra["full_basis"] = {"s_per_solve": k0.elapsed_time(k1) / args.steps / 1e3, "iterations": stf["iterations"]}
         # FP64 solve back on its own workspace
         solver = T.TransportSolver(ctx, rtol=1e-8, precision="fp64", pc="sweep", restart=30, max_it=500)
 
@@ -364,6 +410,7 @@ def main():
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, PCG64 20261203+1)",
                 "config": {"workload": WORKLOAD, "rows": n, "rtol": 1e-8, "iterations": its,
+                           "krylov": {1: "full", 2: "compressed"}.get(stats[-1]["krylov"], "?"),
                            "true_residual": res, "preconditioner": "exact upwind sweep (patch tasks)",
                            "restart": 30, "parallelism": f"replicas{world}", "setup_s": setup_s,
                            "l2": "each step (a full solve) streams >4 GB of Krylov vectors, far above the 126 MB L2"},

@@ -230,15 +230,17 @@ typedef struct {
    uint32_t pad_;
 } ubolt_sweep_info;
 
-/* Build the sweep plan: patches of patch_size consecutive cells (0 picks 128
- * in 2D, 64 in 3D; at most 256), per-ordinate upwind orders, task list. Host
+/* Build the sweep plan: patches of patch_size consecutive cells (0 picks 64;
+ * at most 256), per-ordinate upwind orders, task list. Host
  * work plus one upload; independent of the group. Called by the first sweep
  * if not before. The streaming stage of the preconditioner, in place of
  * PCAIR (src/transport_solverk.kokkos.cxx:238-260, composite index 1). */
 int ubolt_sweep_setup(ubolt_ctx *ctx, int patch_size);
 /* psi = L^{-1} q for every ordinate: exact where the per-ordinate upwind
  * graph is acyclic; reflective inflow and cycle-breaking couplings are lagged
- * to zero. Every wait is bounded; check ubolt_sweep_status. */
+ * to zero. psi is first filled with all-ones bytes on `stream` (the kernel's
+ * "not yet stored" sentinel), then every value is overwritten. Every wait is
+ * bounded; check ubolt_sweep_status. */
 int ubolt_sweep(ubolt_ctx *ctx, const double *q, double *psi, void *stream);
 int ubolt_sweep_f32(ubolt_ctx *ctx, const float *q, float *psi, void *stream);
 /* Plan statistics and the sticky timeout flag (synchronises `stream`):
@@ -246,10 +248,10 @@ int ubolt_sweep_f32(ubolt_ctx *ctx, const float *q, float *psi, void *stream);
 int ubolt_sweep_status(ubolt_ctx *ctx, ubolt_sweep_info *info, void *stream);
 /* Failure-path check of the sweep's bounded waits (no reference
  * counterpart): set the wait limit in polls (default 2^22), and with
- * make_one_wait_unmet make one task of the NEXT sweep wait for a flag no task
- * publishes, so that wait runs out: that sweep completes, its result is
- * invalid, ubolt_sweep_status reports UBOLT_ERR_TIMEOUT, and later sweeps
- * are normal again. */
+ * make_one_wait_unmet make one task of the NEXT sweep poll, for its first
+ * upwind value, a word nothing writes, so that wait runs out: that sweep
+ * completes, its result is invalid, ubolt_sweep_status reports
+ * UBOLT_ERR_TIMEOUT, and later sweeps are normal again. */
 int ubolt_sweep_test_wait(ubolt_ctx *ctx, uint32_t spin_limit, int make_one_wait_unmet);
 
 /* The plan on the host alone, for inspection. Tasks are numbered in launch
@@ -332,6 +334,14 @@ int ubolt_dsa_matrix(ubolt_ctx *ctx, double *blocks);
  * ~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~ */
 enum { UBOLT_PC_NONE = 0, UBOLT_PC_BLOCK = 1, UBOLT_PC_SWEEP = 2, UBOLT_PC_SWEEP_DSA = 3 };
 enum { UBOLT_PRECISION_FP64 = 0, UBOLT_PRECISION_MIXED = 1 };
+/* UBOLT_KRYLOV_AUTO: with the sweep preconditioner and an exact sweep (no
+ * reflective side, no lagged coupling), A M^{-1} = I - S L^{-1}, and every
+ * basis vector but the residual's own anisotropic part lies in the
+ * isotropic (scattering) subspace: the basis is kept as one n_nodes vector
+ * and a scalar per vector, with no operator apply inside the Arnoldi loop -
+ * the same iterates in exact arithmetic. Otherwise, or with
+ * UBOLT_KRYLOV_FULL, every basis vector has n_rows entries. */
+enum { UBOLT_KRYLOV_AUTO = 0, UBOLT_KRYLOV_FULL = 1, UBOLT_KRYLOV_COMPRESSED = 2 };
 
 typedef struct {
    double rtol;        /* stop at ||b - A x|| <= rtol ||b|| (true residual, FP64) */
@@ -342,13 +352,15 @@ typedef struct {
    int32_t pc;         /* UBOLT_PC_* */
    int32_t max_outer;  /* mixed: refinement steps */
    int32_t x_zero;     /* 1: start from zero, 0: from the x passed in */
+   int32_t krylov;     /* UBOLT_KRYLOV_*: how the GMRES basis is held */
+   int32_t pad_;
 } ubolt_solve_options;
 
 typedef struct {
    int32_t iterations; /* GMRES iterations (all refinement steps) */
    int32_t outer;      /* refinement steps (1 for FP64) */
    int32_t converged;
-   int32_t pad_;
+   int32_t krylov;     /* the form the basis was held in: UBOLT_KRYLOV_FULL, or 2 for the compressed form */
    double residual;    /* ||b - A x|| / ||b|| of the returned x, FP64 */
    double rnorm0;      /* ||b|| */
    double seconds;     /* host wall time of the call */

@@ -196,7 +196,7 @@ def test_multigroup_downscatter_sweep_matches_oracle():
 
 
 def test_sweep_wait_that_runs_out_is_reported_and_recovers():
-    """A sweep whose one wait can never be met (a flag nothing sets) with a
+    """A sweep whose one wait can never be met (a value nothing stores) with a
     short limit: the sweep still completes, the host reads UBOLT_ERR_TIMEOUT,
     and the next sweep on the same context is exact again."""
     from ubolt_b200 import _lib
@@ -215,4 +215,50 @@ def test_sweep_wait_that_runs_out_is_reported_and_recovers():
     assert sw.status()["timeouts"] == 0
     ref = op.sweep(qv)
     assert np.abs(psi - ref).max() <= 1e-12 * np.abs(ref).max()
+    ctx.close()
+
+
+VACUUM = [c for c in CASES if c[0].endswith("_vac") and not c[0].startswith("tet")]
+
+
+@pytest.mark.parametrize("case", VACUUM, ids=[c[0] for c in VACUUM])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_compressed_krylov_matches_full_basis(case, precision):
+    """Exact sweep, no reflective side: the compressed basis (node-space
+    vectors plus one scalar each) gives the plain form's answer, in about
+    the same iterations, for the forward and the adjoint system."""
+    mesh, g, q, st, ss = build(case)
+    rng = np.random.default_rng(11)
+    src = rng.uniform(0.0, 1.0, g.n_cells)
+    op, b, xr = oracle_solution(g, q, st, ss, src)
+    ctx, keep = ctx_for(g, q, st, ss)
+    rtol = 1e-11 if precision == "fp64" else 1e-8
+    auto = T.TransportSolver(ctx, rtol=rtol, precision=precision, pc="sweep", max_it=2000)
+    x1, s1 = auto.solve(dev(b))
+    full = T.TransportSolver(ctx, rtol=rtol, precision=precision, pc="sweep", max_it=2000, krylov="full")
+    x2, s2 = full.solve(dev(b))
+    assert s1["krylov"] == 2 and s2["krylov"] == 1
+    assert s1["converged"] and s2["converged"] and s1["residual"] <= rtol * 1.01
+    assert abs(s1["iterations"] - s2["iterations"]) <= 1 + s2["iterations"] // 10
+    phi1, phi_r = scalar_flux(x1.cpu().numpy(), g, q), scalar_flux(xr, g, q)
+    assert np.linalg.norm(phi1 - phi_r) <= 10 * rtol * np.linalg.norm(phi_r)
+    # the adjoint: anisotropic source, the weighted isotropic subspace
+    gsrc = rng.standard_normal(op.n)
+    l1, a1 = auto.solve_adjoint(dev(gsrc))
+    l2, a2 = full.solve_adjoint(dev(gsrc))
+    assert a1["krylov"] == 2 and a1["converged"] and a2["converged"]
+    lam1, lam2 = l1.cpu().numpy(), l2.cpu().numpy()
+    assert np.linalg.norm(lam1 - lam2) <= 20 * rtol * np.linalg.norm(lam2)
+    assert np.linalg.norm(op.matrix().T @ lam1 - gsrc) <= 1.01 * rtol * np.linalg.norm(gsrc)
+    ctx.close()
+
+
+def test_compressed_krylov_is_not_used_where_the_sweep_lags():
+    case = [c for c in CASES if c[0] == "tri_dg1_refl"][0]
+    mesh, g, q, st, ss = build(case)
+    src = np.random.default_rng(6).uniform(0.0, 1.0, g.n_cells)
+    op, b, xr = oracle_solution(g, q, st, ss, src)
+    ctx, keep = ctx_for(g, q, st, ss)
+    x, stats = T.TransportSolver(ctx, rtol=1e-10, pc="sweep").solve(dev(b))
+    assert stats["krylov"] == 1 and stats["converged"]
     ctx.close()

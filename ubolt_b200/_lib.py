@@ -99,11 +99,12 @@ class SweepInfo(C.Structure):
 
 class SolveOptions(C.Structure):
     _fields_ = [("rtol", C.c_double), ("inner_rtol", C.c_double), ("max_it", C.c_int32), ("restart", C.c_int32),
-                ("precision", C.c_int32), ("pc", C.c_int32), ("max_outer", C.c_int32), ("x_zero", C.c_int32)]
+                ("precision", C.c_int32), ("pc", C.c_int32), ("max_outer", C.c_int32), ("x_zero", C.c_int32),
+                ("krylov", C.c_int32), ("pad_", C.c_int32)]
 
 
 class SolveStats(C.Structure):
-    _fields_ = [("iterations", C.c_int32), ("outer", C.c_int32), ("converged", C.c_int32), ("pad_", C.c_int32),
+    _fields_ = [("iterations", C.c_int32), ("outer", C.c_int32), ("converged", C.c_int32), ("krylov", C.c_int32),
                 ("residual", C.c_double), ("rnorm0", C.c_double), ("seconds", C.c_double)]
 
 

@@ -12,11 +12,22 @@
 // Vacuum inflow slots are nulled (their value is rhs), s == 0 adds nothing.
 //
 // One block holds K whole cells, one thread per (cell, angle); a thread
-// computes all n_basis rows of its (cell, angle). The cells' angular flux is
-// staged in shared memory once: the scatter's per-node angular moment is a
-// warp-shuffle reduction over it and a reflective face reads its mirrored
-// angle from it. Upwind neighbours are gathered straight from HBM/L2; a
-// node's angles are contiguous so a warp's gather is a few full sectors.
+// computes all n_basis rows of its (cell, angle).
+//
+// Forward (L - S and L): everything a block needs besides its upwind
+// neighbours is staged in shared memory by coalesced cooperative loads
+// issued together - the cells' angular flux, their shape data (normals,
+// face matrices, gradients), face codes and cross sections - so a block
+// waits on two rounds of memory latency (class id -> shape data, face code
+// -> neighbour flux) instead of a chain of per-face loads. The upwind
+// neighbours' values are loaded into registers before the scatter's
+// per-node angular moment (a warp-shuffle reduction over the staged flux)
+// is formed, so those loads overlap it. A reflective face reads its
+// mirrored angle from the staged flux.
+//
+// Adjoint ((L - S)^T): a column also needs the NEIGHBOUR's shape data (its
+// face slot and matrix for the shared face), so that kernel gathers class
+// data straight from L1/L2.
 #include "ctx.h"
 
 namespace ubolt {
@@ -31,8 +42,186 @@ __device__ __forceinline__ T WarpSum(T v)
    return v;
 }
 
-template <typename T, int NB, int F, int MODE>
-__global__ void __launch_bounds__(512) ApplyKernel(const DevGeom<T> g, const T *__restrict__ x, T *__restrict__ y, int K)
+// Per-cell shape data as staged in shared memory: [nA F x 3][face_own
+// F x nb x nb][face_up F x nb x nb][grad phi nb x 3][1 / V], padded to 16 bytes
+template <typename T, int NB, int F>
+struct StagedShape {
+   static constexpr int nA = 0;
+   static constexpr int fown = nA + F * 3;
+   static constexpr int fup = fown + (NB > 1 ? F * NB * NB : 0);
+   static constexpr int bgrad = fup + (NB > 1 ? F * NB * NB : 0);
+   static constexpr int ivol = bgrad + (NB > 1 ? NB * 3 : 0);
+   static constexpr int raw = ivol + 1;
+   static constexpr int per16 = 16 / (int)sizeof(T);
+   static constexpr int size = (raw + per16 - 1) / per16 * per16;
+};
+
+// Two 256-thread blocks per SM at most 64 registers; the FP64 4 x 4 block
+// needs more and takes them
+template <typename T, int NB, int F>
+constexpr int ApplyMinBlocks() { return (sizeof(T) == 8 && NB == 4) ? 1 : 2; }
+
+template <typename T, int NB, int F, bool SCATTER>
+__global__ void __launch_bounds__(512, ApplyMinBlocks<T, NB, F>()) ApplyKernel(const DevGeom<T> g, const T *__restrict__ x, T *__restrict__ y, int K)
+{
+   using L = StagedShape<T, NB, F>;
+   extern __shared__ __align__(16) unsigned char smem_raw[];
+   const int A = g.A;
+   T *geo = reinterpret_cast<T *>(smem_raw);                   // [K][L::size]
+   T *xs = geo + K * L::size;                                   // [K][NB][A]
+   T *mom = xs + K * NB * A;                                    // [K][NB]
+   T *sig = mom + K * NB;                                       // [K][2]: sigma_t, sigma_s / W
+   int32_t *codes = reinterpret_cast<int32_t *>(sig + 2 * K);  // [K][F]
+   const int t = threadIdx.x;
+   const int k = t / A;
+   const int a = t - k * A;
+   const int64_t c0 = (int64_t)blockIdx.x * K;
+   const int kc = (int)min((int64_t)K, g.n_cells - c0);  // cells in this block
+   const int64_t c = c0 + k;
+   const bool live = k < kc;
+
+   // Round 1: own flux, face codes, cross sections; class ids -> shape data
+   if (live) {
+#pragma unroll
+      for (int j = 0; j < NB; j++) xs[(k * NB + j) * A + a] = x[(c * NB + j) * A + a];
+   }
+   for (int e = t; e < kc * F; e += blockDim.x) codes[e] = g.code[c0 * F + e];
+   for (int e = t; e < kc; e += blockDim.x) {
+      sig[2 * e] = g.sigma_t[c0 + e];
+      sig[2 * e + 1] = SCATTER ? g.sigma_s[c0 + e] * g.inv_sum_weights : T(0);
+   }
+   for (int e = t; e < kc * L::raw; e += blockDim.x) {
+      const int kk = e / L::raw;
+      const int r = e - kk * L::raw;
+      const int64_t cl = g.cls[c0 + kk];
+      T v;
+      if (r < L::fown) v = g.nA[cl * (F * 3) + r];
+      else if (NB > 1 && r < L::fup) v = g.fown[cl * (F * NB * NB) + (r - L::fown)];
+      else if (NB > 1 && r < L::bgrad) v = g.fup[cl * (F * NB * NB) + (r - L::fup)];
+      else if (NB > 1 && r < L::ivol) v = g.bgrad[cl * (NB * 3) + (r - L::bgrad)];
+      else v = g.inv_vol[cl];
+      geo[kk * L::size + r] = v;
+   }
+   __syncthreads();
+
+   // Round 2: the upwind neighbours of this (cell, angle), loaded together
+   // and folded in at once (inflow faces: the upwind neighbour, or the
+   // mirrored angle here), so they hold no registers past this point
+   const T *gs = geo + k * L::size;
+   T ox = T(0), oy = T(0), oz = T(0);
+   T sf[F];
+   T acc[NB];
+#pragma unroll
+   for (int i = 0; i < NB; i++) acc[i] = T(0);
+   if (live) {
+      ox = g.omega[3 * a];
+      oy = g.omega[3 * a + 1];
+      oz = g.omega[3 * a + 2];
+#pragma unroll
+      for (int f = 0; f < F; f++) sf[f] = Dot3(ox, oy, oz, gs + L::nA + 3 * f);
+      // Faces in chunks of FC: every load of a chunk is in flight at once
+      constexpr int FC = (F * NB <= 9) ? F : (F % 3 == 0 ? 3 : 2);
+#pragma unroll
+      for (int f0 = 0; f0 < F; f0 += FC) {
+      T xn[FC][NB];
+#pragma unroll
+      for (int ff = 0; ff < FC; ff++) {
+         const int32_t code = codes[k * F + f0 + ff];
+         const bool up = sf[f0 + ff] < T(0) && FaceInterior(code);
+#pragma unroll
+         for (int j = 0; j < NB; j++) xn[ff][j] = up ? x[((int64_t)code * NB + j) * A + a] : T(0);
+      }
+#pragma unroll
+      for (int ff = 0; ff < FC; ff++) {
+         const int f = f0 + ff;
+         if (!(sf[f] < T(0))) continue;
+         const int32_t code = codes[k * F + f];
+         if (!FaceInterior(code)) {
+            const int side = FaceSide(code);
+            if (g.side_bc[side] != UBOLT_BC_REFLECT) continue;
+            const int ar = g.refl[(side >> 1) * A + a];
+#pragma unroll
+            for (int j = 0; j < NB; j++) xn[ff][j] = xs[(k * NB + j) * A + ar];
+         }
+         if constexpr (NB == 1) {
+            acc[0] += sf[f] * gs[L::ivol] * xn[ff][0];
+         } else {
+            const T *M = gs + L::fup + f * NB * NB;
+#pragma unroll
+            for (int i = 0; i < NB; i++) {
+               T u = T(0);
+#pragma unroll
+               for (int j = 0; j < NB; j++) u += M[i * NB + j] * xn[ff][j];
+               acc[i] += sf[f] * u;
+            }
+         }
+      }
+      }
+   }
+   if constexpr (SCATTER) {
+      // Per node: sigma_s / W sum_b w_b x(node, b)
+      const int warp = t >> 5, lane = t & 31, n_warps = blockDim.x >> 5;
+      for (int n = warp; n < kc * NB; n += n_warps) {
+         T s = T(0);
+         for (int b = lane; b < A; b += 32) s += g.w[b] * xs[n * A + b];
+         s = WarpSum(s);
+         if (lane == 0) mom[n] = s * sig[2 * (n / NB) + 1];
+      }
+      __syncthreads();
+   }
+   if (!live) return;
+
+   // Own block: outflow faces, volume term, removal
+   if constexpr (NB == 1) {
+      T out = T(0);
+#pragma unroll
+      for (int f = 0; f < F; f++)
+         if (sf[f] > T(0)) out += sf[f];
+      acc[0] += (out * gs[L::ivol] + sig[2 * k]) * xs[k * A + a];
+   } else {
+      T B[NB][NB];
+#pragma unroll
+      for (int i = 0; i < NB; i++)
+#pragma unroll
+         for (int j = 0; j < NB; j++) B[i][j] = T(0);
+#pragma unroll
+      for (int f = 0; f < F; f++) {
+         if (sf[f] > T(0)) {
+            const T *M = gs + L::fown + f * NB * NB;
+#pragma unroll
+            for (int i = 0; i < NB; i++)
+#pragma unroll
+               for (int j = 0; j < NB; j++) B[i][j] += sf[f] * M[i * NB + j];
+         }
+      }
+#pragma unroll
+      for (int i = 1; i < NB; i++) B[i][0] -= Dot3(ox, oy, oz, gs + L::bgrad + 3 * i);
+#pragma unroll
+      for (int i = 0; i < NB; i++) B[i][i] += sig[2 * k];
+      T xo[NB];
+#pragma unroll
+      for (int j = 0; j < NB; j++) xo[j] = xs[(k * NB + j) * A + a];
+#pragma unroll
+      for (int i = 0; i < NB; i++) {
+         T u = T(0);
+#pragma unroll
+         for (int j = 0; j < NB; j++) u += B[i][j] * xo[j];
+         acc[i] += u;
+      }
+   }
+   if constexpr (SCATTER) {
+#pragma unroll
+      for (int i = 0; i < NB; i++) acc[i] -= mom[k * NB + i];
+   }
+#pragma unroll
+   for (int i = 0; i < NB; i++) y[(c * NB + i) * A + a] = acc[i];
+}
+
+// Column (c, j, a) of L - S: the own block transposed, the scatter's
+// column, and every row that reads this cell as its upwind neighbour
+template <typename T, int NB, int F>
+__global__ void __launch_bounds__(512) AdjointApplyKernel(const DevGeom<T> g, const T *__restrict__ x, T *__restrict__ y,
+                                                          int K)
 {
    extern __shared__ __align__(16) unsigned char smem_raw[];
    T *xs = reinterpret_cast<T *>(smem_raw);  // [K][NB][A]
@@ -53,14 +242,14 @@ __global__ void __launch_bounds__(512) ApplyKernel(const DevGeom<T> g, const T *
       }
    }
    __syncthreads();
-   if constexpr (MODE != kUnscattered) {
-      // Per node: sum_b w_b x(node, b) (forward) or sum_b x(node, b) (adjoint)
+   {
+      // Per node: sigma_s / W sum_b x(node, b)
       const int warp = t >> 5, lane = t & 31, n_warps = blockDim.x >> 5;
       for (int n = warp; n < K * NB; n += n_warps) {
          const int64_t cc = (int64_t)blockIdx.x * K + n / NB;
          T s = T(0);
          if (cc < g.n_cells)
-            for (int b = lane; b < A; b += 32) s += (MODE == kFull ? g.w[b] : T(1)) * xs[n * A + b];
+            for (int b = lane; b < A; b += 32) s += xs[n * A + b];
          s = WarpSum(s);
          if (lane == 0 && cc < g.n_cells) mom[n] = s * (g.sigma_s[cc] * g.inv_sum_weights);
       }
@@ -70,113 +259,62 @@ __global__ void __launch_bounds__(512) ApplyKernel(const DevGeom<T> g, const T *
 
    const int32_t cl = g.cls[c];
    const T om[3] = {g.omega[3 * a], g.omega[3 * a + 1], g.omega[3 * a + 2]};
-   const T st = g.sigma_t[c];
    T acc[NB];
-
-   if constexpr (MODE != kAdjoint) {
-      // Own block: outflow faces, volume term, removal
-      T B[NB][NB];
-      BuildBlock<T, NB, F>(g, cl, om, st, B);
+   T B[NB][NB];
+   BuildBlock<T, NB, F>(g, cl, om, g.sigma_t[c], B);
 #pragma unroll
-      for (int i = 0; i < NB; i++) {
-         T s = T(0);
+   for (int j = 0; j < NB; j++) {
+      T s = T(0);
 #pragma unroll
-         for (int j = 0; j < NB; j++) s += B[i][j] * xo[j];
-         acc[i] = s;
-      }
-      if constexpr (MODE == kFull) {
+      for (int i = 0; i < NB; i++) s += B[i][j] * xo[i];
+      acc[j] = s - g.w[a] * mom[k * NB + j];
+   }
 #pragma unroll
-         for (int i = 0; i < NB; i++) acc[i] -= mom[k * NB + i];
-      }
-      // Inflow faces: the upwind neighbour, or the mirrored angle here
-#pragma unroll
-      for (int f = 0; f < F; f++) {
-         const T s = Dot3(om, g.nA + ((int64_t)cl * F + f) * 3);
+   for (int f = 0; f < F; f++) {
+      const int32_t code = g.code[c * F + f];
+      if (FaceInterior(code)) {
+         // Row (n, i, a) couples to (c, j, a) through n's slot for this face
+         const int64_t n = code;
+         const int mf = g.mirror[c * F + f];
+         const int32_t ncl = g.cls[n];
+         const T s = Dot3(om, g.nA + ((int64_t)ncl * F + mf) * 3);
          if (!(s < T(0))) continue;
-         const int32_t code = g.code[c * F + f];
          T xn[NB];
-         if (FaceInterior(code)) {
 #pragma unroll
-            for (int j = 0; j < NB; j++) xn[j] = x[((int64_t)code * NB + j) * A + a];
+         for (int i = 0; i < NB; i++) xn[i] = x[(n * NB + i) * A + a];
+         if constexpr (NB == 1) {
+            acc[0] += s * g.inv_vol[ncl] * xn[0];
          } else {
-            const int side = FaceSide(code);
-            if (g.side_bc[side] != UBOLT_BC_REFLECT) continue;
-            const int ar = g.refl[(side >> 1) * A + a];
+            const T *M = g.fup + ((int64_t)ncl * F + mf) * NB * NB;
 #pragma unroll
-            for (int j = 0; j < NB; j++) xn[j] = xs[(k * NB + j) * A + ar];
+            for (int j = 0; j < NB; j++) {
+               T u = T(0);
+#pragma unroll
+               for (int i = 0; i < NB; i++) u += M[i * NB + j] * xn[i];
+               acc[j] += s * u;
+            }
          }
+      } else {
+         // Row (c, i, refl(a)) reads (c, j, a) through this reflective face
+         const int side = FaceSide(code);
+         if (g.side_bc[side] != UBOLT_BC_REFLECT) continue;
+         const int ar = g.refl[(side >> 1) * A + a];
+         const T orr[3] = {g.omega[3 * ar], g.omega[3 * ar + 1], g.omega[3 * ar + 2]};
+         const T s = Dot3(orr, g.nA + ((int64_t)cl * F + f) * 3);
+         if (!(s < T(0))) continue;
+         T xn[NB];
+#pragma unroll
+         for (int i = 0; i < NB; i++) xn[i] = xs[(k * NB + i) * A + ar];
          if constexpr (NB == 1) {
             acc[0] += s * g.inv_vol[cl] * xn[0];
          } else {
             const T *M = g.fup + ((int64_t)cl * F + f) * NB * NB;
 #pragma unroll
-            for (int i = 0; i < NB; i++) {
+            for (int j = 0; j < NB; j++) {
                T u = T(0);
 #pragma unroll
-               for (int j = 0; j < NB; j++) u += M[i * NB + j] * xn[j];
-               acc[i] += s * u;
-            }
-         }
-      }
-   } else {
-      // Column (c, j, a) of L - S: the own block transposed, the scatter's
-      // column, and every row that reads this cell as its upwind neighbour
-      T B[NB][NB];
-      BuildBlock<T, NB, F>(g, cl, om, st, B);
-#pragma unroll
-      for (int j = 0; j < NB; j++) {
-         T s = T(0);
-#pragma unroll
-         for (int i = 0; i < NB; i++) s += B[i][j] * xo[i];
-         acc[j] = s - g.w[a] * mom[k * NB + j];
-      }
-#pragma unroll
-      for (int f = 0; f < F; f++) {
-         const int32_t code = g.code[c * F + f];
-         if (FaceInterior(code)) {
-            // Row (n, i, a) couples to (c, j, a) through n's slot for this face
-            const int64_t n = code;
-            const int mf = g.mirror[c * F + f];
-            const int32_t ncl = g.cls[n];
-            const T s = Dot3(om, g.nA + ((int64_t)ncl * F + mf) * 3);
-            if (!(s < T(0))) continue;
-            T xn[NB];
-#pragma unroll
-            for (int i = 0; i < NB; i++) xn[i] = x[(n * NB + i) * A + a];
-            if constexpr (NB == 1) {
-               acc[0] += s * g.inv_vol[ncl] * xn[0];
-            } else {
-               const T *M = g.fup + ((int64_t)ncl * F + mf) * NB * NB;
-#pragma unroll
-               for (int j = 0; j < NB; j++) {
-                  T u = T(0);
-#pragma unroll
-                  for (int i = 0; i < NB; i++) u += M[i * NB + j] * xn[i];
-                  acc[j] += s * u;
-               }
-            }
-         } else {
-            // Row (c, i, refl(a)) reads (c, j, a) through this reflective face
-            const int side = FaceSide(code);
-            if (g.side_bc[side] != UBOLT_BC_REFLECT) continue;
-            const int ar = g.refl[(side >> 1) * A + a];
-            const T orr[3] = {g.omega[3 * ar], g.omega[3 * ar + 1], g.omega[3 * ar + 2]};
-            const T s = Dot3(orr, g.nA + ((int64_t)cl * F + f) * 3);
-            if (!(s < T(0))) continue;
-            T xn[NB];
-#pragma unroll
-            for (int i = 0; i < NB; i++) xn[i] = xs[(k * NB + i) * A + ar];
-            if constexpr (NB == 1) {
-               acc[0] += s * g.inv_vol[cl] * xn[0];
-            } else {
-               const T *M = g.fup + ((int64_t)cl * F + f) * NB * NB;
-#pragma unroll
-               for (int j = 0; j < NB; j++) {
-                  T u = T(0);
-#pragma unroll
-                  for (int i = 0; i < NB; i++) u += M[i * NB + j] * xn[i];
-                  acc[j] += s * u;
-               }
+               for (int i = 0; i < NB; i++) u += M[i * NB + j] * xn[i];
+               acc[j] += s * u;
             }
          }
       }
@@ -208,10 +346,14 @@ int LaunchApply(const ubolt_ctx *ctx, const DevGeom<T> &g, const T *x, T *y, int
    const int K = CellsPerBlock(g.A);
    const int threads = ((K * g.A + 31) / 32) * 32;
    const int64_t blocks = (g.n_cells + K - 1) / K;
-   const size_t smem = sizeof(T) * (size_t)(K * NB * g.A + K * NB);
-   if (mode == kFull) ApplyKernel<T, NB, F, kFull><<<blocks, threads, smem, s>>>(g, x, y, K);
-   else if (mode == kUnscattered) ApplyKernel<T, NB, F, kUnscattered><<<blocks, threads, smem, s>>>(g, x, y, K);
-   else ApplyKernel<T, NB, F, kAdjoint><<<blocks, threads, smem, s>>>(g, x, y, K);
+   if (mode == kAdjoint) {
+      const size_t smem = sizeof(T) * (size_t)(K * NB * g.A + K * NB);
+      AdjointApplyKernel<T, NB, F><<<blocks, threads, smem, s>>>(g, x, y, K);
+   } else {
+      const size_t smem = sizeof(T) * (size_t)K * (StagedShape<T, NB, F>::size + NB * g.A + NB + 2) + sizeof(int32_t) * K * F;
+      if (mode == kFull) ApplyKernel<T, NB, F, true><<<blocks, threads, smem, s>>>(g, x, y, K);
+      else ApplyKernel<T, NB, F, false><<<blocks, threads, smem, s>>>(g, x, y, K);
+   }
    return CheckLaunch("apply");
 }
 

@@ -49,8 +49,8 @@ __global__ void BlockCountKernel(const DevGeom<T> g, unsigned long long *n_singu
    if ((threadIdx.x & 31) == 0 && m) atomicAdd(n_singular, (unsigned long long)__popc(m));
 }
 
-// The explicit inverse by Gauss-Jordan with partial pivoting, [B | I] ->
-// [I | B^{-1}], in InvertBlocksKernel's order (block_inversek.kokkos.cxx:83-150).
+// The explicit inverse of every (cell, angle) block (InvertBlocksKernel,
+// block_inversek.kokkos.cxx:83-150); a singular block is stored as zero.
 template <typename T, int NB, int F>
 __global__ void BlockInverseKernel(const DevGeom<T> g, T *__restrict__ inv)
 {
@@ -61,46 +61,7 @@ __global__ void BlockInverseKernel(const DevGeom<T> g, T *__restrict__ inv)
    const T om[3] = {g.omega[3 * a], g.omega[3 * a + 1], g.omega[3 * a + 2]};
    T m[NB][NB], w[NB][NB];
    BuildBlock<T, NB, F>(g, g.cls[c], om, g.sigma_t[c], m);
-#pragma unroll
-   for (int i = 0; i < NB; i++)
-#pragma unroll
-      for (int j = 0; j < NB; j++) w[i][j] = (i == j) ? T(1) : T(0);
-   bool ok = true;
-#pragma unroll
-   for (int k = 0; k < NB; k++) {
-      if (!ok) break;
-      int piv = k;
-#pragma unroll
-      for (int i = k + 1; i < NB; i++)
-         if (fabs(m[i][k]) > fabs(m[piv][k])) piv = i;
-      T pv = T(0);
-#pragma unroll
-      for (int i = 0; i < NB; i++)
-         if (i == piv) pv = m[i][k];
-      if (pv == T(0)) { ok = false; break; }
-      if (piv != k) {
-#pragma unroll
-         for (int i = 0; i < NB; i++)
-            if (i == piv && i != k) {
-#pragma unroll
-               for (int j = 0; j < NB; j++) {
-                  T t = m[k][j]; m[k][j] = m[i][j]; m[i][j] = t;
-                  t = w[k][j]; w[k][j] = w[i][j]; w[i][j] = t;
-               }
-            }
-      }
-      const T inv_piv = T(1) / m[k][k];
-#pragma unroll
-      for (int j = 0; j < NB; j++) { m[k][j] *= inv_piv; w[k][j] *= inv_piv; }
-#pragma unroll
-      for (int i = 0; i < NB; i++) {
-         if (i == k) continue;
-         const T f = m[i][k];
-         if (f == T(0)) continue;
-#pragma unroll
-         for (int j = 0; j < NB; j++) { m[i][j] -= f * m[k][j]; w[i][j] -= f * w[k][j]; }
-      }
-   }
+   const bool ok = InvertBlock<T, NB>(m, w);
 #pragma unroll
    for (int i = 0; i < NB; i++)
 #pragma unroll

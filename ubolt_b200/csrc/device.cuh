@@ -57,6 +57,11 @@ __device__ __forceinline__ T Dot3(const T *__restrict__ om, const T *__restrict_
    // Omega . nA in the reference's term order (FaceFlux, plex_commonk.hpp:314-317)
    return om[0] * n[0] + om[1] * n[1] + om[2] * n[2];
 }
+template <typename T>
+__device__ __forceinline__ T Dot3(T ox, T oy, T oz, const T *__restrict__ n)
+{
+   return ox * n[0] + oy * n[1] + oz * n[2];
+}
 
 // The (cell, angle) element block of streaming + removal:
 //   B(i, j) = sum_{f: s_f > 0} s_f face_own_f(i, j) - [j == 0, i > 0] Omega . grad phi_i + sigma_t delta_ij
@@ -208,6 +213,52 @@ __device__ __forceinline__ void LuSolve(const T B[NB][NB], const int perm[NB], T
    }
 #pragma unroll
    for (int i = 0; i < NB; i++) r[i] = y[i];
+}
+
+// The explicit inverse by Gauss-Jordan with partial pivoting, [B | I] ->
+// [I | B^{-1}], in InvertBlocksKernel's order (block_inversek.kokkos.cxx:83-150).
+// B is destroyed. False on a zero pivot, with W left partial.
+template <typename T, int NB>
+__device__ __forceinline__ bool InvertBlock(T m[NB][NB], T w[NB][NB])
+{
+#pragma unroll
+   for (int i = 0; i < NB; i++)
+#pragma unroll
+      for (int j = 0; j < NB; j++) w[i][j] = (i == j) ? T(1) : T(0);
+#pragma unroll
+   for (int k = 0; k < NB; k++) {
+      int piv = k;
+      T best = fabs(m[k][k]);
+#pragma unroll
+      for (int i = k + 1; i < NB; i++) {
+         const T v = fabs(m[i][k]);
+         if (v > best) { best = v; piv = i; }
+      }
+      if (best == T(0)) return false;
+      if (piv != k) {
+#pragma unroll
+         for (int i = 0; i < NB; i++)
+            if (i == piv && i != k) {
+#pragma unroll
+               for (int j = 0; j < NB; j++) {
+                  T t = m[k][j]; m[k][j] = m[i][j]; m[i][j] = t;
+                  t = w[k][j]; w[k][j] = w[i][j]; w[i][j] = t;
+               }
+            }
+      }
+      const T inv_piv = T(1) / m[k][k];
+#pragma unroll
+      for (int j = 0; j < NB; j++) { m[k][j] *= inv_piv; w[k][j] *= inv_piv; }
+#pragma unroll
+      for (int i = 0; i < NB; i++) {
+         if (i == k) continue;
+         const T f = m[i][k];
+         if (f == T(0)) continue;
+#pragma unroll
+         for (int j = 0; j < NB; j++) { m[i][j] -= f * m[k][j]; w[i][j] -= f * w[k][j]; }
+      }
+   }
+   return true;
 }
 
 template <typename T, int NB>

@@ -26,6 +26,7 @@ template <typename T>
 int BlockApply(ubolt_ctx *ctx, const T *x, T *y, bool trans, void *stream);
 template <typename T>
 int DsaCorrect(ubolt_ctx *ctx, const T *r, T *y, T *tmp, void *stream);
+bool SweepIsExact(ubolt_ctx *ctx);
 }  // namespace ubolt
 
 struct ubolt_solver {
@@ -45,6 +46,11 @@ struct ubolt_solver {
    // Reductions: partial[red_blocks][restart + 2], h[3 * (restart + 2)]
    double *partial = nullptr, *h = nullptr;
    int red_blocks = 0;
+   // The compressed form (sweep preconditioner, exact sweep): node-space
+   // basis (restart + 1) x n_nodes, the residual's isotropic part, a node
+   // scratch, the basis scalars alpha[restart + 2] and four reduction slots
+   int64_t n_nodes = 0;
+   double *Phi = nullptr, *rho = nullptr, *phiy = nullptr, *alpha = nullptr, *scal = nullptr;
 };
 
 namespace ubolt {
@@ -343,6 +349,247 @@ static int Gmres(ubolt_ctx *ctx, const ubolt_solver *ws, S *V, S *Zb, S *z, S *t
    return CheckLaunch("gmres");
 }
 
+// ~~~ GMRES on the sweep-preconditioned system in compressed form
+//
+// With the exact sweep as M^{-1} = L^{-1}: A M^{-1} = (L - S) L^{-1} =
+// I - S L^{-1}, and S maps every vector into Iso_u = {u_a phi(node)} - u = 1
+// for L - S (S psi = sigma_s / W sum_b w_b psi(node, b), alike for every
+// ordinate), u = w for its transpose. Split the cycle's starting residual
+// r0 = E_u rho + r_perp, rho = R_u r0 / kappa (R_u r = sum_a u_a r(., a),
+// kappa = sum_a u_a^2), so r_perp is orthogonal to Iso_u. Every Arnoldi vector
+// is then v = alpha r_perp + E_u phi, with
+//    <v_i, v_j> = alpha_i alpha_j |r_perp|^2 + kappa <phi_i, phi_j>,
+//    A M^{-1} v = v - E_u m(M^{-1} v),  m = the scattering moment,
+// so the basis is n_nodes-long phi plus one scalar each, the Arnoldi step
+// needs no operator apply, and Gram-Schmidt runs on n_nodes-long vectors.
+// In exact arithmetic these are the plain form's iterates. Used only where
+// the sweep inverts L exactly (no lagged coupling: no reflective side, no
+// cycle break); the true residual of every cycle is still b - A x.
+
+template <typename T>
+__device__ __forceinline__ T WarpSumSolver(T v)
+{
+#pragma unroll
+   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+   return v;
+}
+
+// rho(node) = R_u r0 (node) / kappa, and this block's share of |r0 - E_u rho|^2
+template <typename S>
+__global__ void __launch_bounds__(256) IsoSplitKernel(const S *__restrict__ r0, const S *__restrict__ u, int A,
+                                                      int64_t n_nodes, double inv_kappa, double *__restrict__ rho,
+                                                      double *__restrict__ partial)
+{
+   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+   double acc = 0.0;
+   for (int64_t node = (int64_t)blockIdx.x * 8 + warp; node < n_nodes; node += (int64_t)gridDim.x * 8) {
+      const S *rn = r0 + node * A;
+      double sum = 0.0;
+      for (int a = lane; a < A; a += 32) sum += (u ? (double)u[a] : 1.0) * (double)rn[a];
+      const double rh = WarpSumSolver(sum) * inv_kappa;
+      if (lane == 0) rho[node] = rh;
+      for (int a = lane; a < A; a += 32) {
+         const double d = (double)rn[a] - (u ? (double)u[a] : 1.0) * rh;
+         acc += d * d;
+      }
+   }
+   __shared__ double red[8];
+   acc = WarpSumSolver(acc);
+   if (lane == 0) red[warp] = acc;
+   __syncthreads();
+   if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int k = 0; k < 8; k++) t += red[k];
+      partial[blockIdx.x] = t;
+   }
+}
+
+// t(node, a) = alpha r0(node, a) + u_a (phi(node) - alpha rho(node)) = alpha r_perp + E_u phi
+template <typename S>
+__global__ void __launch_bounds__(256) IsoExpandKernel(const S *__restrict__ r0, const double *__restrict__ alpha_p,
+                                                       const double *__restrict__ phi, const double *__restrict__ rho,
+                                                       const S *__restrict__ u, int A, int64_t n_nodes,
+                                                       S *__restrict__ t)
+{
+   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+   const double al = *alpha_p;
+   for (int64_t node = (int64_t)blockIdx.x * 8 + warp; node < n_nodes; node += (int64_t)gridDim.x * 8) {
+      const double iso = phi[node] - al * rho[node];
+      for (int a = lane; a < A; a += 32)
+         t[node * A + a] = (S)(al * (double)r0[node * A + a] + (u ? (double)u[a] : 1.0) * iso);
+   }
+}
+
+// phi_out(node) = phi_in(node) - sigma_s(c) / W (R_w z)(node) for L - S, or
+// - sigma_s(c) / W (R_1 z)(node) for the transpose: v - S z in Iso_u terms
+template <typename S>
+__global__ void __launch_bounds__(256) IsoScatterKernel(const S *__restrict__ z, const S *__restrict__ w,
+                                                        const S *__restrict__ sigma_s, double inv_W, int nb, int A,
+                                                        int64_t n_nodes, const double *__restrict__ phi_in,
+                                                        double *__restrict__ phi_out)
+{
+   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+   for (int64_t node = (int64_t)blockIdx.x * 8 + warp; node < n_nodes; node += (int64_t)gridDim.x * 8) {
+      double sum = 0.0;
+      for (int a = lane; a < A; a += 32) sum += (w ? (double)w[a] : 1.0) * (double)z[node * A + a];
+      sum = WarpSumSolver(sum);
+      if (lane == 0) phi_out[node] = phi_in[node] - (double)sigma_s[node / nb] * inv_W * sum;
+   }
+}
+
+// h[i] = alpha[i] alpha[j1] |r_perp|^2 + kappa d[i] for i < j1 (in place over
+// d), then alpha[j1] -= sum_i h[i] alpha[i]: one Gram-Schmidt pass's scalars
+__global__ void IsoCombineKernel(double *__restrict__ d, double *__restrict__ alpha, int j1, double rp2, double kappa)
+{
+   if (threadIdx.x != 0 || blockIdx.x != 0) return;
+   const double aw = alpha[j1];
+   double upd = 0.0;
+   for (int i = 0; i < j1; i++) {
+      const double h = alpha[i] * aw * rp2 + kappa * d[i];
+      d[i] = h;
+      upd += h * alpha[i];
+   }
+   alpha[j1] = aw - upd;
+}
+
+static int IsoGrid(int64_t n_nodes)
+{
+   return (int)std::max<int64_t>(1, std::min<int64_t>((n_nodes + 7) / 8, 148 * 16));
+}
+
+template <typename S>
+static int GmresIso(ubolt_ctx *ctx, const ubolt_solver *ws, S *work, const S *b, S *x, double bnorm, double rtol,
+                    int max_it, bool adjoint, bool x_zero, GmresResult *out, void *stream)
+{
+   cudaStream_t s = (cudaStream_t)stream;
+   const int64_t n = ws->n, nn = ws->n_nodes;
+   const int m = ws->restart, A = ctx->A;
+   const int grid = GridFor(n), igrid = IsoGrid(nn);
+   const DevGeom<S> &g = ctx->geom<S>();
+   const S *u = adjoint ? g.w : nullptr;
+   const S *wgt = adjoint ? nullptr : g.w;
+   const S *sig_s = g.sigma_s;
+   double kappa = 0.0;
+   if (adjoint)
+      for (double wa : ctx->h_w) kappa += wa * wa;
+   else
+      kappa = (double)A;
+   // Full-length vectors live in the (unused) plain basis: r0, t, z, tmp
+   S *r0 = work, *t = work + n, *z = work + 2 * n, *tmp = work + 3 * n;
+   double *Phi = ws->Phi, *alpha = ws->alpha, *scal = ws->scal;
+   std::vector<double> H((size_t)(m + 1) * m, 0.0), cs(m), sn(m), gv(m + 1), y(m), h1(m + 1), h2(m + 2),
+       alpha_h(m + 2, 0.0);
+   double *dh1 = ws->h, *dh2 = ws->h + (m + 2), *dy = ws->h + 2 * (m + 2);
+   int rc = 0;
+   out->iterations = 0;
+   out->converged = false;
+   while (out->iterations < max_it) {
+      if (x_zero) {
+         rc = CudaCheck(cudaMemcpyAsync(r0, b, n * sizeof(S), cudaMemcpyDeviceToDevice, s), "gmres");
+         x_zero = false;
+      } else {
+         rc = OperatorApply<S>(ctx, adjoint, x, r0, stream);
+         ResidualKernel<S><<<grid, 256, 0, s>>>(b, r0, n);
+         CountLaunch();
+      }
+      if (rc) return rc;
+      // r0 = E_u rho + r_perp; beta^2 = |r_perp|^2 + kappa |rho|^2
+      IsoSplitKernel<S><<<igrid, 256, 0, s>>>(r0, u, A, nn, 1.0 / kappa, ws->rho, ws->partial);
+      ReducePartialKernel<<<1, 256, 0, s>>>(ws->partial, igrid, 1, scal);
+      CountLaunch(2);
+      MultiDot<double>(ws, ws->rho, 1, ws->rho, nn, scal + 1, s);
+      double sc[2] = {0.0, 0.0};
+      cudaMemcpyAsync(sc, scal, sizeof sc, cudaMemcpyDeviceToHost, s);
+      if ((rc = CudaCheck(cudaStreamSynchronize(s), "gmres"))) return rc;
+      const double rp2 = sc[0];
+      const double beta = std::sqrt(rp2 + kappa * sc[1]);
+      if (!std::isfinite(beta)) return SetError(UBOLT_ERR_NONFINITE, "GMRES residual is not finite");
+      out->estimate = bnorm > 0 ? beta / bnorm : 0.0;
+      if (beta <= rtol * bnorm || beta == 0.0) {
+         out->converged = true;
+         break;
+      }
+      // v_0 = r0 / beta: alpha_0 = 1 / beta, phi_0 = rho / beta
+      alpha_h[0] = 1.0 / beta;
+      cudaMemcpyAsync(alpha, alpha_h.data(), sizeof(double), cudaMemcpyHostToDevice, s);
+      ScaleKernel<double, double><<<igrid, 256, 0, s>>>(ws->rho, Phi, 1.0 / beta, nn);
+      CountLaunch();
+      std::fill(gv.begin(), gv.end(), 0.0);
+      gv[0] = beta;
+      int j = 0;
+      for (; j < m && out->iterations < max_it; j++) {
+         double *pj = Phi + (int64_t)j * nn, *pn = Phi + (int64_t)(j + 1) * nn;
+         // w = v_j - E_u m(M^{-1} v_j): alpha_w = alpha_j, phi_w = phi_j - m
+         IsoExpandKernel<S><<<igrid, 256, 0, s>>>(r0, alpha + j, pj, ws->rho, u, A, nn, t);
+         CountLaunch();
+         if ((rc = Precondition<S>(ctx, UBOLT_PC_SWEEP, adjoint, t, z, tmp, n, stream))) return rc;
+         IsoScatterKernel<S><<<igrid, 256, 0, s>>>(z, wgt, sig_s, 1.0 / ctx->sum_weights, ctx->nb, A, nn, pj, pn);
+         CountLaunch();
+         cudaMemcpyAsync(alpha + j + 1, alpha + j, sizeof(double), cudaMemcpyDeviceToDevice, s);
+         // Classical Gram-Schmidt, twice, in the compressed inner product
+         for (int pass = 0; pass < 2; pass++) {
+            double *dh = pass ? dh2 : dh1;
+            MultiDot<double>(ws, Phi, j + 1, pn, nn, dh, s);
+            IsoCombineKernel<<<1, 32, 0, s>>>(dh, alpha, j + 1, rp2, kappa);
+            MultiAxpyKernel<double><<<igrid, 256, 0, s>>>(Phi, nn, j + 1, dh, -1.0, pn, 1);
+            CountLaunch(2);
+         }
+         MultiDot<double>(ws, pn, 1, pn, nn, dh2 + j + 1, s);
+         cudaMemcpyAsync(h1.data(), dh1, (j + 1) * sizeof(double), cudaMemcpyDeviceToHost, s);
+         cudaMemcpyAsync(h2.data(), dh2, (j + 2) * sizeof(double), cudaMemcpyDeviceToHost, s);
+         cudaMemcpyAsync(&alpha_h[j + 1], alpha + j + 1, sizeof(double), cudaMemcpyDeviceToHost, s);
+         if ((rc = CudaCheck(cudaStreamSynchronize(s), "gmres"))) return rc;
+         out->iterations++;
+         const double aw = alpha_h[j + 1];
+         const double hn = std::sqrt(aw * aw * rp2 + kappa * h2[j + 1]);
+         if (!std::isfinite(hn)) return SetError(UBOLT_ERR_NONFINITE, "GMRES Arnoldi vector is not finite");
+         for (int i = 0; i <= j; i++) H[i * m + j] = h1[i] + h2[i];
+         if (hn > 0.0) {
+            ScaleKernel<double, double><<<igrid, 256, 0, s>>>(pn, pn, 1.0 / hn, nn);
+            CountLaunch();
+            alpha_h[j + 1] = aw / hn;
+            cudaMemcpyAsync(alpha + j + 1, &alpha_h[j + 1], sizeof(double), cudaMemcpyHostToDevice, s);
+         }
+         for (int i = 0; i < j; i++) {
+            const double tt = cs[i] * H[i * m + j] + sn[i] * H[(i + 1) * m + j];
+            H[(i + 1) * m + j] = -sn[i] * H[i * m + j] + cs[i] * H[(i + 1) * m + j];
+            H[i * m + j] = tt;
+         }
+         const double d = std::hypot(H[j * m + j], hn);
+         if (d == 0.0) return SetError(UBOLT_ERR_BREAKDOWN, "GMRES breakdown at iteration %d", out->iterations);
+         cs[j] = H[j * m + j] / d;
+         sn[j] = hn / d;
+         H[j * m + j] = d;
+         gv[j + 1] = -sn[j] * gv[j];
+         gv[j] = cs[j] * gv[j];
+         out->estimate = bnorm > 0 ? std::fabs(gv[j + 1]) / bnorm : 0.0;
+         if (std::fabs(gv[j + 1]) <= rtol * bnorm || hn == 0.0) {
+            j++;
+            out->converged = true;
+            break;
+         }
+      }
+      // x += M^{-1} (sum_i y_i v_i) = M^{-1} (gamma r_perp + E_u sum_i y_i phi_i)
+      for (int i = j - 1; i >= 0; i--) {
+         double tt = gv[i];
+         for (int k = i + 1; k < j; k++) tt -= H[i * m + k] * y[k];
+         y[i] = tt / H[i * m + i];
+      }
+      double gamma = 0.0;
+      for (int i = 0; i < j; i++) gamma += y[i] * alpha_h[i];
+      cudaMemcpyAsync(dy, y.data(), j * sizeof(double), cudaMemcpyHostToDevice, s);
+      cudaMemcpyAsync(scal + 2, &gamma, sizeof(double), cudaMemcpyHostToDevice, s);
+      MultiAxpyKernel<double><<<igrid, 256, 0, s>>>(Phi, nn, j, dy, 1.0, ws->phiy, 0);
+      IsoExpandKernel<S><<<igrid, 256, 0, s>>>(r0, scal + 2, ws->phiy, ws->rho, u, A, nn, t);
+      CountLaunch(2);
+      if ((rc = Precondition<S>(ctx, UBOLT_PC_SWEEP, adjoint, t, z, tmp, n, stream))) return rc;
+      AxpyKernel<S, S><<<grid, 256, 0, s>>>(z, x, 1.0, n);
+      CountLaunch();
+      if (out->converged) break;
+   }
+   return CheckLaunch("gmres");
+}
+
 static void FreeWorkspace(ubolt_ctx *ctx)
 {
    ubolt_solver *ws = ctx->solver;
@@ -350,7 +597,8 @@ static void FreeWorkspace(ubolt_ctx *ctx)
    cudaDeviceSynchronize();
    for (void *p : {(void *)ws->r, (void *)ws->z, (void *)ws->t, (void *)ws->V, (void *)ws->V32, (void *)ws->z32,
                    (void *)ws->b32, (void *)ws->t32, (void *)ws->d32, (void *)ws->Z, (void *)ws->Z32,
-                   (void *)ws->partial, (void *)ws->h})
+                   (void *)ws->partial, (void *)ws->h, (void *)ws->Phi, (void *)ws->rho, (void *)ws->phiy,
+                   (void *)ws->alpha, (void *)ws->scal})
       if (p) cudaFree(p);
    delete ws;
    ctx->solver = nullptr;
@@ -388,6 +636,11 @@ static int EnsureWorkspace(ubolt_ctx *ctx, const ubolt_solve_options *o)
        (rc = alloc((void **)&ws->t, n * 8)) || (rc = alloc((void **)&ws->partial, (size_t)ws->red_blocks * (m + 2) * 8)) ||
        (rc = alloc((void **)&ws->h, 3 * (size_t)(m + 2) * 8)))
       return rc;
+   ws->n_nodes = ctx->n_nodes;
+   if (!flexible && ((rc = alloc((void **)&ws->Phi, (size_t)(m + 1) * ws->n_nodes * 8)) ||
+                     (rc = alloc((void **)&ws->rho, ws->n_nodes * 8)) || (rc = alloc((void **)&ws->phiy, ws->n_nodes * 8)) ||
+                     (rc = alloc((void **)&ws->alpha, (size_t)(m + 2) * 8)) || (rc = alloc((void **)&ws->scal, 4 * 8))))
+      return rc;
    if (!mixed) {
       if ((rc = alloc((void **)&ws->V, (size_t)(m + 1) * n * 8))) return rc;
       if (flexible && (rc = alloc((void **)&ws->Z, (size_t)m * n * 8))) return rc;
@@ -418,6 +671,8 @@ extern "C" void ubolt_solve_defaults(ubolt_solve_options *o)
    o->inner_rtol = 1e-5;
    o->max_outer = 10;
    o->x_zero = 1;
+   o->krylov = UBOLT_KRYLOV_AUTO;
+   o->pad_ = 0;
 }
 
 extern "C" int ubolt_solver_setup(ubolt_ctx *ctx, const ubolt_solve_options *opts)
@@ -449,20 +704,28 @@ static int SolveSystem(ubolt_ctx *ctx, bool adjoint, const double *b, double *x,
    const int64_t n = ws->n;
    const int grid = GridFor(n);
    const auto t0 = std::chrono::steady_clock::now();
+   // The compressed form wherever its identity holds: the exact sweep alone
+   // as preconditioner, and room for its four full-length vectors
+   const bool iso = o.pc == UBOLT_PC_SWEEP && ws->restart >= 3 && ws->Phi && SweepIsExact(ctx) &&
+                    o.krylov == UBOLT_KRYLOV_AUTO;
    if (o.x_zero) cudaMemsetAsync(x, 0, n * sizeof(double), s);
    const double bnorm = Norm<double>(ws, b, n, s, &rc);
    if (rc) return rc;
    if (!std::isfinite(bnorm)) return SetError(UBOLT_ERR_NONFINITE, "the right-hand side is not finite");
 
    ubolt_solve_stats st{};
+   st.krylov = iso ? UBOLT_KRYLOV_COMPRESSED : UBOLT_KRYLOV_FULL;
    bool converged = false;
    if (bnorm == 0.0) {
       cudaMemsetAsync(x, 0, n * sizeof(double), s);
       converged = true;
    } else if (o.precision == UBOLT_PRECISION_FP64) {
       GmresResult res;
-      rc = Gmres<double>(ctx, ws, ws->V, ws->Z, ws->z, ws->t, b, x, bnorm, o.rtol, o.max_it, o.pc, adjoint, o.x_zero != 0, &res,
-                         stream);
+      if (iso)
+         rc = GmresIso<double>(ctx, ws, ws->V, b, x, bnorm, o.rtol, o.max_it, adjoint, o.x_zero != 0, &res, stream);
+      else
+         rc = Gmres<double>(ctx, ws, ws->V, ws->Z, ws->z, ws->t, b, x, bnorm, o.rtol, o.max_it, o.pc, adjoint,
+                            o.x_zero != 0, &res, stream);
       if (rc) return rc;
       st.iterations = res.iterations;
       st.outer = 1;
@@ -493,8 +756,12 @@ static int SolveSystem(ubolt_ctx *ctx, bool adjoint, const double *b, double *x,
          cudaMemsetAsync(ws->d32, 0, n * sizeof(float), s);
          GmresResult res;
          const double inner = std::max(o.inner_rtol, 0.5 * o.rtol * bnorm / rnorm);
-         rc = Gmres<float>(ctx, ws, ws->V32, ws->Z32, ws->z32, ws->t32, ws->b32, ws->d32, 1.0, inner,
-                           o.max_it - st.iterations, o.pc, adjoint, true, &res, stream);
+         if (iso)
+            rc = GmresIso<float>(ctx, ws, ws->V32, ws->b32, ws->d32, 1.0, inner, o.max_it - st.iterations, adjoint,
+                                 true, &res, stream);
+         else
+            rc = Gmres<float>(ctx, ws, ws->V32, ws->Z32, ws->z32, ws->t32, ws->b32, ws->d32, 1.0, inner,
+                              o.max_it - st.iterations, o.pc, adjoint, true, &res, stream);
          if (rc) return rc;
          st.iterations += res.iterations;
          AxpyKernel<float, double><<<grid, 256, 0, s>>>(ws->d32, x, rnorm, n);

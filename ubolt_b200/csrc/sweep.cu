@@ -11,22 +11,34 @@
 // before it. Reflective inflow couples ordinates and is lagged (read as zero),
 // as are the couplings a cycle break releases.
 //
-// Kernel: persistent, one warp per task, tasks taken in number order. The
-// critical path of a sweep is the chain of upwind dependencies, so everything
-// off that chain is moved ahead of the wait: in a prologue the lanes build and
-// LU-factorise every cell's nb x nb block from geometry and sigma_t, and keep
+// Kernel: persistent, one warp per task, tasks taken in number order.
+// Synchronisation is by the data itself: psi is filled with a sentinel bit
+// pattern (all ones, a NaN the kernel never stores) before the launch, and a
+// cell whose upwind neighbour lies in an earlier task polls that neighbour's
+// psi values until none is the sentinel. So a task waits for exactly the
+// values it reads, at the level that reads them, and can start while its
+// upstream tasks are still walking: the chain of dependencies runs cell to
+// cell through L2 with no flags, fences or task-granular barriers.
+//
+// Everything off that chain happens first, in a prologue: the lanes build and
+// invert every cell's nb x nb block from geometry and sigma_t, and keep
 // y0 = B^{-1} q and G_f = B^{-1} s_f face_up_f (one per gathered face) in the
-// warp's shared-memory slice. Then the warp waits, with a bounded spin, on the
-// epoch flags of its upstream tasks, folds their values in once
-// (y0 -= G_f psi(up), read from L2 with ld.global.cg), and walks its levels
-// touching only shared memory: psi_c = y0 - sum G_f psi(up). It publishes its
-// flag with a release store after a device-scope fence. Deadlock-free: a task
-// waits only on lower-numbered tasks, which were taken by warps already running.
+// warp's shared-memory slice. The walk then runs level by level, touching
+// shared memory for in-task neighbours: psi_c = y0 - sum_f G_f psi(up_f).
+// Deadlock-free: a task polls only values of lower-numbered tasks, which were
+// taken by warps already running. Every poll is bounded; a poll that gives up
+// records a timeout, reads the value as zero and the sweep completes.
 #include "ctx.h"
 #include "sweep_plan.h"
 
 #include <algorithm>
 #include <vector>
+
+// The task counter and the error words sit on separate 128-byte lines: every
+// warp increments the counter, and a spinning lane must not contend with it.
+// Words [kCtrlNever, kCtrlNever + 2) hold a sentinel nothing overwrites (the
+// target of the bounded-wait test hook).
+constexpr int kCtrlCounter = 0, kCtrlError = 32, kCtrlNever = 48, kCtrlWords = 64;
 
 struct ubolt_sweep_plan {
    int32_t P = 0, n_patches = 0, A = 0;
@@ -41,12 +53,10 @@ struct ubolt_sweep_plan {
    const uint16_t *tmask = nullptr;     // upwind faces: in task (bit f) / earlier task (bit 8 + f)
    const int32_t *lvl_ptr = nullptr;    // [n_tasks + 1]
    const uint16_t *lvl = nullptr;       // level end positions within the task
-   uint32_t *flags = nullptr;           // [n_tasks] epoch of the last completion
-   uint32_t *ctrl = nullptr;            // [0] task counter, [1] error flag, [2] timeout count
-   uint32_t epoch = 0;
+   uint32_t *ctrl = nullptr;            // [kCtrlCounter] task counter; [kCtrlError] error flag, [kCtrlError + 1] timeout count
    int grid = 0, warps_per_block = 4;
    uint32_t spin_limit = 1u << 22;
-   int64_t unmet_task = -1;  // ubolt_sweep_test_wait: one task waits on a flag nothing sets
+   int64_t unmet_task = -1;  // ubolt_sweep_test_wait: one task polls a value nothing writes
 };
 
 namespace ubolt {
@@ -66,197 +76,317 @@ int UploadVec(ubolt_ctx *ctx, const std::vector<T> &h, const T **d)
 
 }  // namespace
 
-__device__ __forceinline__ uint32_t LoadAcquire(const uint32_t *p)
+// psi values cross warps through L2 as single 4- or 8-byte relaxed accesses:
+// a reader sees the sentinel or the final value, never a torn one
+__device__ __forceinline__ double LoadRelaxed(const double *p)
 {
-   uint32_t v;
-   asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+   double v;
+   asm volatile("ld.relaxed.gpu.global.f64 %0, [%1];" : "=d"(v) : "l"(p) : "memory");
    return v;
 }
-
-__device__ __forceinline__ void StoreRelease(uint32_t *p, uint32_t v)
+__device__ __forceinline__ float LoadRelaxed(const float *p)
 {
-   asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+   float v;
+   asm volatile("ld.relaxed.gpu.global.f32 %0, [%1];" : "=f"(v) : "l"(p) : "memory");
+   return v;
 }
+__device__ __forceinline__ void StoreRelaxed(double *p, double v)
+{
+   asm volatile("st.relaxed.gpu.global.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
+}
+__device__ __forceinline__ void StoreRelaxed(float *p, float v)
+{
+   asm volatile("st.relaxed.gpu.global.f32 [%0], %1;" ::"l"(p), "f"(v) : "memory");
+}
+__device__ __forceinline__ bool IsSentinel(double v) { return __double_as_longlong(v) == -1LL; }
+__device__ __forceinline__ bool IsSentinel(float v) { return __float_as_int(v) == -1; }
+// A computed value equal to the sentinel (a NaN carrying its payload) is
+// stored as another NaN, so a reader can never mistake a result for "not yet"
+__device__ __forceinline__ double Publishable(double v) { return IsSentinel(v) ? __longlong_as_double(0x7ff8000000000001LL) : v; }
+__device__ __forceinline__ float Publishable(float v) { return IsSentinel(v) ? __int_as_float(0x7fc00001) : v; }
 
 struct SweepDev {
    int32_t P, A;
    int64_t n_tasks;
-   const int32_t *task_pa, *dep_ptr, *deps;
+   const int32_t *task_pa;
    const int64_t *cell_ptr;
    const uint8_t *tcell;
    const uint16_t *tmask;
    const int32_t *lvl_ptr;
    const uint16_t *lvl;
-   uint32_t *flags, *ctrl;
-   uint32_t epoch;
+   uint32_t *ctrl;
    uint32_t spin_limit;
    int32_t slots;
    int64_t unmet_task;
 };
 
-template <typename T, int NB, int F>
+// Per-warp shared-memory slice, for P cells and S gathered faces per cell
+struct SweepSlice {
+   size_t loc, G, lend, bytes;
+   __host__ __device__ SweepSlice(int P, int S, int NB, int elem)
+   {
+      auto up = [](size_t v) { return (v + 15) & ~(size_t)15; };
+      loc = 0;                                       // T [P][NB], by local cell
+      G = up(loc + (size_t)P * NB * elem);           // T [P][S][NB][NB], by position
+      lend = up(G + (size_t)P * S * NB * NB * elem);  // uint16 [P]: level end positions
+      bytes = up(lend + (size_t)P * 2);
+   }
+};
+
+// The NB values psi(up, :, a) of an upwind cell in an earlier task, polled
+// until its task has stored them all. Bounded: on giving up the sticky error
+// flag is set, the timeout counted, and the missing values read as zero.
+template <typename T, int NB>
+__device__ __forceinline__ void PollUpwind(const T *p, int stride, const SweepDev &s, T xn[NB])
+{
+   bool missing = false;
+#pragma unroll
+   for (int j = 0; j < NB; j++) {
+      xn[j] = LoadRelaxed(p + (size_t)j * stride);
+      missing |= IsSentinel(xn[j]);
+   }
+   uint32_t spins = 0;
+   while (missing) {
+      // The sticky error flag (another wait gave up) is read once per 1024
+      // spins, so that waiting lanes stay off its line
+      if (++spins > s.spin_limit || ((spins & 1023u) == 0 && *(volatile uint32_t *)&s.ctrl[kCtrlError])) {
+         atomicOr(&s.ctrl[kCtrlError], 1u);
+         atomicAdd(&s.ctrl[kCtrlError + 1], 1u);
+#pragma unroll
+         for (int j = 0; j < NB; j++)
+            if (IsSentinel(xn[j])) xn[j] = T(0);
+         return;
+      }
+      if (spins > 32) __nanosleep(spins < 4096 ? 32 : 256);
+      missing = false;
+#pragma unroll
+      for (int j = 0; j < NB; j++)
+         if (IsSentinel(xn[j])) {
+            xn[j] = LoadRelaxed(p + (size_t)j * stride);
+            missing |= IsSentinel(xn[j]);
+         }
+   }
+}
+
+// y -= G x for one nb x nb coupling held in shared memory
+template <typename T, int NB>
+__device__ __forceinline__ void SubCoupling(const T *__restrict__ Gf, const T xn[NB], T y[NB])
+{
+#pragma unroll
+   for (int ii = 0; ii < NB; ii++) {
+      T u = T(0);
+#pragma unroll
+      for (int j = 0; j < NB; j++) u += Gf[ii * NB + j] * xn[j];
+      y[ii] -= u;
+   }
+}
+
+// PL: positions per lane, P <= 32 PL. Lane l owns positions l, l + 32, ...;
+// its cells' schedule (local index, level, upwind slots) stays in registers.
+template <typename T, int NB, int F, int PL>
 __global__ void __launch_bounds__(128) SweepKernel(const DevGeom<T> g, const SweepDev s, const T *__restrict__ q,
                                                    T *__restrict__ psi)
 {
    extern __shared__ __align__(16) unsigned char smem_raw[];
    const int lane = threadIdx.x & 31;
    const int warp = threadIdx.x >> 5;
-   const int S = s.slots;  // coupling matrices kept per cell
-   // Per warp: loc[P][NB] (the right-hand side, then the solution) and
-   // G[P][S][NB][NB], G_f = B^{-1} s_f face_up_f for each gathered face
-   T *loc = reinterpret_cast<T *>(smem_raw) + (size_t)warp * s.P * (NB + S * NB * NB);
-   T *G = loc + (size_t)s.P * NB;
+   const int S = s.slots;     // coupling matrices kept per cell
+   constexpr int SM = F - 1;  // most gathered faces of a cell
+   const SweepSlice L(s.P, S, NB, (int)sizeof(T));
+   unsigned char *slice = smem_raw + (size_t)warp * L.bytes;
+   T *loc = reinterpret_cast<T *>(slice + L.loc);
+   T *G = reinterpret_cast<T *>(slice + L.G);
+   uint16_t *lend = reinterpret_cast<uint16_t *>(slice + L.lend);
    const int A = s.A;
+   const T *never = reinterpret_cast<const T *>(s.ctrl + kCtrlNever);
 
    for (;;) {
       int64_t t = 0;
-      if (lane == 0) t = (int64_t)atomicAdd(&s.ctrl[0], 1u);
+      if (lane == 0) t = (int64_t)atomicAdd(&s.ctrl[kCtrlCounter], 1u);
       t = __shfl_sync(0xffffffffu, t, 0);
       if (t >= s.n_tasks) break;
-      const int32_t pa = s.task_pa[t];
+      // The task's five scalars, one lane each, in one round trip
+      int64_t v = 0;
+      if (lane == 0) v = s.task_pa[t];
+      else if (lane == 1) v = s.cell_ptr[t];
+      else if (lane == 2) v = s.cell_ptr[t + 1];
+      else if (lane == 3) v = s.lvl_ptr[t];
+      else if (lane == 4) v = s.lvl_ptr[t + 1];
+      const int32_t pa = (int32_t)__shfl_sync(0xffffffffu, v, 0);
+      const int64_t off = __shfl_sync(0xffffffffu, v, 1);
+      const int ncell = (int)(__shfl_sync(0xffffffffu, v, 2) - off);
+      const int32_t l0 = (int32_t)__shfl_sync(0xffffffffu, v, 3);
+      const int nlev = (int)(__shfl_sync(0xffffffffu, v, 4) - l0);
       const int32_t p = pa / A;
       const int a = pa - p * A;
       const int64_t base = (int64_t)p * s.P;
-      const int64_t off = s.cell_ptr[t];
-      const int ncell = (int)(s.cell_ptr[t + 1] - off);
       const T om[3] = {g.omega[3 * a], g.omega[3 * a + 1], g.omega[3 * a + 2]};
 
-      // Prologue, before the wait - nothing here depends on upstream values:
-      // every cell's block B factorised once, y0 = B^{-1} q into loc, and
-      // G_f = B^{-1} (s_f face_up_f) for every gathered face into G
-      for (int i = lane; i < ncell; i += 32) {
+      // Prologue - nothing here depends on upstream values. Every cell's
+      // block is inverted once; loc gets y0 = B^{-1} q, G the couplings
+      // G_f = B^{-1} (s_f face_up_f) of its gathered faces.
+      for (int l = lane; l < nlev; l += 32) lend[l] = s.lvl[l0 + l];
+      int my_local[PL], my_lev[PL], my_ul[PL][SM];
+      int32_t my_up[PL][SM];
+#pragma unroll
+      for (int k = 0; k < PL; k++) {
+         const int i = lane + 32 * k;
+         my_local[k] = 0;
+         my_lev[k] = -1;
+#pragma unroll
+         for (int sl = 0; sl < SM; sl++) {
+            my_ul[k][sl] = -1;
+            my_up[k][sl] = -1;
+         }
+         if (i >= ncell) continue;
          const int local = s.tcell[off + i];
          const uint32_t mask = s.tmask[off + i];
+         my_local[k] = local;
          const int64_t c = base + local;
          const int32_t cl = g.cls[c];
-         T B[NB][NB];
-         int perm[NB];
+         T r[NB], B[NB][NB], W[NB][NB];
+#pragma unroll
+         for (int j = 0; j < NB; j++) r[j] = q[(c * NB + j) * A + a];
          BuildBlock<T, NB, F>(g, cl, om, g.sigma_t[c], B);
-         const bool ok = LuFactor<T, NB>(B, perm);
-         T r[NB];
+         const bool ok = InvertBlock<T, NB>(B, W);
 #pragma unroll
-         for (int j = 0; j < NB; j++) r[j] = ok ? q[(c * NB + j) * A + a] : T(0);
-         if (ok) LuSolve<T, NB>(B, perm, r);
+         for (int ii = 0; ii < NB; ii++) {
+            T u = T(0);
 #pragma unroll
-         for (int j = 0; j < NB; j++) loc[local * NB + j] = r[j];
-         int slot = 0;
-#pragma unroll
-         for (int f = 0; f < F; f++) {
-            if (!(((mask >> f) | (mask >> (8 + f))) & 1u)) continue;
-            const T sf = Dot3(om, g.nA + ((int64_t)cl * F + f) * 3);
-            T *Gf = G + ((size_t)local * S + slot) * NB * NB;
-            if constexpr (NB == 1) {
-               Gf[0] = ok ? sf * g.inv_vol[cl] / B[0][0] : T(0);
-            } else {
-               const T *M = g.fup + ((int64_t)cl * F + f) * NB * NB;
-#pragma unroll
-               for (int j = 0; j < NB; j++) {
-                  T col[NB];
-#pragma unroll
-                  for (int ii = 0; ii < NB; ii++) col[ii] = sf * M[ii * NB + j];
-                  if (ok) LuSolve<T, NB>(B, perm, col);
-#pragma unroll
-                  for (int ii = 0; ii < NB; ii++) Gf[ii * NB + j] = ok ? col[ii] : T(0);
-               }
-            }
-            slot++;
+            for (int j = 0; j < NB; j++) u += W[ii][j] * r[j];
+            loc[local * NB + ii] = ok ? u : T(0);
          }
-      }
-
-      // Wait for the upstream tasks: bounded, and a timeout is reported
-      for (int d = s.dep_ptr[t] + lane; d < s.dep_ptr[t + 1]; d += 32) {
-         const uint32_t *f = &s.flags[s.deps[d]];
-         uint32_t spins = 0;
-         const uint32_t want = (t == s.unmet_task) ? s.epoch + 1u : s.epoch;
-         while (LoadAcquire(f) != want) {
-            if (++spins > s.spin_limit || *(volatile uint32_t *)&s.ctrl[1]) {
-               atomicOr(&s.ctrl[1], 1u);
-               atomicAdd(&s.ctrl[2], 1u);
-               break;
-            }
-            __nanosleep(spins < 64 ? 32 : 256);
-         }
-      }
-      __syncwarp();
-      __threadfence();
-
-      // Fold the upwind values from earlier tasks in: y0 -= G_f psi(up)
-      for (int i = lane; i < ncell; i += 32) {
-         const uint32_t mask = s.tmask[off + i];
-         if (!(mask >> 8)) continue;
-         const int local = s.tcell[off + i];
-         const int64_t c = base + local;
-         T y[NB];
-#pragma unroll
-         for (int j = 0; j < NB; j++) y[j] = loc[local * NB + j];
          int slot = 0;
 #pragma unroll
          for (int f = 0; f < F; f++) {
             const bool here = (mask >> f) & 1u, earlier = (mask >> (8 + f)) & 1u;
             if (!(here || earlier)) continue;
-            if (earlier) {
-               const int64_t up = g.code[c * F + f];
-               const T *Gf = G + ((size_t)local * S + slot) * NB * NB;
-               T xn[NB];
+            const int32_t code = g.code[c * F + f];
+            const T sf = Dot3(om, g.nA + ((int64_t)cl * F + f) * 3);
+            T *Gf = G + ((size_t)i * S + slot) * NB * NB;
+            if constexpr (NB == 1) {
+               Gf[0] = ok ? W[0][0] * (sf * g.inv_vol[cl]) : T(0);
+            } else {
+               const T *M = g.fup + ((int64_t)cl * F + f) * NB * NB;
+               T Ms[NB][NB];
 #pragma unroll
-               for (int j = 0; j < NB; j++) xn[j] = __ldcg(&psi[(up * NB + j) * A + a]);
+               for (int kk = 0; kk < NB; kk++)
 #pragma unroll
-               for (int ii = 0; ii < NB; ii++) {
-                  T u = T(0);
+                  for (int j = 0; j < NB; j++) Ms[kk][j] = sf * M[kk * NB + j];
 #pragma unroll
-                  for (int j = 0; j < NB; j++) u += Gf[ii * NB + j] * xn[j];
-                  y[ii] -= u;
-               }
+               for (int ii = 0; ii < NB; ii++)
+#pragma unroll
+                  for (int j = 0; j < NB; j++) {
+                     T u = T(0);
+#pragma unroll
+                     for (int kk = 0; kk < NB; kk++) u += W[ii][kk] * Ms[kk][j];
+                     Gf[ii * NB + j] = ok ? u : T(0);
+                  }
             }
+#pragma unroll
+            for (int sl = 0; sl < SM; sl++)
+               if (sl == slot) {
+                  my_ul[k][sl] = here ? (int)(code - base) : -1;
+                  my_up[k][sl] = earlier ? code : -1;
+               }
             slot++;
          }
+      }
+      __syncwarp();
+      // The level of each owned position: the number of level ends at or before it
+      for (int l = 0; l < nlev; l++) {
+         const int e = lend[l];
 #pragma unroll
-         for (int j = 0; j < NB; j++) loc[local * NB + j] = y[j];
+         for (int k = 0; k < PL; k++)
+            if (lane + 32 * k < ncell && e <= lane + 32 * k) my_lev[k] = l + 1;
+      }
+#pragma unroll
+      for (int k = 0; k < PL; k++)
+         if (lane + 32 * k < ncell && my_lev[k] < 0) my_lev[k] = 0;
+
+      // Upwind values from earlier tasks that are stored already are folded
+      // in now, all loads in flight together; the rest are polled at their level
+      bool hook = (t == s.unmet_task);
+      if constexpr (PL <= 2) {
+         if (!hook) {
+            T xn[PL][SM][NB];
+#pragma unroll
+            for (int k = 0; k < PL; k++)
+#pragma unroll
+               for (int sl = 0; sl < SM; sl++)
+#pragma unroll
+                  for (int j = 0; j < NB; j++)
+                     xn[k][sl][j] = my_up[k][sl] >= 0 ? LoadRelaxed(psi + ((int64_t)my_up[k][sl] * NB + j) * A + a) : T(0);
+#pragma unroll
+            for (int k = 0; k < PL; k++) {
+               bool any = false;
+               T y[NB];
+#pragma unroll
+               for (int j = 0; j < NB; j++) y[j] = T(0);
+#pragma unroll
+               for (int sl = 0; sl < SM; sl++) {
+                  if (my_up[k][sl] < 0) continue;
+                  bool ready = true;
+#pragma unroll
+                  for (int j = 0; j < NB; j++) ready &= !IsSentinel(xn[k][sl][j]);
+                  if (!ready) continue;
+                  if (!any) {
+#pragma unroll
+                     for (int j = 0; j < NB; j++) y[j] = loc[my_local[k] * NB + j];
+                     any = true;
+                  }
+                  SubCoupling<T, NB>(G + ((size_t)(lane + 32 * k) * S + sl) * NB * NB, xn[k][sl], y);
+                  my_up[k][sl] = -1;
+               }
+               if (any) {
+#pragma unroll
+                  for (int j = 0; j < NB; j++) loc[my_local[k] * NB + j] = y[j];
+               }
+            }
+         }
       }
       __syncwarp();
 
-      // Level by level, shared memory only: psi_c = y0 - sum_{in-task f} G_f psi(up)
-      int lo = 0;
-      for (int l = s.lvl_ptr[t]; l < s.lvl_ptr[t + 1]; l++) {
-         const int hi = s.lvl[l];
-         for (int i = lo + lane; i < hi; i += 32) {
-            const int local = s.tcell[off + i];
-            const uint32_t mask = s.tmask[off + i];
-            const int64_t c = base + local;
+      // Level by level: psi_c = y0 - sum_f G_f psi(up_f), an in-task
+      // neighbour from shared memory, an earlier task's polled from L2
+      for (int l = 0; l < nlev; l++) {
+#pragma unroll
+         for (int k = 0; k < PL; k++) {
+            if (my_lev[k] != l) continue;
+            const int i = lane + 32 * k;
+            const int local = my_local[k];
             T y[NB];
 #pragma unroll
             for (int j = 0; j < NB; j++) y[j] = loc[local * NB + j];
-            if (mask & 0xffu) {
-               int slot = 0;
 #pragma unroll
-               for (int f = 0; f < F; f++) {
-                  const bool here = (mask >> f) & 1u, earlier = (mask >> (8 + f)) & 1u;
-                  if (!(here || earlier)) continue;
-                  if (here) {
-                     const int ul = (int)(g.code[c * F + f] - base);
-                     const T *Gf = G + ((size_t)local * S + slot) * NB * NB;
+            for (int sl = 0; sl < SM; sl++) {
+               T xn[NB];
+               if (my_ul[k][sl] >= 0) {
 #pragma unroll
-                     for (int ii = 0; ii < NB; ii++) {
-                        T u = T(0);
-#pragma unroll
-                        for (int j = 0; j < NB; j++) u += Gf[ii * NB + j] * loc[ul * NB + j];
-                        y[ii] -= u;
-                     }
+                  for (int j = 0; j < NB; j++) xn[j] = loc[my_ul[k][sl] * NB + j];
+               } else if (my_up[k][sl] >= 0) {
+                  const T *src = psi + (int64_t)my_up[k][sl] * NB * A + a;
+                  int stride = A;
+                  if (hook) {
+                     src = never;  // test hook: this wait can never be met
+                     stride = 0;
+                     hook = false;
                   }
-                  slot++;
+                  PollUpwind<T, NB>(src, stride, s, xn);
+               } else {
+                  continue;
                }
-#pragma unroll
-               for (int j = 0; j < NB; j++) loc[local * NB + j] = y[j];
+               SubCoupling<T, NB>(G + ((size_t)i * S + sl) * NB * NB, xn, y);
             }
+            const int64_t c = base + local;
 #pragma unroll
-            for (int j = 0; j < NB; j++) psi[(c * NB + j) * A + a] = y[j];
+            for (int j = 0; j < NB; j++) {
+               loc[local * NB + j] = y[j];
+               StoreRelaxed(&psi[(c * NB + j) * A + a], Publishable(y[j]));
+            }
          }
-         lo = hi;
          __syncwarp();
       }
-      __threadfence();
-      __syncwarp();
-      if (lane == 0) StoreRelease(&s.flags[t], s.epoch);
    }
 }
 
@@ -281,6 +411,10 @@ int BuildSweepPlan(ubolt_ctx *ctx, int patch_size)
    plan->n_split = h.n_split;
    plan->max_levels = h.max_levels;
    plan->max_inflow = h.max_inflow;
+   if (h.max_inflow > ctx->F - 1) {
+      delete plan;
+      return SetError(UBOLT_ERR_ARG, "a cell has %d upwind faces for one ordinate (at most %d)", h.max_inflow, ctx->F - 1);
+   }
    plan->total_levels = (int64_t)h.lvl.size();
    int rc = 0;
    if ((rc = UploadVec(ctx, h.task_pa, &plan->task_pa)) || (rc = UploadVec(ctx, h.dep_ptr, &plan->dep_ptr)) ||
@@ -291,12 +425,10 @@ int BuildSweepPlan(ubolt_ctx *ctx, int patch_size)
       return rc;
    }
    void *p = nullptr;
-   if ((rc = CtxAlloc(ctx, h.n_tasks * sizeof(uint32_t), &p))) { delete plan; return rc; }
-   plan->flags = static_cast<uint32_t *>(p);
-   cudaMemset(plan->flags, 0, h.n_tasks * sizeof(uint32_t));
-   if ((rc = CtxAlloc(ctx, 4 * sizeof(uint32_t), &p))) { delete plan; return rc; }
+   if ((rc = CtxAlloc(ctx, kCtrlWords * sizeof(uint32_t), &p))) { delete plan; return rc; }
    plan->ctrl = static_cast<uint32_t *>(p);
-   cudaMemset(plan->ctrl, 0, 4 * sizeof(uint32_t));
+   cudaMemset(plan->ctrl, 0, kCtrlWords * sizeof(uint32_t));
+   cudaMemset(plan->ctrl + kCtrlNever, 0xff, 2 * sizeof(uint32_t));
    delete ctx->sweep;
    ctx->sweep = plan;
    return CudaCheck(cudaDeviceSynchronize(), "sweep plan");
@@ -308,8 +440,8 @@ static int LaunchSweep(ubolt_ctx *ctx, const T *q, T *psi, cudaStream_t st)
    ubolt_sweep_plan *pl = ctx->sweep;
    const int threads = 32 * pl->warps_per_block;
    const int slots = std::max(1, std::min(F - 1, (int)pl->max_inflow));
-   const size_t smem = sizeof(T) * (size_t)pl->warps_per_block * pl->P * (NB + slots * NB * NB);
-   auto kern = SweepKernel<T, NB, F>;
+   const size_t smem = (size_t)pl->warps_per_block * SweepSlice(pl->P, slots, NB, (int)sizeof(T)).bytes;
+   auto kern = pl->P <= 64 ? SweepKernel<T, NB, F, 2> : SweepKernel<T, NB, F, 8>;
    if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
    int per_sm = 0, n_sm = 0, dev = 0;
    cudaGetDevice(&dev);
@@ -318,28 +450,24 @@ static int LaunchSweep(ubolt_ctx *ctx, const T *q, T *psi, cudaStream_t st)
    const int64_t want = (pl->n_tasks + pl->warps_per_block - 1) / pl->warps_per_block;
    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)std::max(per_sm, 1) * n_sm, want));
    pl->grid = grid;
-   pl->epoch++;
-   if (pl->epoch == 0) pl->epoch = 1;
    SweepDev s;
    s.P = pl->P;
    s.A = pl->A;
    s.n_tasks = pl->n_tasks;
    s.task_pa = pl->task_pa;
-   s.dep_ptr = pl->dep_ptr;
-   s.deps = pl->deps;
    s.cell_ptr = pl->cell_ptr;
    s.tcell = pl->tcell;
    s.tmask = pl->tmask;
    s.lvl_ptr = pl->lvl_ptr;
    s.lvl = pl->lvl;
-   s.flags = pl->flags;
    s.ctrl = pl->ctrl;
-   s.epoch = pl->epoch;
    s.spin_limit = pl->spin_limit;
    s.unmet_task = pl->unmet_task;
    pl->unmet_task = -1;
    s.slots = slots;
-   cudaMemsetAsync(pl->ctrl, 0, sizeof(uint32_t), st);  // task counter; the error flag stays sticky
+   cudaMemsetAsync(pl->ctrl + kCtrlCounter, 0, sizeof(uint32_t), st);  // task counter; the error flag stays sticky
+   // Every psi value starts as the sentinel: "not yet stored by its task"
+   cudaMemsetAsync(psi, 0xff, (size_t)ctx->n_cells * NB * ctx->A * sizeof(T), st);
    kern<<<grid, threads, smem, st>>>(ctx->geom<T>(), s, q, psi);
    return CheckLaunch("sweep");
 }
@@ -354,6 +482,14 @@ int Sweep(ubolt_ctx *ctx, const T *q, T *psi, void *stream)
       return SetError(UBOLT_ERR_ARG, "sweep: q and psi must be distinct device arrays");
    UBOLT_DISPATCH(ctx->nb, ctx->F, return (LaunchSweep<T, NB_, F_>(ctx, q, psi, (cudaStream_t)stream)));
    return SetError(UBOLT_ERR_STATE, "no sweep kernel for this shape");
+}
+
+// True where the sweep is L^{-1} exactly: a plan with no lagged coupling and
+// no reflective side (reflective inflow is lagged)
+bool SweepIsExact(ubolt_ctx *ctx)
+{
+   if (!ctx->sweep && BuildSweepPlan(ctx, 0)) return false;
+   return ctx->sweep->n_lagged == 0 && !ctx->has_reflect;
 }
 
 template int Sweep<double>(ubolt_ctx *, const double *, double *, void *);
@@ -393,9 +529,9 @@ extern "C" int ubolt_sweep_status(ubolt_ctx *ctx, ubolt_sweep_info *info, void *
    if (rc) return rc;
    if (!ctx->sweep) return SetError(UBOLT_ERR_STATE, "no sweep plan");
    ubolt_sweep_plan *pl = ctx->sweep;
-   uint32_t h[4] = {0, 0, 0, 0};
+   uint32_t h[2] = {0, 0};  // error flag, timeout count
    cudaStream_t s = (cudaStream_t)stream;
-   cudaMemcpyAsync(h, pl->ctrl, sizeof h, cudaMemcpyDeviceToHost, s);
+   cudaMemcpyAsync(h, pl->ctrl + kCtrlError, sizeof h, cudaMemcpyDeviceToHost, s);
    if ((rc = CudaCheck(cudaStreamSynchronize(s), "sweep_status"))) return rc;
    if (info) {
       info->patch_size = pl->P;
@@ -406,12 +542,12 @@ extern "C" int ubolt_sweep_status(ubolt_ctx *ctx, ubolt_sweep_info *info, void *
       info->max_levels = pl->max_levels;
       info->total_levels = pl->total_levels;
       info->grid = pl->grid;
-      info->timeouts = h[2];
+      info->timeouts = h[1];
    }
-   if (h[1]) {
-      cudaMemsetAsync(pl->ctrl + 1, 0, 2 * sizeof(uint32_t), s);
+   if (h[0]) {
+      cudaMemsetAsync(pl->ctrl + kCtrlError, 0, 2 * sizeof(uint32_t), s);
       cudaStreamSynchronize(s);
-      return SetError(UBOLT_ERR_TIMEOUT, "a sweep wait gave up (%u timeouts); its result is not valid", h[2]);
+      return SetError(UBOLT_ERR_TIMEOUT, "a sweep wait gave up (%u timeouts); its result is not valid", h[1]);
    }
    return UBOLT_OK;
 }
@@ -426,7 +562,8 @@ extern "C" int ubolt_sweep_test_wait(ubolt_ctx *ctx, uint32_t spin_limit, int ma
    pl->spin_limit = spin_limit;
    pl->unmet_task = -1;
    if (make_one_wait_unmet) {
-      // The first task that has an upstream task waits for an epoch that no
+      // The first task that has an upstream task polls, for its first
+      // upwind value, a word nothing writes
       // task of this sweep publishes
       std::vector<int32_t> dp(pl->n_tasks + 1);
       cudaMemcpy(dp.data(), pl->dep_ptr, dp.size() * sizeof(int32_t), cudaMemcpyDeviceToHost);

@@ -12,7 +12,8 @@
 // with the fewest unresolved inputs; those inputs are lagged (read as zero).
 //
 // All ordinates' tasks are merged by depth (1 + the deepest upstream task),
-// which is topological for every ordinate, and renumbered in that order.
+// which is topological for every ordinate, patch by patch within a depth,
+// and renumbered in that order.
 #include "sweep_plan.h"
 
 #include "ubolt_internal.h"
@@ -164,9 +165,13 @@ void BuildHostSweepPlan(int64_t nc, int F, int A, int P, const double *om, const
    std::vector<std::pair<int32_t, int32_t>> all;  // (angle, angle-local id)
    for (int a = 0; a < A; a++)
       for (int32_t t = 0; t < (int32_t)per_angle[a].size(); t++) all.emplace_back(a, t);
+   // Within one depth, the tasks of one patch sit together (ordinates of one
+   // octant reach a patch at about the same depth), so warps taking
+   // consecutive tasks read that patch's geometry while it is in L2
    std::stable_sort(all.begin(), all.end(), [&](const auto &x, const auto &y) {
-      const int32_t dx = per_angle[x.first][x.second].depth, dy = per_angle[y.first][y.second].depth;
-      if (dx != dy) return dx < dy;
+      const AngleTask &tx = per_angle[x.first][x.second], &ty = per_angle[y.first][y.second];
+      if (tx.depth != ty.depth) return tx.depth < ty.depth;
+      if (tx.patch != ty.patch) return tx.patch < ty.patch;
       return x.first < y.first;
    });
    std::vector<std::vector<int32_t>> gid(A);

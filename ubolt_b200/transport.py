@@ -199,11 +199,12 @@ class TransportSolver:
     """GMRES (right-preconditioned) on the current group: TransportSolver::solve."""
 
     def __init__(self, ctx, rtol=1e-8, precision="fp64", pc="sweep", restart=30, max_it=500, inner_rtol=1e-5,
-                 max_outer=10):
+                 max_outer=10, krylov="auto"):
         self.ctx = ctx
         o = _lib.SolveOptions()
         lib.ubolt_solve_defaults(C.byref(o))
         o.rtol, o.inner_rtol, o.max_it, o.restart, o.max_outer = rtol, inner_rtol, max_it, restart, max_outer
+        o.krylov = {"auto": 0, "full": 1}[krylov]
         o.precision = {"fp64": _lib.PRECISION_FP64, "mixed": _lib.PRECISION_MIXED}[precision]
         o.pc = {"none": _lib.PC_NONE, "block": _lib.PC_BLOCK, "sweep": _lib.PC_SWEEP,
                 "sweep+dsa": _lib.PC_SWEEP_DSA}[pc]
