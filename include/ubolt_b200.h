@@ -228,6 +228,7 @@ typedef struct {
    int64_t total_levels;
    uint32_t timeouts;     /* bounded waits that gave up since the last status */
    uint32_t pad_;
+   int64_t factor_bytes;  /* device bytes held by the factor stores (FP64 + FP32) */
 } ubolt_sweep_info;
 
 /* Build the sweep plan: patches of patch_size consecutive cells (0 picks 64;
@@ -243,6 +244,15 @@ int ubolt_sweep_setup(ubolt_ctx *ctx, int patch_size);
  * bounded; check ubolt_sweep_status. */
 int ubolt_sweep(ubolt_ctx *ctx, const double *q, double *psi, void *stream);
 int ubolt_sweep_f32(ubolt_ctx *ctx, const float *q, float *psi, void *stream);
+/* The factor store: each cell-ordinate's B^{-1} and upwind couplings
+ * G_f = B^{-1} s_f face_up_f, which depend on geometry and sigma_t but not on
+ * q, built once per group (ubolt_set_group starts a new group) and read by
+ * every sweep instead of being recomputed: n_cells A nb^2 (1 + slots)
+ * values per precision, in task order. bytes < 0 (the default): build it
+ * when it fits a quarter of the free device memory, at most 64 GiB; 0: never;
+ * otherwise the limit in bytes. Either way the result is the same, bit for
+ * bit. Frees a store the new limit does not admit. */
+int ubolt_sweep_set_factor_limit(ubolt_ctx *ctx, int64_t bytes);
 /* Plan statistics and the sticky timeout flag (synchronises `stream`):
  * returns UBOLT_ERR_TIMEOUT, and clears the flag, if a wait gave up. */
 int ubolt_sweep_status(ubolt_ctx *ctx, ubolt_sweep_info *info, void *stream);

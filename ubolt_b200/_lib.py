@@ -94,7 +94,8 @@ def declared_symbols(header=None):
 class SweepInfo(C.Structure):
     _fields_ = [("patch_size", C.c_int32), ("n_patches", C.c_int32), ("n_tasks", C.c_int64),
                 ("n_lagged", C.c_int64), ("n_split", C.c_int64), ("max_levels", C.c_int32), ("grid", C.c_int32),
-                ("total_levels", C.c_int64), ("timeouts", C.c_uint32), ("pad_", C.c_uint32)]
+                ("total_levels", C.c_int64), ("timeouts", C.c_uint32), ("pad_", C.c_uint32),
+                ("factor_bytes", C.c_int64)]
 
 
 class SolveOptions(C.Structure):
@@ -116,6 +117,7 @@ _sig("ubolt_sweep", C.c_int, vp, vp, vp, vp)
 _sig("ubolt_sweep_f32", C.c_int, vp, vp, vp, vp)
 _sig("ubolt_sweep_status", C.c_int, vp, C.POINTER(SweepInfo), vp)
 _sig("ubolt_sweep_test_wait", C.c_int, vp, C.c_uint32, C.c_int)
+_sig("ubolt_sweep_set_factor_limit", C.c_int, vp, C.c_int64)
 _sig("ubolt_solve_defaults", None, C.POINTER(SolveOptions))
 _sig("ubolt_solver_setup", C.c_int, vp, C.POINTER(SolveOptions))
 _sig("ubolt_solve", C.c_int, vp, vp, vp, C.POINTER(SolveOptions), C.POINTER(SolveStats), vp)

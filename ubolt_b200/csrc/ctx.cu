@@ -335,5 +335,6 @@ extern "C" int ubolt_set_group(ubolt_ctx *ctx, const double *sigma_t, const doub
    rc = CheckLaunch("set_group");
    if (rc) return rc;
    ctx->group_set = true;
+   ctx->group_epoch++;
    return UBOLT_OK;
 }

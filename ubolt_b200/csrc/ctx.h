@@ -35,6 +35,7 @@ struct ubolt_ctx {
    const int32_t *d_opp = nullptr;             // [A] the ordinate opposite each ordinate
    unsigned long long *d_counters = nullptr;   // 64 counters/flags for set-up calls
    bool group_set = false;
+   uint64_t group_epoch = 0;  // bumped by every ubolt_set_group: caches keyed on the cross sections
 
    ubolt_sweep_plan *sweep = nullptr;
    ubolt_dsa *dsa = nullptr;

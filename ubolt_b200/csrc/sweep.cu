@@ -53,10 +53,22 @@ struct ubolt_sweep_plan {
    const uint16_t *tmask = nullptr;     // upwind faces: in task (bit f) / earlier task (bit 8 + f)
    const int32_t *lvl_ptr = nullptr;    // [n_tasks + 1]
    const uint16_t *lvl = nullptr;       // level end positions within the task
+   const int32_t *tlink = nullptr;      // [entries][slots] upwind link per gathered face: >= 0 the cell in an
+                                        // earlier task, -2 - local for a cell of this task, -1 none
    uint32_t *ctrl = nullptr;            // [kCtrlCounter] task counter; [kCtrlError] error flag, [kCtrlError + 1] timeout count
-   int grid = 0, warps_per_block = 4;
+   int grid = 0, warps_per_block = 4, slots = 1;
    uint32_t spin_limit = 1u << 22;
    int64_t unmet_task = -1;  // ubolt_sweep_test_wait: one task polls a value nothing writes
+   // The factor store (B^{-1} and couplings per task entry) per precision,
+   // valid for the group epoch it was built in; limit < 0: automatic
+   void *fac[2] = {nullptr, nullptr};
+   uint64_t fac_epoch[2] = {0, 0};
+   int64_t fac_limit = -1;
+   ~ubolt_sweep_plan()
+   {
+      for (void *f : fac)
+         if (f) cudaFree(f);
+   }
 };
 
 namespace ubolt {
@@ -112,6 +124,7 @@ struct SweepDev {
    const int64_t *cell_ptr;
    const uint8_t *tcell;
    const uint16_t *tmask;
+   const int32_t *tlink;
    const int32_t *lvl_ptr;
    const uint16_t *lvl;
    uint32_t *ctrl;
@@ -126,8 +139,8 @@ struct SweepSlice {
    __host__ __device__ SweepSlice(int P, int S, int NB, int elem)
    {
       auto up = [](size_t v) { return (v + 15) & ~(size_t)15; };
-      loc = 0;                                       // T [P][NB], by local cell
-      G = up(loc + (size_t)P * NB * elem);           // T [P][S][NB][NB], by position
+      loc = 0;                                        // T [P][NB], by local cell
+      G = up(loc + (size_t)P * NB * elem);            // T [P][S][NB][NB], by position
       lend = up(G + (size_t)P * S * NB * NB * elem);  // uint16 [P]: level end positions
       bytes = up(lend + (size_t)P * 2);
    }
@@ -181,11 +194,92 @@ __device__ __forceinline__ void SubCoupling(const T *__restrict__ Gf, const T xn
    }
 }
 
+// The factors of one (cell, ordinate) for the sweep: W = B^{-1} of its
+// streaming + removal block, and G_s = W (s_f face_up_f) for each gathered
+// face f in face order (slot s); element (s, ii, j) goes to Gout[s * gs + (ii * NB + j) * ge].
+// A singular block gives zero factors. Returns false then.
+template <typename T, int NB, int F>
+__device__ __forceinline__ bool CellFactors(const DevGeom<T> &g, int64_t c, const T om[3], uint32_t mask, T W[NB][NB],
+                                            T *Gout, size_t gs, size_t ge)
+{
+   const int32_t cl = g.cls[c];
+   T B[NB][NB];
+   BuildBlock<T, NB, F>(g, cl, om, g.sigma_t[c], B);
+   const bool ok = InvertBlock<T, NB>(B, W);
+   if (!ok)
+#pragma unroll
+      for (int ii = 0; ii < NB; ii++)
+#pragma unroll
+         for (int j = 0; j < NB; j++) W[ii][j] = T(0);
+   int slot = 0;
+#pragma unroll
+   for (int f = 0; f < F; f++) {
+      if (!(((mask >> f) | (mask >> (8 + f))) & 1u)) continue;
+      const T sf = Dot3(om, g.nA + ((int64_t)cl * F + f) * 3);
+      T *Gf = Gout + (size_t)slot * gs;
+      if constexpr (NB == 1) {
+         Gf[0] = W[0][0] * (sf * g.inv_vol[cl]);
+      } else {
+         const T *M = g.fup + ((int64_t)cl * F + f) * NB * NB;
+         T Ms[NB][NB];
+#pragma unroll
+         for (int kk = 0; kk < NB; kk++)
+#pragma unroll
+            for (int j = 0; j < NB; j++) Ms[kk][j] = sf * M[kk * NB + j];
+#pragma unroll
+         for (int ii = 0; ii < NB; ii++)
+#pragma unroll
+            for (int j = 0; j < NB; j++) {
+               T u = T(0);
+#pragma unroll
+               for (int kk = 0; kk < NB; kk++) u += W[ii][kk] * Ms[kk][j];
+               Gf[(size_t)(ii * NB + j) * ge] = u;
+            }
+      }
+      slot++;
+   }
+   return ok;
+}
+
+// The factor store: per task, element-major over its positions, so a warp's
+// lanes read consecutive words - element r of position i of task t at
+// cell_ptr[t] R + r ncell_t + i, R = NB^2 (1 + S): W, then G_0 .. G_{S-1}.
+// Independent of the right-hand side: built once per group, read by every sweep.
+template <typename T, int NB, int F>
+__global__ void __launch_bounds__(128) FactorKernel(const DevGeom<T> g, const SweepDev s, T *__restrict__ fac)
+{
+   const int lane = threadIdx.x & 31;
+   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+   const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+   const int S = s.slots;
+   const size_t R = (size_t)NB * NB * (1 + S);
+   for (int64_t t = warp; t < s.n_tasks; t += n_warps) {
+      const int32_t pa = s.task_pa[t];
+      const int64_t off = s.cell_ptr[t];
+      const int ncell = (int)(s.cell_ptr[t + 1] - off);
+      const int32_t p = pa / s.A;
+      const int a = pa - p * s.A;
+      const int64_t base = (int64_t)p * s.P;
+      const T om[3] = {g.omega[3 * a], g.omega[3 * a + 1], g.omega[3 * a + 2]};
+      T *ft = fac + (size_t)off * R;
+      for (int i = lane; i < ncell; i += 32) {
+         T W[NB][NB];
+         CellFactors<T, NB, F>(g, base + s.tcell[off + i], om, s.tmask[off + i], W, ft + (size_t)NB * NB * ncell + i,
+                               (size_t)NB * NB * ncell, (size_t)ncell);
+#pragma unroll
+         for (int ii = 0; ii < NB; ii++)
+#pragma unroll
+            for (int j = 0; j < NB; j++) ft[(size_t)(ii * NB + j) * ncell + i] = W[ii][j];
+      }
+   }
+}
+
 // PL: positions per lane, P <= 32 PL. Lane l owns positions l, l + 32, ...;
-// its cells' schedule (local index, level, upwind slots) stays in registers.
-template <typename T, int NB, int F, int PL>
+// its cells' schedule (local index, level, upwind links) stays in registers.
+// CACHED: the factors come from the store, else they are computed here.
+template <typename T, int NB, int F, int PL, bool CACHED>
 __global__ void __launch_bounds__(128) SweepKernel(const DevGeom<T> g, const SweepDev s, const T *__restrict__ q,
-                                                   T *__restrict__ psi)
+                                                   T *__restrict__ psi, const T *__restrict__ fac)
 {
    extern __shared__ __align__(16) unsigned char smem_raw[];
    const int lane = threadIdx.x & 31;
@@ -199,6 +293,7 @@ __global__ void __launch_bounds__(128) SweepKernel(const DevGeom<T> g, const Swe
    uint16_t *lend = reinterpret_cast<uint16_t *>(slice + L.lend);
    const int A = s.A;
    const T *never = reinterpret_cast<const T *>(s.ctrl + kCtrlNever);
+   const size_t R = (size_t)NB * NB * (1 + S);
 
    for (;;) {
       int64_t t = 0;
@@ -220,11 +315,10 @@ __global__ void __launch_bounds__(128) SweepKernel(const DevGeom<T> g, const Swe
       const int32_t p = pa / A;
       const int a = pa - p * A;
       const int64_t base = (int64_t)p * s.P;
-      const T om[3] = {g.omega[3 * a], g.omega[3 * a + 1], g.omega[3 * a + 2]};
 
-      // Prologue - nothing here depends on upstream values. Every cell's
-      // block is inverted once; loc gets y0 = B^{-1} q, G the couplings
-      // G_f = B^{-1} (s_f face_up_f) of its gathered faces.
+      // Prologue - nothing here depends on upstream values: loc gets
+      // y0 = B^{-1} q, G the couplings of the gathered faces, and each lane
+      // its positions' schedule
       for (int l = lane; l < nlev; l += 32) lend[l] = s.lvl[l0 + l];
       int my_local[PL], my_lev[PL], my_ul[PL][SM];
       int32_t my_up[PL][SM];
@@ -240,56 +334,34 @@ __global__ void __launch_bounds__(128) SweepKernel(const DevGeom<T> g, const Swe
          }
          if (i >= ncell) continue;
          const int local = s.tcell[off + i];
-         const uint32_t mask = s.tmask[off + i];
          my_local[k] = local;
+#pragma unroll
+         for (int sl = 0; sl < SM; sl++) {
+            const int32_t lk = sl < S ? s.tlink[(off + i) * S + sl] : -1;
+            if (lk >= 0) my_up[k][sl] = lk;
+            else if (lk <= -2) my_ul[k][sl] = -2 - lk;
+         }
          const int64_t c = base + local;
-         const int32_t cl = g.cls[c];
-         T r[NB], B[NB][NB], W[NB][NB];
+         T r[NB], W[NB][NB];
 #pragma unroll
          for (int j = 0; j < NB; j++) r[j] = q[(c * NB + j) * A + a];
-         BuildBlock<T, NB, F>(g, cl, om, g.sigma_t[c], B);
-         const bool ok = InvertBlock<T, NB>(B, W);
+         if constexpr (CACHED) {
+            const T *ft = fac + (size_t)off * R + i;
+#pragma unroll
+            for (int ii = 0; ii < NB; ii++)
+#pragma unroll
+               for (int j = 0; j < NB; j++) W[ii][j] = ft[(size_t)(ii * NB + j) * ncell];
+            for (int e = 0; e < S * NB * NB; e++) G[(size_t)i * S * NB * NB + e] = ft[(size_t)(NB * NB + e) * ncell];
+         } else {
+            const T om[3] = {g.omega[3 * a], g.omega[3 * a + 1], g.omega[3 * a + 2]};
+            CellFactors<T, NB, F>(g, c, om, s.tmask[off + i], W, G + (size_t)i * S * NB * NB, (size_t)NB * NB, 1);
+         }
 #pragma unroll
          for (int ii = 0; ii < NB; ii++) {
             T u = T(0);
 #pragma unroll
             for (int j = 0; j < NB; j++) u += W[ii][j] * r[j];
-            loc[local * NB + ii] = ok ? u : T(0);
-         }
-         int slot = 0;
-#pragma unroll
-         for (int f = 0; f < F; f++) {
-            const bool here = (mask >> f) & 1u, earlier = (mask >> (8 + f)) & 1u;
-            if (!(here || earlier)) continue;
-            const int32_t code = g.code[c * F + f];
-            const T sf = Dot3(om, g.nA + ((int64_t)cl * F + f) * 3);
-            T *Gf = G + ((size_t)i * S + slot) * NB * NB;
-            if constexpr (NB == 1) {
-               Gf[0] = ok ? W[0][0] * (sf * g.inv_vol[cl]) : T(0);
-            } else {
-               const T *M = g.fup + ((int64_t)cl * F + f) * NB * NB;
-               T Ms[NB][NB];
-#pragma unroll
-               for (int kk = 0; kk < NB; kk++)
-#pragma unroll
-                  for (int j = 0; j < NB; j++) Ms[kk][j] = sf * M[kk * NB + j];
-#pragma unroll
-               for (int ii = 0; ii < NB; ii++)
-#pragma unroll
-                  for (int j = 0; j < NB; j++) {
-                     T u = T(0);
-#pragma unroll
-                     for (int kk = 0; kk < NB; kk++) u += W[ii][kk] * Ms[kk][j];
-                     Gf[ii * NB + j] = ok ? u : T(0);
-                  }
-            }
-#pragma unroll
-            for (int sl = 0; sl < SM; sl++)
-               if (sl == slot) {
-                  my_ul[k][sl] = here ? (int)(code - base) : -1;
-                  my_up[k][sl] = earlier ? code : -1;
-               }
-            slot++;
+            loc[local * NB + ii] = u;
          }
       }
       __syncwarp();
@@ -304,8 +376,11 @@ __global__ void __launch_bounds__(128) SweepKernel(const DevGeom<T> g, const Swe
       for (int k = 0; k < PL; k++)
          if (lane + 32 * k < ncell && my_lev[k] < 0) my_lev[k] = 0;
 
-      // Upwind values from earlier tasks that are stored already are folded
-      // in now, all loads in flight together; the rest are polled at their level
+      // A position whose upwind values from earlier tasks are all stored
+      // already has them folded in now, every load in flight together; the
+      // others poll at their level. Either way a cell subtracts its
+      // earlier-task couplings first, in slot order, then its in-task ones:
+      // the result does not depend on timing.
       bool hook = (t == s.unmet_task);
       if constexpr (PL <= 2) {
          if (!hook) {
@@ -319,29 +394,25 @@ __global__ void __launch_bounds__(128) SweepKernel(const DevGeom<T> g, const Swe
                      xn[k][sl][j] = my_up[k][sl] >= 0 ? LoadRelaxed(psi + ((int64_t)my_up[k][sl] * NB + j) * A + a) : T(0);
 #pragma unroll
             for (int k = 0; k < PL; k++) {
-               bool any = false;
+               bool any = false, ready = true;
+#pragma unroll
+               for (int sl = 0; sl < SM; sl++) {
+                  any |= my_up[k][sl] >= 0;
+#pragma unroll
+                  for (int j = 0; j < NB; j++) ready &= !(my_up[k][sl] >= 0 && IsSentinel(xn[k][sl][j]));
+               }
+               if (!(any && ready)) continue;
                T y[NB];
 #pragma unroll
-               for (int j = 0; j < NB; j++) y[j] = T(0);
+               for (int j = 0; j < NB; j++) y[j] = loc[my_local[k] * NB + j];
 #pragma unroll
                for (int sl = 0; sl < SM; sl++) {
                   if (my_up[k][sl] < 0) continue;
-                  bool ready = true;
-#pragma unroll
-                  for (int j = 0; j < NB; j++) ready &= !IsSentinel(xn[k][sl][j]);
-                  if (!ready) continue;
-                  if (!any) {
-#pragma unroll
-                     for (int j = 0; j < NB; j++) y[j] = loc[my_local[k] * NB + j];
-                     any = true;
-                  }
                   SubCoupling<T, NB>(G + ((size_t)(lane + 32 * k) * S + sl) * NB * NB, xn[k][sl], y);
                   my_up[k][sl] = -1;
                }
-               if (any) {
 #pragma unroll
-                  for (int j = 0; j < NB; j++) loc[my_local[k] * NB + j] = y[j];
-               }
+               for (int j = 0; j < NB; j++) loc[my_local[k] * NB + j] = y[j];
             }
          }
       }
@@ -360,22 +431,24 @@ __global__ void __launch_bounds__(128) SweepKernel(const DevGeom<T> g, const Swe
             for (int j = 0; j < NB; j++) y[j] = loc[local * NB + j];
 #pragma unroll
             for (int sl = 0; sl < SM; sl++) {
-               T xn[NB];
-               if (my_ul[k][sl] >= 0) {
-#pragma unroll
-                  for (int j = 0; j < NB; j++) xn[j] = loc[my_ul[k][sl] * NB + j];
-               } else if (my_up[k][sl] >= 0) {
-                  const T *src = psi + (int64_t)my_up[k][sl] * NB * A + a;
-                  int stride = A;
-                  if (hook) {
-                     src = never;  // test hook: this wait can never be met
-                     stride = 0;
-                     hook = false;
-                  }
-                  PollUpwind<T, NB>(src, stride, s, xn);
-               } else {
-                  continue;
+               if (my_up[k][sl] < 0) continue;
+               const T *src = psi + (int64_t)my_up[k][sl] * NB * A + a;
+               int stride = A;
+               if (hook) {
+                  src = never;  // test hook: this wait can never be met
+                  stride = 0;
+                  hook = false;
                }
+               T xn[NB];
+               PollUpwind<T, NB>(src, stride, s, xn);
+               SubCoupling<T, NB>(G + ((size_t)i * S + sl) * NB * NB, xn, y);
+            }
+#pragma unroll
+            for (int sl = 0; sl < SM; sl++) {
+               if (my_ul[k][sl] < 0) continue;
+               T xn[NB];
+#pragma unroll
+               for (int j = 0; j < NB; j++) xn[j] = loc[my_ul[k][sl] * NB + j];
                SubCoupling<T, NB>(G + ((size_t)i * S + sl) * NB * NB, xn, y);
             }
             const int64_t c = base + local;
@@ -416,11 +489,31 @@ int BuildSweepPlan(ubolt_ctx *ctx, int patch_size)
       return SetError(UBOLT_ERR_ARG, "a cell has %d upwind faces for one ordinate (at most %d)", h.max_inflow, ctx->F - 1);
    }
    plan->total_levels = (int64_t)h.lvl.size();
+   const int S = std::max(1, std::min(ctx->F - 1, (int)h.max_inflow));
+   plan->slots = S;
+   // The upwind link of every gathered face, in face order: the task's own
+   // cell (-2 - local) or a cell of an earlier task (its id)
+   std::vector<int32_t> tlink(h.tcell.size() * S, -1);
+   for (int64_t t = 0; t < h.n_tasks; t++) {
+      const int64_t base = (int64_t)(h.task_pa[t] / h.A) * h.P;
+      for (int64_t e = h.cell_ptr[t]; e < h.cell_ptr[t + 1]; e++) {
+         const int64_t c = base + h.tcell[e];
+         const uint32_t mask = h.tmask[e];
+         int slot = 0;
+         for (int f = 0; f < ctx->F; f++) {
+            const bool here = (mask >> f) & 1u, earlier = (mask >> (8 + f)) & 1u;
+            if (!(here || earlier)) continue;
+            const int32_t code = ctx->h_code[c * ctx->F + f];
+            tlink[e * S + slot++] = earlier ? code : (int32_t)(-2 - (code - base));
+         }
+      }
+   }
    int rc = 0;
    if ((rc = UploadVec(ctx, h.task_pa, &plan->task_pa)) || (rc = UploadVec(ctx, h.dep_ptr, &plan->dep_ptr)) ||
        (rc = UploadVec(ctx, h.deps, &plan->deps)) || (rc = UploadVec(ctx, h.cell_ptr, &plan->cell_ptr)) ||
        (rc = UploadVec(ctx, h.tcell, &plan->tcell)) || (rc = UploadVec(ctx, h.tmask, &plan->tmask)) ||
-       (rc = UploadVec(ctx, h.lvl_ptr, &plan->lvl_ptr)) || (rc = UploadVec(ctx, h.lvl, &plan->lvl))) {
+       (rc = UploadVec(ctx, h.lvl_ptr, &plan->lvl_ptr)) || (rc = UploadVec(ctx, h.lvl, &plan->lvl)) ||
+       (rc = UploadVec(ctx, tlink, &plan->tlink))) {
       delete plan;
       return rc;
    }
@@ -429,27 +522,14 @@ int BuildSweepPlan(ubolt_ctx *ctx, int patch_size)
    plan->ctrl = static_cast<uint32_t *>(p);
    cudaMemset(plan->ctrl, 0, kCtrlWords * sizeof(uint32_t));
    cudaMemset(plan->ctrl + kCtrlNever, 0xff, 2 * sizeof(uint32_t));
+   if (ctx->sweep) plan->fac_limit = ctx->sweep->fac_limit;
    delete ctx->sweep;
    ctx->sweep = plan;
    return CudaCheck(cudaDeviceSynchronize(), "sweep plan");
 }
 
-template <typename T, int NB, int F>
-static int LaunchSweep(ubolt_ctx *ctx, const T *q, T *psi, cudaStream_t st)
+static SweepDev DevPlan(const ubolt_sweep_plan *pl)
 {
-   ubolt_sweep_plan *pl = ctx->sweep;
-   const int threads = 32 * pl->warps_per_block;
-   const int slots = std::max(1, std::min(F - 1, (int)pl->max_inflow));
-   const size_t smem = (size_t)pl->warps_per_block * SweepSlice(pl->P, slots, NB, (int)sizeof(T)).bytes;
-   auto kern = pl->P <= 64 ? SweepKernel<T, NB, F, 2> : SweepKernel<T, NB, F, 8>;
-   if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-   int per_sm = 0, n_sm = 0, dev = 0;
-   cudaGetDevice(&dev);
-   cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
-   const int64_t want = (pl->n_tasks + pl->warps_per_block - 1) / pl->warps_per_block;
-   const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)std::max(per_sm, 1) * n_sm, want));
-   pl->grid = grid;
    SweepDev s;
    s.P = pl->P;
    s.A = pl->A;
@@ -458,17 +538,81 @@ static int LaunchSweep(ubolt_ctx *ctx, const T *q, T *psi, cudaStream_t st)
    s.cell_ptr = pl->cell_ptr;
    s.tcell = pl->tcell;
    s.tmask = pl->tmask;
+   s.tlink = pl->tlink;
    s.lvl_ptr = pl->lvl_ptr;
    s.lvl = pl->lvl;
    s.ctrl = pl->ctrl;
    s.spin_limit = pl->spin_limit;
+   s.unmet_task = -1;
+   s.slots = pl->slots;
+   return s;
+}
+
+// Bytes of the factor store for one precision
+static int64_t FactorBytes(const ubolt_ctx *ctx, const ubolt_sweep_plan *pl, size_t elem)
+{
+   return (int64_t)ctx->n_cells * ctx->A * ctx->nb * ctx->nb * (1 + pl->slots) * (int64_t)elem;
+}
+
+// The factor store for precision T, (re)built for the current group if it
+// fits the limit: by default a quarter of the free device memory, at most
+// 64 GiB. Returns the store, or nullptr to compute factors in the sweep.
+template <typename T, int NB, int F>
+static T *EnsureFactors(ubolt_ctx *ctx, cudaStream_t st)
+{
+   ubolt_sweep_plan *pl = ctx->sweep;
+   const int which = sizeof(T) == 8 ? 0 : 1;
+   if (pl->fac[which] && pl->fac_epoch[which] == ctx->group_epoch) return static_cast<T *>(pl->fac[which]);
+   const int64_t bytes = FactorBytes(ctx, pl, sizeof(T));
+   if (!pl->fac[which]) {
+      int64_t limit = pl->fac_limit;
+      if (limit < 0) {
+         size_t free_b = 0, total_b = 0;
+         if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return nullptr;
+         limit = std::min<int64_t>((int64_t)(free_b / 4), (int64_t)64 << 30);
+      }
+      if (bytes > limit) return nullptr;
+      void *p = nullptr;
+      if (cudaMalloc(&p, (size_t)bytes) != cudaSuccess) {
+         cudaGetLastError();
+         return nullptr;
+      }
+      pl->fac[which] = p;
+   }
+   int n_sm = 0, dev = 0;
+   cudaGetDevice(&dev);
+   cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+   const int64_t grid = std::min<int64_t>((pl->n_tasks + 3) / 4, (int64_t)n_sm * 16);
+   FactorKernel<T, NB, F><<<(int)grid, 128, 0, st>>>(ctx->geom<T>(), DevPlan(pl), static_cast<T *>(pl->fac[which]));
+   if (CheckLaunch("sweep factors")) return nullptr;
+   pl->fac_epoch[which] = ctx->group_epoch;
+   return static_cast<T *>(pl->fac[which]);
+}
+
+template <typename T, int NB, int F>
+static int LaunchSweep(ubolt_ctx *ctx, const T *q, T *psi, cudaStream_t st)
+{
+   ubolt_sweep_plan *pl = ctx->sweep;
+   const T *fac = EnsureFactors<T, NB, F>(ctx, st);
+   const int threads = 32 * pl->warps_per_block;
+   const size_t smem = (size_t)pl->warps_per_block * SweepSlice(pl->P, pl->slots, NB, (int)sizeof(T)).bytes;
+   auto kern = fac ? (pl->P <= 64 ? SweepKernel<T, NB, F, 2, true> : SweepKernel<T, NB, F, 8, true>)
+                   : (pl->P <= 64 ? SweepKernel<T, NB, F, 2, false> : SweepKernel<T, NB, F, 8, false>);
+   if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+   int per_sm = 0, n_sm = 0, dev = 0;
+   cudaGetDevice(&dev);
+   cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+   const int64_t want = (pl->n_tasks + pl->warps_per_block - 1) / pl->warps_per_block;
+   const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)std::max(per_sm, 1) * n_sm, want));
+   pl->grid = grid;
+   SweepDev s = DevPlan(pl);
    s.unmet_task = pl->unmet_task;
    pl->unmet_task = -1;
-   s.slots = slots;
    cudaMemsetAsync(pl->ctrl + kCtrlCounter, 0, sizeof(uint32_t), st);  // task counter; the error flag stays sticky
    // Every psi value starts as the sentinel: "not yet stored by its task"
    cudaMemsetAsync(psi, 0xff, (size_t)ctx->n_cells * NB * ctx->A * sizeof(T), st);
-   kern<<<grid, threads, smem, st>>>(ctx->geom<T>(), s, q, psi);
+   kern<<<grid, threads, smem, st>>>(ctx->geom<T>(), s, q, psi, fac);
    return CheckLaunch("sweep");
 }
 
@@ -523,6 +667,22 @@ extern "C" int ubolt_sweep_f32(ubolt_ctx *ctx, const float *q, float *psi, void 
    return Sweep<float>(ctx, q, psi, stream);
 }
 
+extern "C" int ubolt_sweep_set_factor_limit(ubolt_ctx *ctx, int64_t bytes)
+{
+   int rc = CheckReady(ctx, false);
+   if (rc) return rc;
+   if (!ctx->sweep && (rc = BuildSweepPlan(ctx, 0))) return rc;
+   ubolt_sweep_plan *pl = ctx->sweep;
+   pl->fac_limit = bytes;
+   for (int which = 0; which < 2; which++)
+      if (pl->fac[which] && bytes >= 0 && FactorBytes(ctx, pl, which ? 4 : 8) > bytes) {
+         cudaDeviceSynchronize();
+         cudaFree(pl->fac[which]);
+         pl->fac[which] = nullptr;
+      }
+   return UBOLT_OK;
+}
+
 extern "C" int ubolt_sweep_status(ubolt_ctx *ctx, ubolt_sweep_info *info, void *stream)
 {
    int rc = CheckReady(ctx, false);
@@ -543,6 +703,7 @@ extern "C" int ubolt_sweep_status(ubolt_ctx *ctx, ubolt_sweep_info *info, void *
       info->total_levels = pl->total_levels;
       info->grid = pl->grid;
       info->timeouts = h[1];
+      info->factor_bytes = (pl->fac[0] ? FactorBytes(ctx, pl, 8) : 0) + (pl->fac[1] ? FactorBytes(ctx, pl, 4) : 0);
    }
    if (h[0]) {
       cudaMemsetAsync(pl->ctrl + kCtrlError, 0, 2 * sizeof(uint32_t), s);

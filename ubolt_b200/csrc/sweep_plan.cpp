@@ -11,9 +11,8 @@
 // A cycle (possible on tetrahedra) is broken by releasing the waiting cell
 // with the fewest unresolved inputs; those inputs are lagged (read as zero).
 //
-// All ordinates' tasks are merged by depth (1 + the deepest upstream task),
-// which is topological for every ordinate, patch by patch within a depth,
-// and renumbered in that order.
+// All ordinates' tasks are merged by a modelled pickup time that is
+// topological for every ordinate (see kLevelCost), and renumbered in that order.
 #include "sweep_plan.h"
 
 #include "ubolt_internal.h"
@@ -33,8 +32,18 @@ struct AngleTask {
    std::vector<uint16_t> mask;
    std::vector<uint16_t> lvl;    // level ends
    std::vector<int32_t> deps;    // angle-local task ids
-   int32_t depth = 0;
+   double start = 0.0;           // modelled pickup time (see below)
 };
+
+// Launch order. The kernel walks a task level by level and each level waits
+// for its earlier-task inputs, so a task taken too early holds a warp while
+// it waits, and one taken too late delays everything downstream. Model the
+// walk at level granularity: a level takes kLevelCost, an input crossing
+// from another task kHopCost (both in level units); a task's pickup time is
+// the latest time at which none of its levels would wait. Tasks are numbered
+// by that time, raised above every upstream task's so the order stays
+// topological.
+constexpr double kLevelCost = 1.0, kHopCost = 6.0;
 
 }  // namespace
 
@@ -145,7 +154,6 @@ void BuildHostSweepPlan(int64_t nc, int F, int A, int P, const double *om, const
             }
             std::sort(T.deps.begin(), T.deps.end());
             T.deps.erase(std::unique(T.deps.begin(), T.deps.end()), T.deps.end());
-            for (int32_t d : T.deps) T.depth = std::max(T.depth, tasks[d].depth + 1);
          }
          if (done < nc) {
             // A cycle: release the waiting cell with the fewest unresolved inputs
@@ -153,6 +161,32 @@ void BuildHostSweepPlan(int64_t nc, int F, int A, int P, const double *om, const
             for (int64_t c = 0; c < nc; c++)
                if (!released[c] && (best < 0 || indeg[c] < indeg[best])) best = c;
             release(best);
+         }
+      }
+      // Modelled pickup times, tasks in (topological) creation order
+      {
+         std::vector<double> cfin(nc, 0.0);
+         for (auto &T : tasks) {
+            const int64_t base = (int64_t)T.patch * P;
+            double prev = -1e300, start = -1e300;
+            size_t lo = 0;
+            for (size_t L = 0; L < T.lvl.size(); L++) {
+               const size_t hi = T.lvl[L];
+               double ready = -1e300;
+               for (size_t i = lo; i < hi; i++) {
+                  const int64_t c = base + T.cells[i];
+                  for (int f = 0; f < F; f++)
+                     if ((T.mask[i] >> (8 + f)) & 1u) ready = std::max(ready, cfin[code[c * F + f]] + kHopCost);
+               }
+               start = std::max(start, ready - (double)L * kLevelCost);
+               const double end = std::max(prev, ready) + kLevelCost;
+               for (size_t i = lo; i < hi; i++) cfin[base + T.cells[i]] = end;
+               prev = end;
+               lo = hi;
+            }
+            start = std::max(start, 0.0);
+            for (int32_t d : T.deps) start = std::max(start, tasks[d].start + 1e-6);
+            T.start = start;
          }
       }
       // Patches solved in more than one task for this ordinate
@@ -165,12 +199,11 @@ void BuildHostSweepPlan(int64_t nc, int F, int A, int P, const double *om, const
    std::vector<std::pair<int32_t, int32_t>> all;  // (angle, angle-local id)
    for (int a = 0; a < A; a++)
       for (int32_t t = 0; t < (int32_t)per_angle[a].size(); t++) all.emplace_back(a, t);
-   // Within one depth, the tasks of one patch sit together (ordinates of one
-   // octant reach a patch at about the same depth), so warps taking
-   // consecutive tasks read that patch's geometry while it is in L2
+   // By modelled pickup time; ties (the same time) by patch, so warps taking
+   // consecutive tasks read that patch's data while it is in L2
    std::stable_sort(all.begin(), all.end(), [&](const auto &x, const auto &y) {
       const AngleTask &tx = per_angle[x.first][x.second], &ty = per_angle[y.first][y.second];
-      if (tx.depth != ty.depth) return tx.depth < ty.depth;
+      if (tx.start != ty.start) return tx.start < ty.start;
       if (tx.patch != ty.patch) return tx.patch < ty.patch;
       return x.first < y.first;
    });

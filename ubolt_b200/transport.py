@@ -179,9 +179,15 @@ class GroupTransfer:
 class Sweep:
     """psi = L^{-1} q for every ordinate - the streaming stage (PCAIR's place)."""
 
-    def __init__(self, ctx, patch_size=0):
+    def __init__(self, ctx, patch_size=0, factor_limit=None):
         self.ctx = ctx
         check(lib.ubolt_sweep_setup(ctx.handle, patch_size))
+        if factor_limit is not None:
+            self.set_factor_limit(factor_limit)
+
+    def set_factor_limit(self, nbytes):
+        """Cache each cell-ordinate's B^{-1} and couplings (-1 automatic, 0 never, else a byte limit)."""
+        check(lib.ubolt_sweep_set_factor_limit(self.ctx.handle, int(nbytes)))
 
     def apply(self, q, psi=None, stream=None):
         psi = torch.empty_like(q) if psi is None else psi
