@@ -42,20 +42,6 @@ __device__ __forceinline__ T WarpSum(T v)
    return v;
 }
 
-// Per-cell shape data as staged in shared memory: [nA F x 3][face_own
-// F x nb x nb][face_up F x nb x nb][grad phi nb x 3][1 / V], padded to 16 bytes
-template <typename T, int NB, int F>
-struct StagedShape {
-   static constexpr int nA = 0;
-   static constexpr int fown = nA + F * 3;
-   static constexpr int fup = fown + (NB > 1 ? F * NB * NB : 0);
-   static constexpr int bgrad = fup + (NB > 1 ? F * NB * NB : 0);
-   static constexpr int ivol = bgrad + (NB > 1 ? NB * 3 : 0);
-   static constexpr int raw = ivol + 1;
-   static constexpr int per16 = 16 / (int)sizeof(T);
-   static constexpr int size = (raw + per16 - 1) / per16 * per16;
-};
-
 // Two 256-thread blocks per SM at most 64 registers; the FP64 4 x 4 block
 // needs more and takes them
 template <typename T, int NB, int F>
@@ -64,11 +50,12 @@ constexpr int ApplyMinBlocks() { return (sizeof(T) == 8 && NB == 4) ? 1 : 2; }
 template <typename T, int NB, int F, bool SCATTER>
 __global__ void __launch_bounds__(512, ApplyMinBlocks<T, NB, F>()) ApplyKernel(const DevGeom<T> g, const T *__restrict__ x, T *__restrict__ y, int K)
 {
-   using L = StagedShape<T, NB, F>;
+   constexpr RecordLayout L(NB, F, (int)sizeof(T));
+   constexpr int U = L.size * (int)sizeof(T) / 16;  // 16-byte units per class record
    extern __shared__ __align__(16) unsigned char smem_raw[];
    const int A = g.A;
-   T *geo = reinterpret_cast<T *>(smem_raw);                   // [K][L::size]
-   T *xs = geo + K * L::size;                                   // [K][NB][A]
+   T *geo = reinterpret_cast<T *>(smem_raw);                   // [K][L.size]
+   T *xs = geo + K * L.size;                                    // [K][NB][A]
    T *mom = xs + K * NB * A;                                    // [K][NB]
    T *sig = mom + K * NB;                                       // [K][2]: sigma_t, sigma_s / W
    int32_t *codes = reinterpret_cast<int32_t *>(sig + 2 * K);  // [K][F]
@@ -77,37 +64,32 @@ __global__ void __launch_bounds__(512, ApplyMinBlocks<T, NB, F>()) ApplyKernel(c
    const int a = t - k * A;
    const int64_t c0 = (int64_t)blockIdx.x * K;
    const int kc = (int)min((int64_t)K, g.n_cells - c0);  // cells in this block
-   const int64_t c = c0 + k;
    const bool live = k < kc;
+   const T *xb = x + c0 * NB * A;  // this block's rows, then 32-bit offsets
+   T *yb = y + c0 * NB * A;
 
    // Round 1: own flux, face codes, cross sections; class ids -> shape data
    if (live) {
 #pragma unroll
-      for (int j = 0; j < NB; j++) xs[(k * NB + j) * A + a] = x[(c * NB + j) * A + a];
+      for (int j = 0; j < NB; j++) xs[(k * NB + j) * A + a] = xb[(k * NB + j) * A + a];
    }
    for (int e = t; e < kc * F; e += blockDim.x) codes[e] = g.code[c0 * F + e];
    for (int e = t; e < kc; e += blockDim.x) {
       sig[2 * e] = g.sigma_t[c0 + e];
       sig[2 * e + 1] = SCATTER ? g.sigma_s[c0 + e] * g.inv_sum_weights : T(0);
    }
-   for (int e = t; e < kc * L::raw; e += blockDim.x) {
-      const int kk = e / L::raw;
-      const int r = e - kk * L::raw;
+   for (int e = t; e < kc * U; e += blockDim.x) {
+      const int kk = e / U;
+      const int u = e - kk * U;
       const int64_t cl = g.cls[c0 + kk];
-      T v;
-      if (r < L::fown) v = g.nA[cl * (F * 3) + r];
-      else if (NB > 1 && r < L::fup) v = g.fown[cl * (F * NB * NB) + (r - L::fown)];
-      else if (NB > 1 && r < L::bgrad) v = g.fup[cl * (F * NB * NB) + (r - L::fup)];
-      else if (NB > 1 && r < L::ivol) v = g.bgrad[cl * (NB * 3) + (r - L::bgrad)];
-      else v = g.inv_vol[cl];
-      geo[kk * L::size + r] = v;
+      reinterpret_cast<int4 *>(geo)[kk * U + u] = reinterpret_cast<const int4 *>(g.rec)[cl * U + u];
    }
    __syncthreads();
 
    // Round 2: the upwind neighbours of this (cell, angle), loaded together
    // and folded in at once (inflow faces: the upwind neighbour, or the
    // mirrored angle here), so they hold no registers past this point
-   const T *gs = geo + k * L::size;
+   const T *gs = geo + k * L.size;
    T ox = T(0), oy = T(0), oz = T(0);
    T sf[F];
    T acc[NB];
@@ -118,7 +100,7 @@ __global__ void __launch_bounds__(512, ApplyMinBlocks<T, NB, F>()) ApplyKernel(c
       oy = g.omega[3 * a + 1];
       oz = g.omega[3 * a + 2];
 #pragma unroll
-      for (int f = 0; f < F; f++) sf[f] = Dot3(ox, oy, oz, gs + L::nA + 3 * f);
+      for (int f = 0; f < F; f++) sf[f] = Dot3(ox, oy, oz, gs + L.nA + 3 * f);
       // Faces in chunks of FC: every load of a chunk is in flight at once
       constexpr int FC = (F * NB <= 9) ? F : (F % 3 == 0 ? 3 : 2);
 #pragma unroll
@@ -128,8 +110,9 @@ __global__ void __launch_bounds__(512, ApplyMinBlocks<T, NB, F>()) ApplyKernel(c
       for (int ff = 0; ff < FC; ff++) {
          const int32_t code = codes[k * F + f0 + ff];
          const bool up = sf[f0 + ff] < T(0) && FaceInterior(code);
+         const T *xu = x + (size_t)(up ? code : 0) * (NB * A) + a;
 #pragma unroll
-         for (int j = 0; j < NB; j++) xn[ff][j] = up ? x[((int64_t)code * NB + j) * A + a] : T(0);
+         for (int j = 0; j < NB; j++) xn[ff][j] = up ? xu[j * A] : T(0);
       }
 #pragma unroll
       for (int ff = 0; ff < FC; ff++) {
@@ -144,9 +127,9 @@ __global__ void __launch_bounds__(512, ApplyMinBlocks<T, NB, F>()) ApplyKernel(c
             for (int j = 0; j < NB; j++) xn[ff][j] = xs[(k * NB + j) * A + ar];
          }
          if constexpr (NB == 1) {
-            acc[0] += sf[f] * gs[L::ivol] * xn[ff][0];
+            acc[0] += sf[f] * gs[L.ivol] * xn[ff][0];
          } else {
-            const T *M = gs + L::fup + f * NB * NB;
+            const T *M = gs + L.fup + f * NB * NB;
 #pragma unroll
             for (int i = 0; i < NB; i++) {
                T u = T(0);
@@ -177,7 +160,7 @@ __global__ void __launch_bounds__(512, ApplyMinBlocks<T, NB, F>()) ApplyKernel(c
 #pragma unroll
       for (int f = 0; f < F; f++)
          if (sf[f] > T(0)) out += sf[f];
-      acc[0] += (out * gs[L::ivol] + sig[2 * k]) * xs[k * A + a];
+      acc[0] += (out * gs[L.ivol] + sig[2 * k]) * xs[k * A + a];
    } else {
       T B[NB][NB];
 #pragma unroll
@@ -187,7 +170,7 @@ __global__ void __launch_bounds__(512, ApplyMinBlocks<T, NB, F>()) ApplyKernel(c
 #pragma unroll
       for (int f = 0; f < F; f++) {
          if (sf[f] > T(0)) {
-            const T *M = gs + L::fown + f * NB * NB;
+            const T *M = gs + L.fown + f * NB * NB;
 #pragma unroll
             for (int i = 0; i < NB; i++)
 #pragma unroll
@@ -195,7 +178,7 @@ __global__ void __launch_bounds__(512, ApplyMinBlocks<T, NB, F>()) ApplyKernel(c
          }
       }
 #pragma unroll
-      for (int i = 1; i < NB; i++) B[i][0] -= Dot3(ox, oy, oz, gs + L::bgrad + 3 * i);
+      for (int i = 1; i < NB; i++) B[i][0] -= Dot3(ox, oy, oz, gs + L.bgrad + 3 * i);
 #pragma unroll
       for (int i = 0; i < NB; i++) B[i][i] += sig[2 * k];
       T xo[NB];
@@ -214,7 +197,7 @@ __global__ void __launch_bounds__(512, ApplyMinBlocks<T, NB, F>()) ApplyKernel(c
       for (int i = 0; i < NB; i++) acc[i] -= mom[k * NB + i];
    }
 #pragma unroll
-   for (int i = 0; i < NB; i++) y[(c * NB + i) * A + a] = acc[i];
+   for (int i = 0; i < NB; i++) yb[(k * NB + i) * A + a] = acc[i];
 }
 
 // Column (c, j, a) of L - S: the own block transposed, the scatter's
@@ -350,7 +333,8 @@ int LaunchApply(const ubolt_ctx *ctx, const DevGeom<T> &g, const T *x, T *y, int
       const size_t smem = sizeof(T) * (size_t)(K * NB * g.A + K * NB);
       AdjointApplyKernel<T, NB, F><<<blocks, threads, smem, s>>>(g, x, y, K);
    } else {
-      const size_t smem = sizeof(T) * (size_t)K * (StagedShape<T, NB, F>::size + NB * g.A + NB + 2) + sizeof(int32_t) * K * F;
+      const size_t smem = sizeof(T) * (size_t)K * (RecordLayout(NB, F, (int)sizeof(T)).size + NB * g.A + NB + 2) +
+                          sizeof(int32_t) * K * F;
       if (mode == kFull) ApplyKernel<T, NB, F, true><<<blocks, threads, smem, s>>>(g, x, y, K);
       else ApplyKernel<T, NB, F, false><<<blocks, threads, smem, s>>>(g, x, y, K);
    }

@@ -24,6 +24,20 @@ constexpr int kMaxFaces = 6;
 __host__ __device__ inline bool FaceInterior(int32_t code) { return code >= 0; }
 __host__ __device__ inline int FaceSide(int32_t code) { return -1 - code; }
 
+// A geometry class packed as one record: [nA F x 3][face_own F x nb x nb]
+// [face_up F x nb x nb][grad phi nb x 3][1 / V], padded to 16 bytes (the
+// matrices and gradients only for nb > 1). Offsets in elements of `elem` bytes.
+struct RecordLayout {
+   int nA, fown, fup, bgrad, ivol, raw, size;
+   __host__ __device__ constexpr RecordLayout(int nb, int F, int elem)
+       : nA(0), fown(F * 3), fup(F * 3 + (nb > 1 ? F * nb * nb : 0)),
+         bgrad(F * 3 + (nb > 1 ? 2 * F * nb * nb : 0)), ivol(F * 3 + (nb > 1 ? 2 * F * nb * nb + nb * 3 : 0)),
+         raw(F * 3 + (nb > 1 ? 2 * F * nb * nb + nb * 3 : 0) + 1),
+         size((F * 3 + (nb > 1 ? 2 * F * nb * nb + nb * 3 : 0) + 1 + 16 / elem - 1) / (16 / elem) * (16 / elem))
+   {
+   }
+};
+
 template <typename T>
 struct DevGeom {
    int32_t dim, nb, F, A;
@@ -37,6 +51,7 @@ struct DevGeom {
    const T *bgrad;    // [class][nb][3]
    const T *fbv;      // [class][F][nb]
    const T *inv_vol;  // [class]
+   const T *rec;      // [class][RecordLayout(nb, F, sizeof(T)).size]: the same data packed per class
    // Per cell
    const int32_t *cls;     // [cell]
    const int32_t *code;    // [cell][F]

@@ -27,6 +27,9 @@ int BlockApply(ubolt_ctx *ctx, const T *x, T *y, bool trans, void *stream);
 template <typename T>
 int DsaCorrect(ubolt_ctx *ctx, const T *r, T *y, T *tmp, void *stream);
 bool SweepIsExact(ubolt_ctx *ctx);
+template <typename T>
+int SweepAffine(ubolt_ctx *ctx, const T *r0, const double *alpha, const double *phi, const double *rho, const T *u,
+                T *psi, void *stream);
 }  // namespace ubolt
 
 struct ubolt_solver {
@@ -374,32 +377,53 @@ __device__ __forceinline__ T WarpSumSolver(T v)
    return v;
 }
 
+// The node kernels below take nodes 8 lanes at a time, 4 per warp: each lane
+// strides a node's A ordinates by 8, so every load of a warp covers four
+// runs of 8 consecutive values (whole sectors), and the warp's four nodes are
+// summed with 3 shuffle steps. All lanes of a warp run the same iterations.
+constexpr int kLpn = 8;
+
+__device__ __forceinline__ double GroupSum(double v)
+{
+   v += __shfl_xor_sync(0xffffffffu, v, 4);
+   v += __shfl_xor_sync(0xffffffffu, v, 2);
+   v += __shfl_xor_sync(0xffffffffu, v, 1);
+   return v;
+}
+
 // rho(node) = R_u r0 (node) / kappa, and this block's share of |r0 - E_u rho|^2
 template <typename S>
 __global__ void __launch_bounds__(256) IsoSplitKernel(const S *__restrict__ r0, const S *__restrict__ u, int A,
                                                       int64_t n_nodes, double inv_kappa, double *__restrict__ rho,
                                                       double *__restrict__ partial)
 {
-   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+   const int lane = threadIdx.x & 31, sub = lane & (kLpn - 1);
+   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+   const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
    double acc = 0.0;
-   for (int64_t node = (int64_t)blockIdx.x * 8 + warp; node < n_nodes; node += (int64_t)gridDim.x * 8) {
+   for (int64_t nb0 = warp * 4; nb0 < n_nodes; nb0 += n_warps * 4) {
+      const int64_t node = nb0 + (lane >> 3);
+      const bool live = node < n_nodes;
       const S *rn = r0 + node * A;
       double sum = 0.0;
-      for (int a = lane; a < A; a += 32) sum += (u ? (double)u[a] : 1.0) * (double)rn[a];
-      const double rh = WarpSumSolver(sum) * inv_kappa;
-      if (lane == 0) rho[node] = rh;
-      for (int a = lane; a < A; a += 32) {
-         const double d = (double)rn[a] - (u ? (double)u[a] : 1.0) * rh;
-         acc += d * d;
+      if (live)
+         for (int a = sub; a < A; a += kLpn) sum += (u ? (double)u[a] : 1.0) * (double)rn[a];
+      const double rh = GroupSum(sum) * inv_kappa;
+      if (live) {
+         if (sub == 0) rho[node] = rh;
+         for (int a = sub; a < A; a += kLpn) {
+            const double d = (double)rn[a] - (u ? (double)u[a] : 1.0) * rh;
+            acc += d * d;
+         }
       }
    }
    __shared__ double red[8];
    acc = WarpSumSolver(acc);
-   if (lane == 0) red[warp] = acc;
+   if (lane == 0) red[threadIdx.x >> 5] = acc;
    __syncthreads();
    if (threadIdx.x == 0) {
       double t = 0.0;
-      for (int k = 0; k < 8; k++) t += red[k];
+      for (int k = 0; k < (int)(blockDim.x >> 5); k++) t += red[k];
       partial[blockIdx.x] = t;
    }
 }
@@ -411,11 +435,15 @@ __global__ void __launch_bounds__(256) IsoExpandKernel(const S *__restrict__ r0,
                                                        const S *__restrict__ u, int A, int64_t n_nodes,
                                                        S *__restrict__ t)
 {
-   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+   const int lane = threadIdx.x & 31, sub = lane & (kLpn - 1);
+   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+   const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
    const double al = *alpha_p;
-   for (int64_t node = (int64_t)blockIdx.x * 8 + warp; node < n_nodes; node += (int64_t)gridDim.x * 8) {
+   for (int64_t nb0 = warp * 4; nb0 < n_nodes; nb0 += n_warps * 4) {
+      const int64_t node = nb0 + (lane >> 3);
+      if (node >= n_nodes) continue;
       const double iso = phi[node] - al * rho[node];
-      for (int a = lane; a < A; a += 32)
+      for (int a = sub; a < A; a += kLpn)
          t[node * A + a] = (S)(al * (double)r0[node * A + a] + (u ? (double)u[a] : 1.0) * iso);
    }
 }
@@ -428,12 +456,17 @@ __global__ void __launch_bounds__(256) IsoScatterKernel(const S *__restrict__ z,
                                                         int64_t n_nodes, const double *__restrict__ phi_in,
                                                         double *__restrict__ phi_out)
 {
-   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-   for (int64_t node = (int64_t)blockIdx.x * 8 + warp; node < n_nodes; node += (int64_t)gridDim.x * 8) {
+   const int lane = threadIdx.x & 31, sub = lane & (kLpn - 1);
+   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+   const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+   for (int64_t nb0 = warp * 4; nb0 < n_nodes; nb0 += n_warps * 4) {
+      const int64_t node = nb0 + (lane >> 3);
+      const bool live = node < n_nodes;
       double sum = 0.0;
-      for (int a = lane; a < A; a += 32) sum += (w ? (double)w[a] : 1.0) * (double)z[node * A + a];
-      sum = WarpSumSolver(sum);
-      if (lane == 0) phi_out[node] = phi_in[node] - (double)sigma_s[node / nb] * inv_W * sum;
+      if (live)
+         for (int a = sub; a < A; a += kLpn) sum += (w ? (double)w[a] : 1.0) * (double)z[node * A + a];
+      sum = GroupSum(sum);
+      if (live && sub == 0) phi_out[node] = phi_in[node] - (double)sigma_s[node / nb] * inv_W * sum;
    }
 }
 
@@ -452,9 +485,21 @@ __global__ void IsoCombineKernel(double *__restrict__ d, double *__restrict__ al
    alpha[j1] = aw - upd;
 }
 
+// z = M^{-1} (alpha r_perp + E_u phi). The forward sweep forms its input as
+// it reads it; the adjoint's reversed-ordinate sweep takes it expanded in t.
+template <typename S>
+static int IsoPrecondition(ubolt_ctx *ctx, bool adjoint, const S *r0, const double *alpha, const double *phi,
+                           const double *rho, const S *u, S *t, S *z, S *tmp, int64_t n, int igrid, void *stream)
+{
+   if (!adjoint) return SweepAffine<S>(ctx, r0, alpha, phi, rho, u, z, stream);
+   IsoExpandKernel<S><<<igrid, 256, 0, (cudaStream_t)stream>>>(r0, alpha, phi, rho, u, ctx->A, ctx->n_nodes, t);
+   CountLaunch();
+   return Precondition<S>(ctx, UBOLT_PC_SWEEP, adjoint, t, z, tmp, n, stream);
+}
+
 static int IsoGrid(int64_t n_nodes)
 {
-   return (int)std::max<int64_t>(1, std::min<int64_t>((n_nodes + 7) / 8, 148 * 16));
+   return (int)std::max<int64_t>(1, std::min<int64_t>((n_nodes + 31) / 32, 148 * 16));
 }
 
 template <typename S>
@@ -520,9 +565,8 @@ static int GmresIso(ubolt_ctx *ctx, const ubolt_solver *ws, S *work, const S *b,
       for (; j < m && out->iterations < max_it; j++) {
          double *pj = Phi + (int64_t)j * nn, *pn = Phi + (int64_t)(j + 1) * nn;
          // w = v_j - E_u m(M^{-1} v_j): alpha_w = alpha_j, phi_w = phi_j - m
-         IsoExpandKernel<S><<<igrid, 256, 0, s>>>(r0, alpha + j, pj, ws->rho, u, A, nn, t);
-         CountLaunch();
-         if ((rc = Precondition<S>(ctx, UBOLT_PC_SWEEP, adjoint, t, z, tmp, n, stream))) return rc;
+         if ((rc = IsoPrecondition<S>(ctx, adjoint, r0, alpha + j, pj, ws->rho, u, t, z, tmp, n, igrid, stream)))
+            return rc;
          IsoScatterKernel<S><<<igrid, 256, 0, s>>>(z, wgt, sig_s, 1.0 / ctx->sum_weights, ctx->nb, A, nn, pj, pn);
          CountLaunch();
          cudaMemcpyAsync(alpha + j + 1, alpha + j, sizeof(double), cudaMemcpyDeviceToDevice, s);
@@ -580,9 +624,9 @@ static int GmresIso(ubolt_ctx *ctx, const ubolt_solver *ws, S *work, const S *b,
       cudaMemcpyAsync(dy, y.data(), j * sizeof(double), cudaMemcpyHostToDevice, s);
       cudaMemcpyAsync(scal + 2, &gamma, sizeof(double), cudaMemcpyHostToDevice, s);
       MultiAxpyKernel<double><<<igrid, 256, 0, s>>>(Phi, nn, j, dy, 1.0, ws->phiy, 0);
-      IsoExpandKernel<S><<<igrid, 256, 0, s>>>(r0, scal + 2, ws->phiy, ws->rho, u, A, nn, t);
-      CountLaunch(2);
-      if ((rc = Precondition<S>(ctx, UBOLT_PC_SWEEP, adjoint, t, z, tmp, n, stream))) return rc;
+      CountLaunch();
+      if ((rc = IsoPrecondition<S>(ctx, adjoint, r0, scal + 2, ws->phiy, ws->rho, u, t, z, tmp, n, igrid, stream)))
+         return rc;
       AxpyKernel<S, S><<<grid, 256, 0, s>>>(z, x, 1.0, n);
       CountLaunch();
       if (out->converged) break;

@@ -39,6 +39,8 @@
 // Words [kCtrlNever, kCtrlNever + 2) hold a sentinel nothing overwrites (the
 // target of the bounded-wait test hook).
 constexpr int kCtrlCounter = 0, kCtrlError = 32, kCtrlNever = 48, kCtrlWords = 64;
+constexpr int kSweepBlocksPerSm = 4;  // of 4 warps
+constexpr int kDefaultPatch = 32;
 
 struct ubolt_sweep_plan {
    int32_t P = 0, n_patches = 0, A = 0;
@@ -53,6 +55,7 @@ struct ubolt_sweep_plan {
    const uint16_t *tmask = nullptr;     // upwind faces: in task (bit f) / earlier task (bit 8 + f)
    const int32_t *lvl_ptr = nullptr;    // [n_tasks + 1]
    const uint16_t *lvl = nullptr;       // level end positions within the task
+   const uint16_t *tlev = nullptr;      // [entries] level of each entry within its task
    const int32_t *tlink = nullptr;      // [entries][slots] upwind link per gathered face: >= 0 the cell in an
                                         // earlier task, -2 - local for a cell of this task, -1 none
    uint32_t *ctrl = nullptr;            // [kCtrlCounter] task counter; [kCtrlError] error flag, [kCtrlError + 1] timeout count
@@ -124,6 +127,7 @@ struct SweepDev {
    const int64_t *cell_ptr;
    const uint8_t *tcell;
    const uint16_t *tmask;
+   const uint16_t *tlev;
    const int32_t *tlink;
    const int32_t *lvl_ptr;
    const uint16_t *lvl;
@@ -131,18 +135,22 @@ struct SweepDev {
    uint32_t spin_limit;
    int32_t slots;
    int64_t unmet_task;
+   // Affine input: when aff_alpha is set the sweep reads
+   // q(node, a) = alpha r0(node, a) + u_a (phi(node) - alpha rho(node)),
+   // u_a = aff_u[a] or 1, with r0 passed as q (compressed GMRES's Arnoldi vector)
+   const double *aff_alpha, *aff_phi, *aff_rho;
+   const void *aff_u;
 };
 
 // Per-warp shared-memory slice, for P cells and S gathered faces per cell
 struct SweepSlice {
-   size_t loc, G, lend, bytes;
+   size_t loc, G, bytes;
    __host__ __device__ SweepSlice(int P, int S, int NB, int elem)
    {
       auto up = [](size_t v) { return (v + 15) & ~(size_t)15; };
-      loc = 0;                                        // T [P][NB], by local cell
-      G = up(loc + (size_t)P * NB * elem);            // T [P][S][NB][NB], by position
-      lend = up(G + (size_t)P * S * NB * NB * elem);  // uint16 [P]: level end positions
-      bytes = up(lend + (size_t)P * 2);
+      loc = 0;                                 // T [P][NB], by local cell
+      G = up(loc + (size_t)P * NB * elem);     // T [P][S][NB][NB], by position
+      bytes = up(G + (size_t)P * S * NB * NB * elem);
    }
 };
 
@@ -290,23 +298,27 @@ __global__ void __launch_bounds__(128) SweepKernel(const DevGeom<T> g, const Swe
    unsigned char *slice = smem_raw + (size_t)warp * L.bytes;
    T *loc = reinterpret_cast<T *>(slice + L.loc);
    T *G = reinterpret_cast<T *>(slice + L.G);
-   uint16_t *lend = reinterpret_cast<uint16_t *>(slice + L.lend);
    const int A = s.A;
    const T *never = reinterpret_cast<const T *>(s.ctrl + kCtrlNever);
    const size_t R = (size_t)NB * NB * (1 + S);
-
+   // The task's five scalars, one lane each, in one round trip
+   auto scalars = [&](int64_t tt) -> int64_t {
+      if (tt >= s.n_tasks) return 0;
+      if (lane == 0) return s.task_pa[tt];
+      if (lane == 1) return s.cell_ptr[tt];
+      if (lane == 2) return s.cell_ptr[tt + 1];
+      if (lane == 3) return s.lvl_ptr[tt];
+      if (lane == 4) return s.lvl_ptr[tt + 1];
+      return 0;
+   };
    for (;;) {
+      // A task is claimed only when the warp is free: a task claimed while
+      // the warp still walks (and waits in) another would sit idle behind it
       int64_t t = 0;
       if (lane == 0) t = (int64_t)atomicAdd(&s.ctrl[kCtrlCounter], 1u);
       t = __shfl_sync(0xffffffffu, t, 0);
       if (t >= s.n_tasks) break;
-      // The task's five scalars, one lane each, in one round trip
-      int64_t v = 0;
-      if (lane == 0) v = s.task_pa[t];
-      else if (lane == 1) v = s.cell_ptr[t];
-      else if (lane == 2) v = s.cell_ptr[t + 1];
-      else if (lane == 3) v = s.lvl_ptr[t];
-      else if (lane == 4) v = s.lvl_ptr[t + 1];
+      const int64_t v = scalars(t);
       const int32_t pa = (int32_t)__shfl_sync(0xffffffffu, v, 0);
       const int64_t off = __shfl_sync(0xffffffffu, v, 1);
       const int ncell = (int)(__shfl_sync(0xffffffffu, v, 2) - off);
@@ -319,7 +331,6 @@ __global__ void __launch_bounds__(128) SweepKernel(const DevGeom<T> g, const Swe
       // Prologue - nothing here depends on upstream values: loc gets
       // y0 = B^{-1} q, G the couplings of the gathered faces, and each lane
       // its positions' schedule
-      for (int l = lane; l < nlev; l += 32) lend[l] = s.lvl[l0 + l];
       int my_local[PL], my_lev[PL], my_ul[PL][SM];
       int32_t my_up[PL][SM];
 #pragma unroll
@@ -335,6 +346,7 @@ __global__ void __launch_bounds__(128) SweepKernel(const DevGeom<T> g, const Swe
          if (i >= ncell) continue;
          const int local = s.tcell[off + i];
          my_local[k] = local;
+         my_lev[k] = s.tlev[off + i];
 #pragma unroll
          for (int sl = 0; sl < SM; sl++) {
             const int32_t lk = sl < S ? s.tlink[(off + i) * S + sl] : -1;
@@ -343,15 +355,31 @@ __global__ void __launch_bounds__(128) SweepKernel(const DevGeom<T> g, const Swe
          }
          const int64_t c = base + local;
          T r[NB], W[NB][NB];
+         if (s.aff_alpha) {
+            const double al = *s.aff_alpha;
+            const double ua = s.aff_u ? (double)static_cast<const T *>(s.aff_u)[a] : 1.0;
 #pragma unroll
-         for (int j = 0; j < NB; j++) r[j] = q[(c * NB + j) * A + a];
+            for (int j = 0; j < NB; j++) {
+               const int64_t node = c * NB + j;
+               r[j] = (T)(al * (double)q[node * A + a] + ua * (s.aff_phi[node] - al * s.aff_rho[node]));
+            }
+         } else {
+#pragma unroll
+            for (int j = 0; j < NB; j++) r[j] = q[(c * NB + j) * A + a];
+         }
          if constexpr (CACHED) {
             const T *ft = fac + (size_t)off * R + i;
 #pragma unroll
             for (int ii = 0; ii < NB; ii++)
 #pragma unroll
                for (int j = 0; j < NB; j++) W[ii][j] = ft[(size_t)(ii * NB + j) * ncell];
-            for (int e = 0; e < S * NB * NB; e++) G[(size_t)i * S * NB * NB + e] = ft[(size_t)(NB * NB + e) * ncell];
+            // Every coupling's loads in flight together, then to shared memory
+            T gv[SM * NB * NB];
+#pragma unroll
+            for (int e = 0; e < SM * NB * NB; e++) gv[e] = e < S * NB * NB ? ft[(size_t)(NB * NB + e) * ncell] : T(0);
+#pragma unroll
+            for (int e = 0; e < SM * NB * NB; e++)
+               if (e < S * NB * NB) G[(size_t)i * S * NB * NB + e] = gv[e];
          } else {
             const T om[3] = {g.omega[3 * a], g.omega[3 * a + 1], g.omega[3 * a + 2]};
             CellFactors<T, NB, F>(g, c, om, s.tmask[off + i], W, G + (size_t)i * S * NB * NB, (size_t)NB * NB, 1);
@@ -365,16 +393,6 @@ __global__ void __launch_bounds__(128) SweepKernel(const DevGeom<T> g, const Swe
          }
       }
       __syncwarp();
-      // The level of each owned position: the number of level ends at or before it
-      for (int l = 0; l < nlev; l++) {
-         const int e = lend[l];
-#pragma unroll
-         for (int k = 0; k < PL; k++)
-            if (lane + 32 * k < ncell && e <= lane + 32 * k) my_lev[k] = l + 1;
-      }
-#pragma unroll
-      for (int k = 0; k < PL; k++)
-         if (lane + 32 * k < ncell && my_lev[k] < 0) my_lev[k] = 0;
 
       // A position whose upwind values from earlier tasks are all stored
       // already has them folded in now, every load in flight together; the
@@ -468,7 +486,7 @@ __global__ void __launch_bounds__(128) SweepKernel(const DevGeom<T> g, const Swe
 int BuildSweepPlan(ubolt_ctx *ctx, int patch_size)
 {
    const int64_t nc = ctx->n_cells;
-   int P = patch_size > 0 ? patch_size : 64;
+   int P = patch_size > 0 ? patch_size : kDefaultPatch;
    if (P > 256) P = 256;
    if (P > nc) P = (int)nc;
    if (((nc + P - 1) / P) * (int64_t)ctx->A * 4 >= INT32_MAX) return SetError(UBOLT_ERR_ARG, "too many sweep tasks");
@@ -508,12 +526,18 @@ int BuildSweepPlan(ubolt_ctx *ctx, int patch_size)
          }
       }
    }
+   std::vector<uint16_t> tlev(h.tcell.size(), 0);
+   for (int64_t t = 0; t < h.n_tasks; t++) {
+      int64_t e = h.cell_ptr[t];
+      for (int32_t L = h.lvl_ptr[t]; L < h.lvl_ptr[t + 1]; L++)
+         for (; e < h.cell_ptr[t] + h.lvl[L]; e++) tlev[e] = (uint16_t)(L - h.lvl_ptr[t]);
+   }
    int rc = 0;
    if ((rc = UploadVec(ctx, h.task_pa, &plan->task_pa)) || (rc = UploadVec(ctx, h.dep_ptr, &plan->dep_ptr)) ||
        (rc = UploadVec(ctx, h.deps, &plan->deps)) || (rc = UploadVec(ctx, h.cell_ptr, &plan->cell_ptr)) ||
        (rc = UploadVec(ctx, h.tcell, &plan->tcell)) || (rc = UploadVec(ctx, h.tmask, &plan->tmask)) ||
        (rc = UploadVec(ctx, h.lvl_ptr, &plan->lvl_ptr)) || (rc = UploadVec(ctx, h.lvl, &plan->lvl)) ||
-       (rc = UploadVec(ctx, tlink, &plan->tlink))) {
+       (rc = UploadVec(ctx, tlink, &plan->tlink)) || (rc = UploadVec(ctx, tlev, &plan->tlev))) {
       delete plan;
       return rc;
    }
@@ -538,6 +562,7 @@ static SweepDev DevPlan(const ubolt_sweep_plan *pl)
    s.cell_ptr = pl->cell_ptr;
    s.tcell = pl->tcell;
    s.tmask = pl->tmask;
+   s.tlev = pl->tlev;
    s.tlink = pl->tlink;
    s.lvl_ptr = pl->lvl_ptr;
    s.lvl = pl->lvl;
@@ -545,6 +570,8 @@ static SweepDev DevPlan(const ubolt_sweep_plan *pl)
    s.spin_limit = pl->spin_limit;
    s.unmet_task = -1;
    s.slots = pl->slots;
+   s.aff_alpha = s.aff_phi = s.aff_rho = nullptr;
+   s.aff_u = nullptr;
    return s;
 }
 
@@ -590,23 +617,35 @@ static T *EnsureFactors(ubolt_ctx *ctx, cudaStream_t st)
 }
 
 template <typename T, int NB, int F>
-static int LaunchSweep(ubolt_ctx *ctx, const T *q, T *psi, cudaStream_t st)
+static int LaunchSweep(ubolt_ctx *ctx, const T *q, T *psi, cudaStream_t st, const SweepDev *affine = nullptr)
 {
    ubolt_sweep_plan *pl = ctx->sweep;
    const T *fac = EnsureFactors<T, NB, F>(ctx, st);
    const int threads = 32 * pl->warps_per_block;
    const size_t smem = (size_t)pl->warps_per_block * SweepSlice(pl->P, pl->slots, NB, (int)sizeof(T)).bytes;
-   auto kern = fac ? (pl->P <= 64 ? SweepKernel<T, NB, F, 2, true> : SweepKernel<T, NB, F, 8, true>)
-                   : (pl->P <= 64 ? SweepKernel<T, NB, F, 2, false> : SweepKernel<T, NB, F, 8, false>);
+   auto kern = fac ? (pl->P <= 32 ? SweepKernel<T, NB, F, 1, true>
+                                  : pl->P <= 64 ? SweepKernel<T, NB, F, 2, true> : SweepKernel<T, NB, F, 8, true>)
+                   : (pl->P <= 32 ? SweepKernel<T, NB, F, 1, false>
+                                  : pl->P <= 64 ? SweepKernel<T, NB, F, 2, false> : SweepKernel<T, NB, F, 8, false>);
    if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
    int per_sm = 0, n_sm = 0, dev = 0;
    cudaGetDevice(&dev);
    cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+   // More resident warps than the wavefront keeps busy only take tasks early
+   // and poll L2 while they wait, which slows the chain itself (measured:
+   // 16 warps per SM beat 20-36 at 256^2 DG1 S8, FP64 and FP32)
+   per_sm = std::min(per_sm, kSweepBlocksPerSm);
    const int64_t want = (pl->n_tasks + pl->warps_per_block - 1) / pl->warps_per_block;
    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)std::max(per_sm, 1) * n_sm, want));
    pl->grid = grid;
    SweepDev s = DevPlan(pl);
+   if (affine) {
+      s.aff_alpha = affine->aff_alpha;
+      s.aff_phi = affine->aff_phi;
+      s.aff_rho = affine->aff_rho;
+      s.aff_u = affine->aff_u;
+   }
    s.unmet_task = pl->unmet_task;
    pl->unmet_task = -1;
    cudaMemsetAsync(pl->ctrl + kCtrlCounter, 0, sizeof(uint32_t), st);  // task counter; the error flag stays sticky
@@ -636,6 +675,28 @@ bool SweepIsExact(ubolt_ctx *ctx)
    return ctx->sweep->n_lagged == 0 && !ctx->has_reflect;
 }
 
+// psi = L^{-1} (alpha r0 + E_u (phi - alpha rho)) with the input formed as
+// the sweep reads it (u = 1, or u_a = u[a]); alpha, phi, rho on the device
+template <typename T>
+int SweepAffine(ubolt_ctx *ctx, const T *r0, const double *alpha, const double *phi, const double *rho, const T *u,
+                T *psi, void *stream)
+{
+   int rc = CheckReady(ctx, true);
+   if (rc) return rc;
+   if (!ctx->sweep && (rc = BuildSweepPlan(ctx, 0))) return rc;
+   SweepDev aff{};
+   aff.aff_alpha = alpha;
+   aff.aff_phi = phi;
+   aff.aff_rho = rho;
+   aff.aff_u = u;
+   UBOLT_DISPATCH(ctx->nb, ctx->F, return (LaunchSweep<T, NB_, F_>(ctx, r0, psi, (cudaStream_t)stream, &aff)));
+   return SetError(UBOLT_ERR_STATE, "no sweep kernel for this shape");
+}
+
+template int SweepAffine<double>(ubolt_ctx *, const double *, const double *, const double *, const double *,
+                                 const double *, double *, void *);
+template int SweepAffine<float>(ubolt_ctx *, const float *, const double *, const double *, const double *,
+                                const float *, float *, void *);
 template int Sweep<double>(ubolt_ctx *, const double *, double *, void *);
 template int Sweep<float>(ubolt_ctx *, const float *, float *, void *);
 

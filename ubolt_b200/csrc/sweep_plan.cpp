@@ -265,7 +265,7 @@ extern "C" int ubolt_sweep_plan_build(const ubolt_dg_geometry *g, const ubolt_qu
    const int64_t nc = g->n_cells;
    if (patch_size < 0 || patch_size > 256) return SetError(UBOLT_ERR_ARG, "patch size %d (0..256)", patch_size);
    if (F > 8) return SetError(UBOLT_ERR_ARG, "at most 8 faces per cell");
-   int P = patch_size > 0 ? patch_size : 64;
+   int P = patch_size > 0 ? patch_size : 32;
    if (P > nc) P = (int)nc;
    std::vector<int32_t> code(nc * F);
    for (int64_t k = 0; k < nc * F; k++)
