@@ -23,7 +23,6 @@ all host cores, on the same workload; other ranks exit without work.
 import argparse
 import json
 import os
-import subprocess
 import sys
 import threading
 import time
@@ -62,50 +61,78 @@ def _peaks():
 
 
 class Clocks:
-    """nvidia-smi sampled every 200 ms while the timed region runs."""
+    """SM clock, power and clock-event reasons sampled through NVML every
+    10 ms while the timed region runs (read only; nothing is set)."""
 
     def __init__(self, index=0):
         self.index = index
         self.samples = []
-        self.proc = None
+        self.stop = threading.Event()
+        self.thread = None
 
     def __enter__(self):
-        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
-             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-             "clocks_event_reasons.sw_power_cap")
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
+            import pynvml as nv
+            nv.nvmlInit()
+            self.nv = nv
+            self.h = nv.nvmlDeviceGetHandleByIndex(self.index)
+            self.max_sm = nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM)
+            self.thread = threading.Thread(target=self._run, daemon=True)
             self.thread.start()
         except Exception:
-            self.proc = None
+            self.thread = None
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            parts = [x.strip() for x in line.split(",")]
-            if len(parts) >= 7:
-                self.samples.append(parts)
+    def _run(self):
+        nv = self.nv
+        while not self.stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+                reasons = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                power = nv.nvmlDeviceGetPowerUsage(self.h) / 1e3
+                self.samples.append((sm, reasons, power))
+            except Exception:
+                pass
+            self.stop.wait(0.01)
 
     def __exit__(self, *a):
-        if self.proc:
-            self.proc.terminate()
+        if self.thread:
+            self.stop.set()
+            self.thread.join(timeout=5)
             try:
-                self.proc.wait(timeout=5)
+                self.nv.nvmlShutdown()
             except Exception:
-                self.proc.kill()
+                pass
 
     def summary(self):
         if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
-        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i].lower() == "active"})
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.samples)}
+        nv = self.nv
+        bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+        reasons = sorted({k for _, r, _ in self.samples for k, b in bits.items() if r & b})
+        return {"sm_mhz": float(np.median([s for s, _, _ in self.samples])), "sm_max_mhz": float(self.max_sm),
+                "reasons": reasons, "samples": len(self.samples),
+                "power_w_median": float(np.median([p for _, _, p in self.samples]))}
+
+
+def max_over_ranks(v, world, device):
+    """The slowest rank's value (every rank takes part; world 1: v itself)."""
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_seconds_per_solve(ms_per_step, world):
+    """Replicas: each rank solves its own copy per step, so the job finishes
+    `world` solves per (slowest rank's) step: seconds per solve of the job."""
+    return ms_per_step / 1e3 / world
 
 
 def _dist():
@@ -216,12 +243,6 @@ def main():
         if world > 1:
             dist.barrier()
 
-    def max_over_ranks(v):
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
 
     prob = P.config_tri256(scale=args.scale)
     g, q = prob.geometry, prob.quad
@@ -262,8 +283,8 @@ def main():
     barrier()
     torch.cuda.synchronize()
     launches = (_lib.lib.ubolt_launch_count() - launches0)
-    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
-    value = ms / 1e3 / world if world > 1 else ms / 1e3
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world, "cuda")
+    value = replica_seconds_per_solve(ms, world)
     its = int(np.median([s["iterations"] for s in stats]))
     res = float(max(s["residual"] for s in stats))
 
@@ -297,9 +318,12 @@ def main():
         extra["apply_gbs"] = {"fp64": apply_bytes64 / t_apply64 / 1e6, "fp32": apply_bytes32 / t_apply32 / 1e6,
                               "fp64_us": t_apply64 * 1e3, "fp32_us": t_apply32 * 1e3}
         extra["sweep_us"] = {"fp64": t_sweep64 * 1e3, "fp32": t_sweep32 * 1e3}
-        # Dominant kernel of the solve: one sweep and one apply per iteration
-        sweeps = its + 1
-        dom_sweep = t_sweep64 * sweeps >= t_apply64 * (its + 1)
+        # Dominant kernel of the solve: one sweep per iteration; the full basis
+        # adds one apply per iteration and a sweep per cycle
+        compressed = stats[-1]["krylov"] == 2
+        sweeps = its if compressed else its + 1
+        applies = 2 if compressed else its + 1
+        dom_sweep = t_sweep64 * sweeps >= t_apply64 * applies
         peak, peak_kind = _peaks()
         if dom_sweep:
             ach = sweep_bytes64 / t_sweep64 / 1e6
@@ -316,7 +340,7 @@ def main():
                 traffic = None
         extra["roofline"] = {"bound": "hbm", "kernel": kernel, "achieved": ach, "peak": peak, "unit": "GB/s",
                              "frac": ach / peak, "peak_source": peak_kind, "traffic": traffic,
-                             "share_of_solve": (t_sweep64 * sweeps if dom_sweep else t_apply64 * (its + 1)) / ms}
+                             "share_of_solve": (t_sweep64 * sweeps if dom_sweep else t_apply64 * applies) / ms}
 
         # ~~~ Mixed precision: FP32 operator / sweep / Krylov storage + FP64 refinement
         mixed = T.TransportSolver(ctx, rtol=1e-8, precision="mixed", pc="sweep", restart=30, max_it=500,
@@ -395,7 +419,7 @@ def main():
         hx.copy_(x, non_blocking=True)
     f1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = max_over_ranks(f0.elapsed_time(f1) / args.steps)
+    e2e_ms = max_over_ranks(f0.elapsed_time(f1) / args.steps, world, "cuda")
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -50,10 +50,10 @@ struct ubolt_solver {
    double *partial = nullptr, *h = nullptr;
    int red_blocks = 0;
    // The compressed form (sweep preconditioner, exact sweep): node-space
-   // basis (restart + 1) x n_nodes, the residual's isotropic part, a node
-   // scratch, the basis scalars alpha[restart + 2] and four reduction slots
+   // basis (restart + 1) x n_nodes, the residual's isotropic part, the basis
+   // scalars alpha[restart + 2] and four reduction slots
    int64_t n_nodes = 0;
-   double *Phi = nullptr, *rho = nullptr, *phiy = nullptr, *alpha = nullptr, *scal = nullptr;
+   double *Phi = nullptr, *rho = nullptr, *alpha = nullptr, *scal = nullptr;
 };
 
 namespace ubolt {
@@ -519,8 +519,10 @@ static int GmresIso(ubolt_ctx *ctx, const ubolt_solver *ws, S *work, const S *b,
       for (double wa : ctx->h_w) kappa += wa * wa;
    else
       kappa = (double)A;
-   // Full-length vectors live in the (unused) plain basis: r0, t, z, tmp
-   S *r0 = work, *t = work + n, *z = work + 2 * n, *tmp = work + 3 * n;
+   // Full-length vectors live in the (unused) plain basis: r0, t, tmp, then
+   // the preconditioned vectors z_j = M^{-1} v_j of the cycle, kept so the
+   // update x += sum_j y_j z_j needs no further sweep
+   S *r0 = work, *t = work + n, *tmp = work + 2 * n, *Zb = work + 3 * n;
    double *Phi = ws->Phi, *alpha = ws->alpha, *scal = ws->scal;
    std::vector<double> H((size_t)(m + 1) * m, 0.0), cs(m), sn(m), gv(m + 1), y(m), h1(m + 1), h2(m + 2),
        alpha_h(m + 2, 0.0);
@@ -564,6 +566,7 @@ static int GmresIso(ubolt_ctx *ctx, const ubolt_solver *ws, S *work, const S *b,
       int j = 0;
       for (; j < m && out->iterations < max_it; j++) {
          double *pj = Phi + (int64_t)j * nn, *pn = Phi + (int64_t)(j + 1) * nn;
+         S *z = Zb + (int64_t)j * n;
          // w = v_j - E_u m(M^{-1} v_j): alpha_w = alpha_j, phi_w = phi_j - m
          if ((rc = IsoPrecondition<S>(ctx, adjoint, r0, alpha + j, pj, ws->rho, u, t, z, tmp, n, igrid, stream)))
             return rc;
@@ -613,21 +616,14 @@ static int GmresIso(ubolt_ctx *ctx, const ubolt_solver *ws, S *work, const S *b,
             break;
          }
       }
-      // x += M^{-1} (sum_i y_i v_i) = M^{-1} (gamma r_perp + E_u sum_i y_i phi_i)
+      // x += sum_i y_i z_i = M^{-1} (sum_i y_i v_i)
       for (int i = j - 1; i >= 0; i--) {
          double tt = gv[i];
          for (int k = i + 1; k < j; k++) tt -= H[i * m + k] * y[k];
          y[i] = tt / H[i * m + i];
       }
-      double gamma = 0.0;
-      for (int i = 0; i < j; i++) gamma += y[i] * alpha_h[i];
       cudaMemcpyAsync(dy, y.data(), j * sizeof(double), cudaMemcpyHostToDevice, s);
-      cudaMemcpyAsync(scal + 2, &gamma, sizeof(double), cudaMemcpyHostToDevice, s);
-      MultiAxpyKernel<double><<<igrid, 256, 0, s>>>(Phi, nn, j, dy, 1.0, ws->phiy, 0);
-      CountLaunch();
-      if ((rc = IsoPrecondition<S>(ctx, adjoint, r0, scal + 2, ws->phiy, ws->rho, u, t, z, tmp, n, igrid, stream)))
-         return rc;
-      AxpyKernel<S, S><<<grid, 256, 0, s>>>(z, x, 1.0, n);
+      MultiAxpyKernel<S><<<grid, 256, 0, s>>>(Zb, n, j, dy, 1.0, x, 1);
       CountLaunch();
       if (out->converged) break;
    }
@@ -641,7 +637,7 @@ static void FreeWorkspace(ubolt_ctx *ctx)
    cudaDeviceSynchronize();
    for (void *p : {(void *)ws->r, (void *)ws->z, (void *)ws->t, (void *)ws->V, (void *)ws->V32, (void *)ws->z32,
                    (void *)ws->b32, (void *)ws->t32, (void *)ws->d32, (void *)ws->Z, (void *)ws->Z32,
-                   (void *)ws->partial, (void *)ws->h, (void *)ws->Phi, (void *)ws->rho, (void *)ws->phiy,
+                   (void *)ws->partial, (void *)ws->h, (void *)ws->Phi, (void *)ws->rho,
                    (void *)ws->alpha, (void *)ws->scal})
       if (p) cudaFree(p);
    delete ws;
@@ -682,14 +678,17 @@ static int EnsureWorkspace(ubolt_ctx *ctx, const ubolt_solve_options *o)
       return rc;
    ws->n_nodes = ctx->n_nodes;
    if (!flexible && ((rc = alloc((void **)&ws->Phi, (size_t)(m + 1) * ws->n_nodes * 8)) ||
-                     (rc = alloc((void **)&ws->rho, ws->n_nodes * 8)) || (rc = alloc((void **)&ws->phiy, ws->n_nodes * 8)) ||
+                     (rc = alloc((void **)&ws->rho, ws->n_nodes * 8)) ||
                      (rc = alloc((void **)&ws->alpha, (size_t)(m + 2) * 8)) || (rc = alloc((void **)&ws->scal, 4 * 8))))
       return rc;
+   // The plain basis holds m + 1 vectors; the compressed form keeps r0, two
+   // scratch vectors and the cycle's m preconditioned vectors in the same space
+   const size_t nv = flexible ? (size_t)(m + 1) : (size_t)(m + 3);
    if (!mixed) {
-      if ((rc = alloc((void **)&ws->V, (size_t)(m + 1) * n * 8))) return rc;
+      if ((rc = alloc((void **)&ws->V, nv * n * 8))) return rc;
       if (flexible && (rc = alloc((void **)&ws->Z, (size_t)m * n * 8))) return rc;
    } else {
-      if ((rc = alloc((void **)&ws->V32, (size_t)(m + 1) * n * 4)) || (rc = alloc((void **)&ws->z32, n * 4)) ||
+      if ((rc = alloc((void **)&ws->V32, nv * n * 4)) || (rc = alloc((void **)&ws->z32, n * 4)) ||
           (rc = alloc((void **)&ws->b32, n * 4)) || (rc = alloc((void **)&ws->t32, n * 4)) ||
           (rc = alloc((void **)&ws->d32, n * 4)))
          return rc;
@@ -750,7 +749,7 @@ static int SolveSystem(ubolt_ctx *ctx, bool adjoint, const double *b, double *x,
    const auto t0 = std::chrono::steady_clock::now();
    // The compressed form wherever its identity holds: the exact sweep alone
    // as preconditioner, and room for its four full-length vectors
-   const bool iso = o.pc == UBOLT_PC_SWEEP && ws->restart >= 3 && ws->Phi && SweepIsExact(ctx) &&
+   const bool iso = o.pc == UBOLT_PC_SWEEP && ws->Phi && SweepIsExact(ctx) &&
                     o.krylov == UBOLT_KRYLOV_AUTO;
    if (o.x_zero) cudaMemsetAsync(x, 0, n * sizeof(double), s);
    const double bnorm = Norm<double>(ws, b, n, s, &rc);
