@@ -45,6 +45,9 @@ def _args():
     p.add_argument("--scale", type=float, default=1.0, help="mesh scale (1.0 = the named workload)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--quick", action="store_true", help="skip the secondary measurements")
+    p.add_argument("--workload", default="tri256", choices=["tri256", "hex128", "tet44"],
+                   help="tri256 is the headline line; hex128 (4 groups) and tet44 time the other solve configs")
+    p.add_argument("--restart", type=int, default=0, help="GMRES restart (0: 30, or 10 for hex128)")
     p.add_argument("--profile", default="", choices=["", "apply", "apply32", "sweep", "sweep32", "adjoint"],
                    help="run only this kernel, --warmup + --steps launches on the workload, for a profiler")
     return p.parse_args()
@@ -222,10 +225,57 @@ def profile_kernel(args, ctx, T, stream):
                       "us_per_launch": e0.elapsed_time(e1) / args.steps * 1e3}), flush=True)
 
 
+def run_workload(args):
+    """--workload hex128 | tet44: the other solve configs, FP64 and mixed, as one
+    JSON line each (no CPU baseline: the restatement would take hours here)."""
+    import torch
+    from ubolt_b200 import problem as P
+    from ubolt_b200 import transport as T
+    torch.cuda.set_device(0)
+    t0 = time.perf_counter()
+    prob = P.CONFIGS[args.workload](scale=args.scale)
+    ctx = T.Context(prob.geometry, prob.quad)
+    setup_s = time.perf_counter() - t0
+    restart = args.restart or (10 if args.workload == "hex128" else 30)
+    out = {"workload": prob.name, "cells": prob.geometry.n_cells, "ordinates": prob.quad.n_angles,
+           "n_basis": prob.geometry.n_basis, "groups": prob.n_groups, "rows_per_group": ctx.n_rows,
+           "restart": restart, "setup_s": setup_s}
+    phis = {}
+    for precision in ("fp64", "mixed"):
+        opts = dict(rtol=prob.rtol, precision=precision, pc="sweep", restart=restart, max_it=500)
+        stream = torch.cuda.current_stream()
+        for rep in range(1 + args.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            phi, stats = T.solve_groups(ctx, prob.sigma_t, prob.sigma_s, prob.source, **opts)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if rep == 0:
+                times = []
+                continue
+            times.append(e0.elapsed_time(e1) / 1e3)
+        phis[precision] = [p.clone() for p in phi]
+        out[precision] = {"s_per_solve": float(np.median(times)),
+                          "iterations": [s_["iterations"] for s_ in stats],
+                          "residual": max(s_["residual"] for s_ in stats),
+                          "krylov": [{1: "full", 2: "compressed"}.get(s_["krylov"]) for s_ in stats]}
+    err = max(float((m - f).norm() / f.norm()) for m, f in zip(phis["mixed"], phis["fp64"]))
+    out["mixed"]["phi_rel_err_vs_fp64"] = err
+    out["mixed"]["speedup_vs_fp64"] = out["fp64"]["s_per_solve"] / out["mixed"]["s_per_solve"]
+    sw = T.Sweep.__new__(T.Sweep)
+    sw.ctx = ctx
+    out["sweep"] = {k: v for k, v in sw.status().items() if k in ("n_tasks", "n_lagged", "n_split", "factor_bytes")}
+    print(json.dumps(out), flush=True)
+    ctx.close()
+
+
 def main():
     args = _args()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.workload != "tri256":
+        run_workload(args)
         return
     import torch
     import torch.distributed as dist

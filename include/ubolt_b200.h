@@ -249,7 +249,7 @@ int ubolt_sweep_f32(ubolt_ctx *ctx, const float *q, float *psi, void *stream);
  * q, built once per group (ubolt_set_group starts a new group) and read by
  * every sweep instead of being recomputed: n_cells A nb^2 (1 + slots)
  * values per precision, in task order. bytes < 0 (the default): build it
- * when it fits a quarter of the free device memory, at most 64 GiB; 0: never;
+ * when it fits half the free device memory, at most 96 GiB; 0: never;
  * otherwise the limit in bytes. Either way the result is the same, bit for
  * bit. Frees a store the new limit does not admit. */
 int ubolt_sweep_set_factor_limit(ubolt_ctx *ctx, int64_t bytes);

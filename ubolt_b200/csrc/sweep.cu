@@ -189,6 +189,15 @@ __device__ __forceinline__ void PollUpwind(const T *p, int stride, const SweepDe
    }
 }
 
+// An asynchronous global -> shared copy of one 4- or 8-byte word
+template <int BYTES>
+__device__ __forceinline__ void CpAsync(void *smem_dst, const void *src)
+{
+   const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+   asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(d), "l"(src), "n"(BYTES) : "memory");
+}
+__device__ __forceinline__ void CpAsyncWaitAll() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // y -= G x for one nb x nb coupling held in shared memory
 template <typename T, int NB>
 __device__ __forceinline__ void SubCoupling(const T *__restrict__ Gf, const T xn[NB], T y[NB])
@@ -333,28 +342,42 @@ __global__ void __launch_bounds__(128) SweepKernel(const DevGeom<T> g, const Swe
       // its positions' schedule
       int my_local[PL], my_lev[PL], my_ul[PL][SM];
       int32_t my_up[PL][SM];
+      // The schedule, and with the store every factor load of every owned
+      // position, issued before any is used (the couplings straight into
+      // shared memory by cp.async)
+      T W[CACHED ? PL : 1][NB][NB];
 #pragma unroll
       for (int k = 0; k < PL; k++) {
          const int i = lane + 32 * k;
-         my_local[k] = 0;
-         my_lev[k] = -1;
+         const bool valid = i < ncell;
+         my_local[k] = valid ? s.tcell[off + i] : 0;
+         my_lev[k] = valid ? s.tlev[off + i] : -1;
 #pragma unroll
          for (int sl = 0; sl < SM; sl++) {
-            my_ul[k][sl] = -1;
-            my_up[k][sl] = -1;
+            const int32_t lk = (valid && sl < S) ? s.tlink[(off + i) * S + sl] : -1;
+            my_up[k][sl] = lk >= 0 ? lk : -1;
+            my_ul[k][sl] = lk <= -2 ? -2 - lk : -1;
          }
+         if constexpr (CACHED) {
+            if (valid) {
+               const T *ft = fac + (size_t)off * R + i;
+#pragma unroll
+               for (int ii = 0; ii < NB; ii++)
+#pragma unroll
+                  for (int j = 0; j < NB; j++) W[k][ii][j] = ft[(size_t)(ii * NB + j) * ncell];
+#pragma unroll
+               for (int e = 0; e < SM * NB * NB; e++)
+                  if (e < S * NB * NB) CpAsync<sizeof(T)>(G + (size_t)i * S * NB * NB + e, ft + (size_t)(NB * NB + e) * ncell);
+            }
+         }
+      }
+#pragma unroll
+      for (int k = 0; k < PL; k++) {
+         const int i = lane + 32 * k;
          if (i >= ncell) continue;
-         const int local = s.tcell[off + i];
-         my_local[k] = local;
-         my_lev[k] = s.tlev[off + i];
-#pragma unroll
-         for (int sl = 0; sl < SM; sl++) {
-            const int32_t lk = sl < S ? s.tlink[(off + i) * S + sl] : -1;
-            if (lk >= 0) my_up[k][sl] = lk;
-            else if (lk <= -2) my_ul[k][sl] = -2 - lk;
-         }
+         const int local = my_local[k];
          const int64_t c = base + local;
-         T r[NB], W[NB][NB];
+         T r[NB];
          if (s.aff_alpha) {
             const double al = *s.aff_alpha;
             const double ua = s.aff_u ? (double)static_cast<const T *>(s.aff_u)[a] : 1.0;
@@ -367,31 +390,25 @@ __global__ void __launch_bounds__(128) SweepKernel(const DevGeom<T> g, const Swe
 #pragma unroll
             for (int j = 0; j < NB; j++) r[j] = q[(c * NB + j) * A + a];
          }
+         T Wk[NB][NB];
          if constexpr (CACHED) {
-            const T *ft = fac + (size_t)off * R + i;
 #pragma unroll
             for (int ii = 0; ii < NB; ii++)
 #pragma unroll
-               for (int j = 0; j < NB; j++) W[ii][j] = ft[(size_t)(ii * NB + j) * ncell];
-            // Every coupling's loads in flight together, then to shared memory
-            T gv[SM * NB * NB];
-#pragma unroll
-            for (int e = 0; e < SM * NB * NB; e++) gv[e] = e < S * NB * NB ? ft[(size_t)(NB * NB + e) * ncell] : T(0);
-#pragma unroll
-            for (int e = 0; e < SM * NB * NB; e++)
-               if (e < S * NB * NB) G[(size_t)i * S * NB * NB + e] = gv[e];
+               for (int j = 0; j < NB; j++) Wk[ii][j] = W[k][ii][j];
          } else {
             const T om[3] = {g.omega[3 * a], g.omega[3 * a + 1], g.omega[3 * a + 2]};
-            CellFactors<T, NB, F>(g, c, om, s.tmask[off + i], W, G + (size_t)i * S * NB * NB, (size_t)NB * NB, 1);
+            CellFactors<T, NB, F>(g, c, om, s.tmask[off + i], Wk, G + (size_t)i * S * NB * NB, (size_t)NB * NB, 1);
          }
 #pragma unroll
          for (int ii = 0; ii < NB; ii++) {
             T u = T(0);
 #pragma unroll
-            for (int j = 0; j < NB; j++) u += W[ii][j] * r[j];
+            for (int j = 0; j < NB; j++) u += Wk[ii][j] * r[j];
             loc[local * NB + ii] = u;
          }
       }
+      if constexpr (CACHED) CpAsyncWaitAll();
       __syncwarp();
 
       // A position whose upwind values from earlier tasks are all stored
@@ -582,8 +599,9 @@ static int64_t FactorBytes(const ubolt_ctx *ctx, const ubolt_sweep_plan *pl, siz
 }
 
 // The factor store for precision T, (re)built for the current group if it
-// fits the limit: by default a quarter of the free device memory, at most
-// 64 GiB. Returns the store, or nullptr to compute factors in the sweep.
+// fits the limit: by default half the free device memory (the solver's
+// workspace is allocated before its first sweep), at most 96 GiB. Returns
+// the store, or nullptr to compute factors in the sweep.
 template <typename T, int NB, int F>
 static T *EnsureFactors(ubolt_ctx *ctx, cudaStream_t st)
 {
@@ -596,7 +614,7 @@ static T *EnsureFactors(ubolt_ctx *ctx, cudaStream_t st)
       if (limit < 0) {
          size_t free_b = 0, total_b = 0;
          if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return nullptr;
-         limit = std::min<int64_t>((int64_t)(free_b / 4), (int64_t)64 << 30);
+         limit = std::min<int64_t>((int64_t)(free_b / 2), (int64_t)96 << 30);
       }
       if (bytes > limit) return nullptr;
       void *p = nullptr;
