@@ -231,7 +231,7 @@ typedef struct {
    int64_t factor_bytes;  /* device bytes held by the factor stores (FP64 + FP32) */
 } ubolt_sweep_info;
 
-/* Build the sweep plan: patches of patch_size consecutive cells (0 picks 32;
+/* Build the sweep plan: patches of patch_size consecutive cells (0 picks 64;
  * at most 256), per-ordinate upwind orders, task list. Host
  * work plus one upload; independent of the group. Called by the first sweep
  * if not before. The streaming stage of the preconditioner, in place of

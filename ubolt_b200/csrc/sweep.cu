@@ -40,7 +40,7 @@
 // target of the bounded-wait test hook).
 constexpr int kCtrlCounter = 0, kCtrlError = 32, kCtrlNever = 48, kCtrlWords = 64;
 constexpr int kSweepBlocksPerSm = 4;  // of 4 warps
-constexpr int kDefaultPatch = 32;
+constexpr int kDefaultPatch = 64;
 
 struct ubolt_sweep_plan {
    int32_t P = 0, n_patches = 0, A = 0;

@@ -43,7 +43,7 @@ struct AngleTask {
 // the latest time at which none of its levels would wait. Tasks are numbered
 // by that time, raised above every upstream task's so the order stays
 // topological.
-constexpr double kLevelCost = 1.0, kHopCost = 6.0;
+constexpr double kLevelCost = 1.0, kHopCost = 4.0;
 
 }  // namespace
 
@@ -163,12 +163,53 @@ void BuildHostSweepPlan(int64_t nc, int F, int A, int P, const double *om, const
             release(best);
          }
       }
+      // Levels by modelled finish time. A task's walk is level-synchronous,
+      // so a cell whose earlier-task input is late holds up every later
+      // level. Model each cell's finish: an in-task upwind input adds
+      // kLevelCost, an earlier-task one kHopCost; then order each task's
+      // cells by that time (ties keep the upwind level order) and start a
+      // new level wherever it changes. An in-task upwind cell finishes
+      // strictly earlier, so it still sits at a lower level.
+      {
+         std::vector<double> cf(nc, 0.0), tcf;
+         std::vector<int32_t> idx;
+         std::vector<uint8_t> cells;
+         std::vector<uint16_t> mask;
+         for (auto &T : tasks) {
+            const int64_t base = (int64_t)T.patch * P;
+            const size_t n = T.cells.size();
+            tcf.assign(n, 0.0);
+            for (size_t i = 0; i < n; i++) {
+               const int64_t c = base + T.cells[i];
+               double r = kLevelCost;
+               for (int f = 0; f < F; f++) {
+                  if ((T.mask[i] >> f) & 1u) r = std::max(r, cf[code[c * F + f]] + kLevelCost);
+                  else if ((T.mask[i] >> (8 + f)) & 1u) r = std::max(r, cf[code[c * F + f]] + kHopCost);
+               }
+               cf[c] = r;
+               tcf[i] = r;
+            }
+            idx.resize(n);
+            std::iota(idx.begin(), idx.end(), 0);
+            std::stable_sort(idx.begin(), idx.end(), [&](int32_t x, int32_t y) { return tcf[x] < tcf[y]; });
+            cells.resize(n);
+            mask.resize(n);
+            T.lvl.clear();
+            for (size_t i = 0; i < n; i++) {
+               cells[i] = T.cells[idx[i]];
+               mask[i] = T.mask[idx[i]];
+               if (i + 1 == n || tcf[idx[i + 1]] != tcf[idx[i]]) T.lvl.push_back((uint16_t)(i + 1));
+            }
+            T.cells.swap(cells);
+            T.mask.swap(mask);
+         }
+      }
       // Modelled pickup times, tasks in (topological) creation order
       {
          std::vector<double> cfin(nc, 0.0);
          for (auto &T : tasks) {
             const int64_t base = (int64_t)T.patch * P;
-            double prev = -1e300, start = -1e300;
+            double prev = 0.0, start = -1e300;
             size_t lo = 0;
             for (size_t L = 0; L < T.lvl.size(); L++) {
                const size_t hi = T.lvl[L];
@@ -265,7 +306,7 @@ extern "C" int ubolt_sweep_plan_build(const ubolt_dg_geometry *g, const ubolt_qu
    const int64_t nc = g->n_cells;
    if (patch_size < 0 || patch_size > 256) return SetError(UBOLT_ERR_ARG, "patch size %d (0..256)", patch_size);
    if (F > 8) return SetError(UBOLT_ERR_ARG, "at most 8 faces per cell");
-   int P = patch_size > 0 ? patch_size : 32;
+   int P = patch_size > 0 ? patch_size : 64;
    if (P > nc) P = (int)nc;
    std::vector<int32_t> code(nc * F);
    for (int64_t k = 0; k < nc * F; k++)
