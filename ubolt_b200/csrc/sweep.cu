@@ -39,7 +39,7 @@
 // Words [kCtrlNever, kCtrlNever + 2) hold a sentinel nothing overwrites (the
 // target of the bounded-wait test hook).
 constexpr int kCtrlCounter = 0, kCtrlError = 32, kCtrlNever = 48, kCtrlWords = 64;
-constexpr int kSweepBlocksPerSm = 4;  // of 4 warps
+constexpr int kSweepBlocksPerSm = 8;  // of 4 warps
 constexpr int kDefaultPatch = 64;
 
 struct ubolt_sweep_plan {
@@ -115,6 +115,12 @@ __device__ __forceinline__ void StoreRelaxed(float *p, float v)
 }
 __device__ __forceinline__ bool IsSentinel(double v) { return __double_as_longlong(v) == -1LL; }
 __device__ __forceinline__ bool IsSentinel(float v) { return __float_as_int(v) == -1; }
+template <typename T>
+__device__ __forceinline__ T Sentinel();
+template <>
+__device__ __forceinline__ double Sentinel<double>() { return __longlong_as_double(-1LL); }
+template <>
+__device__ __forceinline__ float Sentinel<float>() { return __int_as_float(-1); }
 // A computed value equal to the sentinel (a NaN carrying its payload) is
 // stored as another NaN, so a reader can never mistake a result for "not yet"
 __device__ __forceinline__ double Publishable(double v) { return IsSentinel(v) ? __longlong_as_double(0x7ff8000000000001LL) : v; }
@@ -294,8 +300,14 @@ __global__ void __launch_bounds__(128) FactorKernel(const DevGeom<T> g, const Sw
 // PL: positions per lane, P <= 32 PL. Lane l owns positions l, l + 32, ...;
 // its cells' schedule (local index, level, upwind links) stays in registers.
 // CACHED: the factors come from the store, else they are computed here.
+// Resident blocks of 4 warps the compiler should fit per SM: the sweep is
+// bound by per-task latency, and FP64 nb <= 3 with one cell per lane fits a
+// fifth block without spilling (with two, the spills cost more than the block)
+template <typename T, int NB, int PL>
+constexpr int SweepMinBlocks() { return (sizeof(T) == 8 && NB <= 3 && PL == 1) ? 5 : 1; }
+
 template <typename T, int NB, int F, int PL, bool CACHED>
-__global__ void __launch_bounds__(128) SweepKernel(const DevGeom<T> g, const SweepDev s, const T *__restrict__ q,
+__global__ void __launch_bounds__(128, SweepMinBlocks<T, NB, PL>()) SweepKernel(const DevGeom<T> g, const SweepDev s, const T *__restrict__ q,
                                                    T *__restrict__ psi, const T *__restrict__ fac)
 {
    extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -344,8 +356,13 @@ __global__ void __launch_bounds__(128) SweepKernel(const DevGeom<T> g, const Swe
       int32_t my_up[PL][SM];
       // The schedule, and with the store every factor load of every owned
       // position, issued before any is used (the couplings straight into
-      // shared memory by cp.async)
-      T W[CACHED ? PL : 1][NB][NB];
+      // shared memory by cp.async); with the links in hand, the upwind values
+      // of earlier tasks are loaded in the same round as q
+      constexpr bool kPreloadW = CACHED && PL <= 2;  // more positions: loaded where used
+      constexpr bool kPrefetch = PL <= 2;
+      T W[kPreloadW ? PL : 1][NB][NB];
+      T xp[kPrefetch ? PL : 1][SM][NB];
+      const bool hook = (t == s.unmet_task);
 #pragma unroll
       for (int k = 0; k < PL; k++) {
          const int i = lane + 32 * k;
@@ -361,14 +378,24 @@ __global__ void __launch_bounds__(128) SweepKernel(const DevGeom<T> g, const Swe
          if constexpr (CACHED) {
             if (valid) {
                const T *ft = fac + (size_t)off * R + i;
+               if constexpr (kPreloadW) {
 #pragma unroll
-               for (int ii = 0; ii < NB; ii++)
+                  for (int ii = 0; ii < NB; ii++)
 #pragma unroll
-                  for (int j = 0; j < NB; j++) W[k][ii][j] = ft[(size_t)(ii * NB + j) * ncell];
+                     for (int j = 0; j < NB; j++) W[k][ii][j] = ft[(size_t)(ii * NB + j) * ncell];
+               }
 #pragma unroll
                for (int e = 0; e < SM * NB * NB; e++)
                   if (e < S * NB * NB) CpAsync<sizeof(T)>(G + (size_t)i * S * NB * NB + e, ft + (size_t)(NB * NB + e) * ncell);
             }
+         }
+         if constexpr (kPrefetch) {
+#pragma unroll
+            for (int sl = 0; sl < SM; sl++)
+#pragma unroll
+               for (int j = 0; j < NB; j++)
+                  xp[k][sl][j] = (my_up[k][sl] >= 0 && !hook) ? LoadRelaxed(psi + ((int64_t)my_up[k][sl] * NB + j) * A + a)
+                                                             : Sentinel<T>();
          }
       }
 #pragma unroll
@@ -391,67 +418,58 @@ __global__ void __launch_bounds__(128) SweepKernel(const DevGeom<T> g, const Swe
             for (int j = 0; j < NB; j++) r[j] = q[(c * NB + j) * A + a];
          }
          T Wk[NB][NB];
-         if constexpr (CACHED) {
+         if constexpr (kPreloadW) {
 #pragma unroll
             for (int ii = 0; ii < NB; ii++)
 #pragma unroll
                for (int j = 0; j < NB; j++) Wk[ii][j] = W[k][ii][j];
+         } else if constexpr (CACHED) {
+            const T *ft = fac + (size_t)off * R + i;
+#pragma unroll
+            for (int ii = 0; ii < NB; ii++)
+#pragma unroll
+               for (int j = 0; j < NB; j++) Wk[ii][j] = ft[(size_t)(ii * NB + j) * ncell];
          } else {
             const T om[3] = {g.omega[3 * a], g.omega[3 * a + 1], g.omega[3 * a + 2]};
             CellFactors<T, NB, F>(g, c, om, s.tmask[off + i], Wk, G + (size_t)i * S * NB * NB, (size_t)NB * NB, 1);
          }
+         T y[NB];
 #pragma unroll
          for (int ii = 0; ii < NB; ii++) {
             T u = T(0);
 #pragma unroll
             for (int j = 0; j < NB; j++) u += Wk[ii][j] * r[j];
-            loc[local * NB + ii] = u;
+            y[ii] = u;
          }
-      }
-      if constexpr (CACHED) CpAsyncWaitAll();
-      __syncwarp();
-
-      // A position whose upwind values from earlier tasks are all stored
-      // already has them folded in now, every load in flight together; the
-      // others poll at their level. Either way a cell subtracts its
-      // earlier-task couplings first, in slot order, then its in-task ones:
-      // the result does not depend on timing.
-      bool hook = (t == s.unmet_task);
-      if constexpr (PL <= 2) {
-         if (!hook) {
-            T xn[PL][SM][NB];
+         // A position whose upwind values from earlier tasks are all stored
+         // already has them folded in now; the others poll at their level.
+         // Either way a cell subtracts its earlier-task couplings first, in
+         // slot order, then its in-task ones: the result does not depend on
+         // timing.
+         if constexpr (kPrefetch) {
+            bool any = false, ready = true;
 #pragma unroll
-            for (int k = 0; k < PL; k++)
+            for (int sl = 0; sl < SM; sl++) {
+               any |= my_up[k][sl] >= 0;
 #pragma unroll
-               for (int sl = 0; sl < SM; sl++)
-#pragma unroll
-                  for (int j = 0; j < NB; j++)
-                     xn[k][sl][j] = my_up[k][sl] >= 0 ? LoadRelaxed(psi + ((int64_t)my_up[k][sl] * NB + j) * A + a) : T(0);
-#pragma unroll
-            for (int k = 0; k < PL; k++) {
-               bool any = false, ready = true;
-#pragma unroll
-               for (int sl = 0; sl < SM; sl++) {
-                  any |= my_up[k][sl] >= 0;
-#pragma unroll
-                  for (int j = 0; j < NB; j++) ready &= !(my_up[k][sl] >= 0 && IsSentinel(xn[k][sl][j]));
-               }
-               if (!(any && ready)) continue;
-               T y[NB];
-#pragma unroll
-               for (int j = 0; j < NB; j++) y[j] = loc[my_local[k] * NB + j];
+               for (int j = 0; j < NB; j++) ready &= !(my_up[k][sl] >= 0 && IsSentinel(xp[k][sl][j]));
+            }
+            if (any && ready) {
+               if constexpr (CACHED) CpAsyncWaitAll();  // this lane's couplings
 #pragma unroll
                for (int sl = 0; sl < SM; sl++) {
                   if (my_up[k][sl] < 0) continue;
-                  SubCoupling<T, NB>(G + ((size_t)(lane + 32 * k) * S + sl) * NB * NB, xn[k][sl], y);
+                  SubCoupling<T, NB>(G + ((size_t)i * S + sl) * NB * NB, xp[k][sl], y);
                   my_up[k][sl] = -1;
                }
-#pragma unroll
-               for (int j = 0; j < NB; j++) loc[my_local[k] * NB + j] = y[j];
             }
          }
+#pragma unroll
+         for (int ii = 0; ii < NB; ii++) loc[local * NB + ii] = y[ii];
       }
+      if constexpr (CACHED) CpAsyncWaitAll();
       __syncwarp();
+      bool hook_left = hook;
 
       // Level by level: psi_c = y0 - sum_f G_f psi(up_f), an in-task
       // neighbour from shared memory, an earlier task's polled from L2
@@ -469,10 +487,10 @@ __global__ void __launch_bounds__(128) SweepKernel(const DevGeom<T> g, const Swe
                if (my_up[k][sl] < 0) continue;
                const T *src = psi + (int64_t)my_up[k][sl] * NB * A + a;
                int stride = A;
-               if (hook) {
+               if (hook_left) {
                   src = never;  // test hook: this wait can never be met
                   stride = 0;
-                  hook = false;
+                  hook_left = false;
                }
                T xn[NB];
                PollUpwind<T, NB>(src, stride, s, xn);
@@ -650,9 +668,8 @@ static int LaunchSweep(ubolt_ctx *ctx, const T *q, T *psi, cudaStream_t st, cons
    cudaGetDevice(&dev);
    cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
-   // More resident warps than the wavefront keeps busy only take tasks early
-   // and poll L2 while they wait, which slows the chain itself (measured:
-   // 16 warps per SM beat 20-36 at 256^2 DG1 S8, FP64 and FP32)
+   // At most 32 warps per SM: beyond the throughput the wavefront can use,
+   // more resident warps only take tasks early and wait
    per_sm = std::min(per_sm, kSweepBlocksPerSm);
    const int64_t want = (pl->n_tasks + pl->warps_per_block - 1) / pl->warps_per_block;
    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)std::max(per_sm, 1) * n_sm, want));
