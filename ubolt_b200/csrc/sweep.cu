@@ -149,14 +149,18 @@ struct SweepDev {
 };
 
 // Per-warp shared-memory slice, for P cells and S gathered faces per cell
+// Each nb x nb coupling in shared memory takes a 16-byte multiple, so the
+// walk reads it with 16-byte loads
+__host__ __device__ constexpr int GStride(int NB, int elem) { return (NB * NB * elem + 15) / 16 * 16 / elem; }
+
 struct SweepSlice {
    size_t loc, G, bytes;
    __host__ __device__ SweepSlice(int P, int S, int NB, int elem)
    {
       auto up = [](size_t v) { return (v + 15) & ~(size_t)15; };
-      loc = 0;                                 // T [P][NB], by local cell
-      G = up(loc + (size_t)P * NB * elem);     // T [P][S][NB][NB], by position
-      bytes = up(G + (size_t)P * S * NB * NB * elem);
+      loc = 0;                                           // T [P][NB], by local cell
+      G = up(loc + (size_t)P * NB * elem);               // T [P][S][GStride], by position
+      bytes = up(G + (size_t)P * S * GStride(NB, elem) * elem);
    }
 };
 
@@ -204,15 +208,33 @@ __device__ __forceinline__ void CpAsync(void *smem_dst, const void *src)
 }
 __device__ __forceinline__ void CpAsyncWaitAll() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-// y -= G x for one nb x nb coupling held in shared memory
+// y -= G x for one nb x nb coupling held in shared memory (16-byte aligned,
+// GStride elements), read with 16-byte loads
 template <typename T, int NB>
 __device__ __forceinline__ void SubCoupling(const T *__restrict__ Gf, const T xn[NB], T y[NB])
 {
+   constexpr int GS = GStride(NB, (int)sizeof(T));
+   constexpr int PER = 16 / (int)sizeof(T);
+   T gv[GS];
+#pragma unroll
+   for (int v = 0; v < GS / PER; v++) {
+      if constexpr (sizeof(T) == 8) {
+         const double2 d = reinterpret_cast<const double2 *>(Gf)[v];
+         gv[2 * v] = d.x;
+         gv[2 * v + 1] = d.y;
+      } else {
+         const float4 d = reinterpret_cast<const float4 *>(Gf)[v];
+         gv[4 * v] = d.x;
+         gv[4 * v + 1] = d.y;
+         gv[4 * v + 2] = d.z;
+         gv[4 * v + 3] = d.w;
+      }
+   }
 #pragma unroll
    for (int ii = 0; ii < NB; ii++) {
       T u = T(0);
 #pragma unroll
-      for (int j = 0; j < NB; j++) u += Gf[ii * NB + j] * xn[j];
+      for (int j = 0; j < NB; j++) u += gv[ii * NB + j] * xn[j];
       y[ii] -= u;
    }
 }
@@ -322,6 +344,7 @@ __global__ void __launch_bounds__(128, SweepMinBlocks<T, NB, PL>()) SweepKernel(
    const int A = s.A;
    const T *never = reinterpret_cast<const T *>(s.ctrl + kCtrlNever);
    const size_t R = (size_t)NB * NB * (1 + S);
+   constexpr int GS = GStride(NB, (int)sizeof(T));
    // The task's five scalars, one lane each, in one round trip
    auto scalars = [&](int64_t tt) -> int64_t {
       if (tt >= s.n_tasks) return 0;
@@ -386,7 +409,9 @@ __global__ void __launch_bounds__(128, SweepMinBlocks<T, NB, PL>()) SweepKernel(
                }
 #pragma unroll
                for (int e = 0; e < SM * NB * NB; e++)
-                  if (e < S * NB * NB) CpAsync<sizeof(T)>(G + (size_t)i * S * NB * NB + e, ft + (size_t)(NB * NB + e) * ncell);
+                  if (e < S * NB * NB)
+                     CpAsync<sizeof(T)>(G + ((size_t)i * S + e / (NB * NB)) * GS + e % (NB * NB),
+                                        ft + (size_t)(NB * NB + e) * ncell);
             }
          }
          if constexpr (kPrefetch) {
@@ -431,7 +456,7 @@ __global__ void __launch_bounds__(128, SweepMinBlocks<T, NB, PL>()) SweepKernel(
                for (int j = 0; j < NB; j++) Wk[ii][j] = ft[(size_t)(ii * NB + j) * ncell];
          } else {
             const T om[3] = {g.omega[3 * a], g.omega[3 * a + 1], g.omega[3 * a + 2]};
-            CellFactors<T, NB, F>(g, c, om, s.tmask[off + i], Wk, G + (size_t)i * S * NB * NB, (size_t)NB * NB, 1);
+            CellFactors<T, NB, F>(g, c, om, s.tmask[off + i], Wk, G + (size_t)i * S * GS, (size_t)GS, 1);
          }
          T y[NB];
 #pragma unroll
@@ -459,7 +484,7 @@ __global__ void __launch_bounds__(128, SweepMinBlocks<T, NB, PL>()) SweepKernel(
 #pragma unroll
                for (int sl = 0; sl < SM; sl++) {
                   if (my_up[k][sl] < 0) continue;
-                  SubCoupling<T, NB>(G + ((size_t)i * S + sl) * NB * NB, xp[k][sl], y);
+                  SubCoupling<T, NB>(G + ((size_t)i * S + sl) * GS, xp[k][sl], y);
                   my_up[k][sl] = -1;
                }
             }
@@ -494,7 +519,7 @@ __global__ void __launch_bounds__(128, SweepMinBlocks<T, NB, PL>()) SweepKernel(
                }
                T xn[NB];
                PollUpwind<T, NB>(src, stride, s, xn);
-               SubCoupling<T, NB>(G + ((size_t)i * S + sl) * NB * NB, xn, y);
+               SubCoupling<T, NB>(G + ((size_t)i * S + sl) * GS, xn, y);
             }
 #pragma unroll
             for (int sl = 0; sl < SM; sl++) {
@@ -502,7 +527,7 @@ __global__ void __launch_bounds__(128, SweepMinBlocks<T, NB, PL>()) SweepKernel(
                T xn[NB];
 #pragma unroll
                for (int j = 0; j < NB; j++) xn[j] = loc[my_ul[k][sl] * NB + j];
-               SubCoupling<T, NB>(G + ((size_t)i * S + sl) * NB * NB, xn, y);
+               SubCoupling<T, NB>(G + ((size_t)i * S + sl) * GS, xn, y);
             }
             const int64_t c = base + local;
 #pragma unroll
