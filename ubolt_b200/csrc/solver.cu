@@ -444,6 +444,10 @@ __global__ void __launch_bounds__(256) IsoExpandKernel(const S *__restrict__ r0,
    for (int64_t nb0 = warp * 4; nb0 < n_nodes; nb0 += n_warps * 4) {
       const int64_t node = nb0 + (lane >> 3);
       if (node >= n_nodes) continue;
+      if (!r0) {  // r0 isotropic: alpha r_perp = 0
+         for (int a = sub; a < A; a += kLpn) t[node * A + a] = (S)((u ? (double)u[a] : 1.0) * phi[node]);
+         continue;
+      }
       const double iso = phi[node] - al * rho[node];
       for (int a = sub; a < A; a += kLpn)
          t[node * A + a] = (S)(al * (double)r0[node * A + a] + (u ? (double)u[a] : 1.0) * iso);
@@ -550,7 +554,13 @@ static int GmresIso(ubolt_ctx *ctx, const ubolt_solver *ws, S *work, const S *b,
       double sc[2] = {0.0, 0.0};
       cudaMemcpyAsync(sc, scal, sizeof sc, cudaMemcpyDeviceToHost, s);
       if ((rc = CudaCheck(cudaStreamSynchronize(s), "gmres"))) return rc;
-      const double rp2 = sc[0];
+      // A residual isotropic to rounding (r_perp below 1e-14 of it: the first
+      // cycle of an isotropic source) is taken as isotropic: r_perp = 0, and
+      // the sweep reads the node vector alone, not r0
+      double rp2 = sc[0];
+      const bool iso_r0 = rp2 <= 1e-28 * (rp2 + kappa * sc[1]);
+      if (iso_r0) rp2 = 0.0;
+      const S *r0_in = iso_r0 ? nullptr : r0;
       const double beta = std::sqrt(rp2 + kappa * sc[1]);
       if (!std::isfinite(beta)) return SetError(UBOLT_ERR_NONFINITE, "GMRES residual is not finite");
       out->estimate = bnorm > 0 ? beta / bnorm : 0.0;
@@ -570,7 +580,7 @@ static int GmresIso(ubolt_ctx *ctx, const ubolt_solver *ws, S *work, const S *b,
          double *pj = Phi + (int64_t)j * nn, *pn = Phi + (int64_t)(j + 1) * nn;
          S *z = Zb + (int64_t)j * n;
          // w = v_j - E_u m(M^{-1} v_j): alpha_w = alpha_j, phi_w = phi_j - m
-         if ((rc = IsoPrecondition<S>(ctx, adjoint, r0, alpha + j, pj, ws->rho, u, t, z, tmp, n, igrid, stream)))
+         if ((rc = IsoPrecondition<S>(ctx, adjoint, r0_in, alpha + j, pj, ws->rho, u, t, z, tmp, n, igrid, stream)))
             return rc;
          IsoScatterKernel<S><<<igrid, 256, 0, s>>>(z, wgt, sig_s, 1.0 / ctx->sum_weights, ctx->nb, A, nn, pj, pn);
          CountLaunch();

@@ -146,6 +146,7 @@ struct SweepDev {
    // u_a = aff_u[a] or 1, with r0 passed as q (compressed GMRES's Arnoldi vector)
    const double *aff_alpha, *aff_phi, *aff_rho;
    const void *aff_u;
+   int32_t aff_iso;  // r0 is isotropic (r0 = E rho): the input is u_a phi(node), q is not read
 };
 
 // Per-warp shared-memory slice, for P cells and S gathered faces per cell
@@ -436,7 +437,8 @@ __global__ void __launch_bounds__(128, SweepMinBlocks<T, NB, PL>()) SweepKernel(
 #pragma unroll
             for (int j = 0; j < NB; j++) {
                const int64_t node = c * NB + j;
-               r[j] = (T)(al * (double)q[node * A + a] + ua * (s.aff_phi[node] - al * s.aff_rho[node]));
+               r[j] = s.aff_iso ? (T)(ua * s.aff_phi[node])
+                                : (T)(al * (double)q[node * A + a] + ua * (s.aff_phi[node] - al * s.aff_rho[node]));
             }
          } else {
 #pragma unroll
@@ -632,6 +634,7 @@ static SweepDev DevPlan(const ubolt_sweep_plan *pl)
    s.slots = pl->slots;
    s.aff_alpha = s.aff_phi = s.aff_rho = nullptr;
    s.aff_u = nullptr;
+   s.aff_iso = 0;
    return s;
 }
 
@@ -705,6 +708,7 @@ static int LaunchSweep(ubolt_ctx *ctx, const T *q, T *psi, cudaStream_t st, cons
       s.aff_phi = affine->aff_phi;
       s.aff_rho = affine->aff_rho;
       s.aff_u = affine->aff_u;
+      s.aff_iso = affine->aff_iso;
    }
    s.unmet_task = pl->unmet_task;
    pl->unmet_task = -1;
@@ -736,7 +740,8 @@ bool SweepIsExact(ubolt_ctx *ctx)
 }
 
 // psi = L^{-1} (alpha r0 + E_u (phi - alpha rho)) with the input formed as
-// the sweep reads it (u = 1, or u_a = u[a]); alpha, phi, rho on the device
+// the sweep reads it (u = 1, or u_a = u[a]); alpha, phi, rho on the device.
+// r0 == nullptr: r0 is isotropic, r0 = E_u rho, and the input is E_u phi.
 template <typename T>
 int SweepAffine(ubolt_ctx *ctx, const T *r0, const double *alpha, const double *phi, const double *rho, const T *u,
                 T *psi, void *stream)
@@ -749,6 +754,7 @@ int SweepAffine(ubolt_ctx *ctx, const T *r0, const double *alpha, const double *
    aff.aff_phi = phi;
    aff.aff_rho = rho;
    aff.aff_u = u;
+   aff.aff_iso = r0 == nullptr;
    UBOLT_DISPATCH(ctx->nb, ctx->F, return (LaunchSweep<T, NB_, F_>(ctx, r0, psi, (cudaStream_t)stream, &aff)));
    return SetError(UBOLT_ERR_STATE, "no sweep kernel for this shape");
 }
