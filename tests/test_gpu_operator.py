@@ -120,3 +120,24 @@ def test_full_size_operator_properties():
     a32 = A.mult(x.float()).double()
     assert (a32 - ax).abs().max() <= 2e-5 * ax.abs().max()
     ctx.close()
+
+
+def test_apply_with_few_ordinates_and_large_cells():
+    """DG1 hexes at S2 (8 ordinates): 32 cells to a block, whose staged shape
+    data and flux need more than 48 KB of shared memory."""
+    from ubolt_b200 import problem as P
+    rng = np.random.default_rng(5)
+    g = P.build_geometry(P.box_hexes(4, 4, 3), 1)
+    q = P.lqn(3, 2)
+    st = rng.uniform(0.5, 2.0, g.n_cells)
+    ss = st * rng.uniform(0.1, 0.9, g.n_cells)
+    ctx = T.Context(g, q)
+    keep = (dev(st), dev(ss))
+    ctx.set_group(*keep)
+    op = O.Operator(g, q, st, ss)
+    x = rng.standard_normal(op.n)
+    A = T.TransportOperator(ctx)
+    assert rel(A.mult(dev(x)), op.apply(x)) < TOL64
+    assert rel(A.mult_unscattered(dev(x)), op.apply(x, scatter=False)) < TOL64
+    assert rel(A.mult(dev(x, torch.float32)), op.apply(dev(x, torch.float32).double().cpu().numpy())) < TOL32
+    ctx.close()

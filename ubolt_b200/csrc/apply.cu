@@ -335,8 +335,10 @@ int LaunchApply(const ubolt_ctx *ctx, const DevGeom<T> &g, const T *x, T *y, int
    } else {
       const size_t smem = sizeof(T) * (size_t)K * (RecordLayout(NB, F, (int)sizeof(T)).size + NB * g.A + NB + 2) +
                           sizeof(int32_t) * K * F;
-      if (mode == kFull) ApplyKernel<T, NB, F, true><<<blocks, threads, smem, s>>>(g, x, y, K);
-      else ApplyKernel<T, NB, F, false><<<blocks, threads, smem, s>>>(g, x, y, K);
+      auto kern = mode == kFull ? ApplyKernel<T, NB, F, true> : ApplyKernel<T, NB, F, false>;
+      // Few ordinates mean many cells per block (DG1 hexes at S2: 32 cells, 67 KB)
+      if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      kern<<<blocks, threads, smem, s>>>(g, x, y, K);
    }
    return CheckLaunch("apply");
 }
