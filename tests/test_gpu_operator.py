@@ -141,3 +141,24 @@ def test_apply_with_few_ordinates_and_large_cells():
     assert rel(A.mult_unscattered(dev(x)), op.apply(x, scatter=False)) < TOL64
     assert rel(A.mult(dev(x, torch.float32)), op.apply(dev(x, torch.float32).double().cpu().numpy())) < TOL32
     ctx.close()
+
+
+def test_apply_with_unaligned_vectors():
+    """Vectors that do not start on a 16-byte boundary take the one-ordinate
+    thread path; it must agree with the oracle as well."""
+    mesh, g, q, st, ss = build(CASES[1])
+    ctx = T.Context(g, q)
+    keep = (dev(st), dev(ss))
+    ctx.set_group(*keep)
+    op = O.Operator(g, q, st, ss)
+    x = np.random.default_rng(4).standard_normal(op.n)
+    A = T.TransportOperator(ctx)
+    for dtype, tol in ((torch.float64, TOL64), (torch.float32, TOL32)):
+        xb = torch.zeros(op.n + 1, dtype=dtype, device="cuda")
+        yb = torch.zeros(op.n + 1, dtype=dtype, device="cuda")
+        xs, ys = xb[1:], yb[1:]
+        xs.copy_(dev(x, dtype))
+        xr = xs.double().cpu().numpy()
+        assert rel(A.mult(xs, ys), op.apply(xr)) < tol
+        assert rel(A.mult_unscattered(xs, ys), op.apply(xr, scatter=False)) < tol
+    ctx.close()

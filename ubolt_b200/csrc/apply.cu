@@ -11,24 +11,30 @@
 //   scatter: - sigma_s(c) / W sum_b w_b x(c,i,b)                           (:584-649)
 // Vacuum inflow slots are nulled (their value is rhs), s == 0 adds nothing.
 //
-// One block holds K whole cells, one thread per (cell, angle); a thread
-// computes all n_basis rows of its (cell, angle).
-//
-// Forward (L - S and L): everything a block needs besides its upwind
-// neighbours is staged in shared memory by coalesced cooperative loads
-// issued together - the cells' angular flux, their shape data (normals,
-// face matrices, gradients), face codes and cross sections - so a block
-// waits on two rounds of memory latency (class id -> shape data, face code
-// -> neighbour flux) instead of a chain of per-face loads. The upwind
-// neighbours' values are loaded into registers before the scatter's
-// per-node angular moment (a warp-shuffle reduction over the staged flux)
-// is formed, so those loads overlap it. A reflective face reads its
-// mirrored angle from the staged flux.
+// Forward (L - S and L): a block holds K whole cells, one thread per (cell,
+// AP consecutive ordinates), AP = 16 bytes / element (2 in FP64, 4 in FP32)
+// where the ordinate count and the vectors' alignment allow, else 1. The
+// block first stages in shared memory, with asynchronous copies all in
+// flight at once: its cells' rows (one contiguous range of x), each cell's
+// class record (per face: normal and both face matrices, 16-byte parts) and
+// each thread's upwind runs (the neighbour's rows at its ordinates). After
+// one wait everything is read from shared memory, so a block costs two
+// rounds of memory latency (face codes and class ids, then the copies). The
+// scatter's node moments are summed from the staged rows by four lanes per
+// node and two shuffles, in a fixed order. Every face is folded in without a
+// branch on the sign of s = Omega . nA: the outflow part max(s, 0) face_own x
+// and the inflow part min(s, 0) face_up x_up (x_up the neighbour, the
+// mirrored ordinate of this cell on a reflective side, zero on a vacuum side).
 //
 // Adjoint ((L - S)^T): a column also needs the NEIGHBOUR's shape data (its
 // face slot and matrix for the shared face), so that kernel gathers class
-// data straight from L1/L2.
+// data straight from L1/L2, one thread per (cell, ordinate).
 #include "ctx.h"
+
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
 
 namespace ubolt {
 
@@ -42,162 +48,269 @@ __device__ __forceinline__ T WarpSum(T v)
    return v;
 }
 
-// Two 256-thread blocks per SM at most 64 registers; the FP64 4 x 4 block
-// needs more and takes them
-template <typename T, int NB, int F>
-constexpr int ApplyMinBlocks() { return (sizeof(T) == 8 && NB == 4) ? 1 : 2; }
+// N consecutive values from an address aligned to 16 bytes (N * sizeof(T)
+// a multiple of 16), to 8 bytes (8), or element-aligned
+template <typename T, int N>
+__device__ __forceinline__ void LoadRun(const T *__restrict__ p, T v[N])
+{
+   constexpr int B = (int)sizeof(T) * N;
+   if constexpr (B % 16 == 0) {
+#pragma unroll
+      for (int u = 0; u < B / 16; u++) {
+         const int4 w = __ldg(reinterpret_cast<const int4 *>(p) + u);
+         memcpy(&v[u * (16 / (int)sizeof(T))], &w, 16);
+      }
+   } else if constexpr (B == 8 && sizeof(T) == 4) {
+      const int2 w = __ldg(reinterpret_cast<const int2 *>(p));
+      memcpy(v, &w, 8);
+   } else {
+#pragma unroll
+      for (int i = 0; i < N; i++) v[i] = __ldg(p + i);
+   }
+}
 
-template <typename T, int NB, int F, bool SCATTER>
-__global__ void __launch_bounds__(512, ApplyMinBlocks<T, NB, F>()) ApplyKernel(const DevGeom<T> g, const T *__restrict__ x, T *__restrict__ y, int K)
+template <typename T, int N>
+__device__ __forceinline__ void StoreRun(T *__restrict__ p, const T v[N])
+{
+   constexpr int B = (int)sizeof(T) * N;
+   if constexpr (B % 16 == 0) {
+#pragma unroll
+      for (int u = 0; u < B / 16; u++) {
+         int4 w;
+         memcpy(&w, &v[u * (16 / (int)sizeof(T))], 16);
+         __stcs(reinterpret_cast<int4 *>(p) + u, w);
+      }
+   } else {
+#pragma unroll
+      for (int i = 0; i < N; i++) p[i] = v[i];
+   }
+}
+
+// N consecutive values from shared memory, 16-byte aligned when N *
+// sizeof(T) is a multiple of 16
+template <typename T, int N>
+__device__ __forceinline__ void LoadShared(const T *p, T v[N])
+{
+   if constexpr ((int)sizeof(T) * N % 16 == 0) {
+#pragma unroll
+      for (int u = 0; u < (int)sizeof(T) * N / 16; u++) {
+         const int4 w = reinterpret_cast<const int4 *>(p)[u];
+         memcpy(&v[u * (16 / (int)sizeof(T))], &w, 16);
+      }
+   } else {
+#pragma unroll
+      for (int i = 0; i < N; i++) v[i] = p[i];
+   }
+}
+
+// Shared memory of one apply block, in elements of T: the cells' class
+// records [K][L.size], each thread's upwind runs [threads][F][NB][AP], the
+// cells' own rows [K][NB][A], then for the scatter the node moments
+// [K][NB], sigma_s / W per cell [K] and the ordinate weights [A]
+template <typename T, int NB, int F, int AP>
+__host__ __device__ constexpr size_t ApplySmemElems(int K, int threads, int A)
+{
+   return (size_t)K * RecordLayout(NB, F, (int)sizeof(T)).size + (size_t)threads * F * NB * AP + (size_t)K * NB * A +
+          (size_t)K * NB + (size_t)K + (size_t)A;
+}
+
+// Three 256-thread blocks per SM (at most 80 registers); two where the four
+// basis functions' rows of AP > 1 ordinates need more
+template <typename T, int NB, int AP>
+constexpr int ApplyMinBlocks() { return (NB == 4 && AP > 1) ? 2 : 3; }
+
+template <typename T, int NB, int F, int AP, bool SCATTER>
+__global__ void __launch_bounds__(256, ApplyMinBlocks<T, NB, AP>()) ApplyKernel(const DevGeom<T> g, const T *__restrict__ x, T *__restrict__ y, int K)
 {
    constexpr RecordLayout L(NB, F, (int)sizeof(T));
-   constexpr int U = L.size * (int)sizeof(T) / 16;  // 16-byte units per class record
+   constexpr int CU = AP * (int)sizeof(T);  // bytes of one thread's run of a row
+   constexpr int RU = L.size * (int)sizeof(T) / 16;
    extern __shared__ __align__(16) unsigned char smem_raw[];
-   const int A = g.A;
-   T *geo = reinterpret_cast<T *>(smem_raw);                   // [K][L.size]
-   T *xs = geo + K * L.size;                                    // [K][NB][A]
-   T *mom = xs + K * NB * A;                                    // [K][NB]
-   T *sig = mom + K * NB;                                       // [K][2]: sigma_t, sigma_s / W
-   int32_t *codes = reinterpret_cast<int32_t *>(sig + 2 * K);  // [K][F]
+   const int A = g.A, QA = A / AP;
+   T *recs = reinterpret_cast<T *>(smem_raw);
+   T *xup = recs + K * L.size;
+   T *xs = xup + (size_t)blockDim.x * F * NB * AP;
+   T *mom = xs + K * NB * A;  // scatter: [K][NB] sigma_s / W sum_b w_b x(node, b)
+   T *ssw = mom + K * NB;     // scatter: [K] sigma_s / W
+   T *ws = ssw + K;           // scatter: [A] the weights
    const int t = threadIdx.x;
-   const int k = t / A;
-   const int a = t - k * A;
+   const int k = t / QA;
+   const int q = t - k * QA;
+   const int a0 = q * AP;
    const int64_t c0 = (int64_t)blockIdx.x * K;
-   const int kc = (int)min((int64_t)K, g.n_cells - c0);  // cells in this block
+   const int64_t c = c0 + k;
+   const int kc = (int)min((int64_t)K, g.n_cells - c0);
    const bool live = k < kc;
-   const T *xb = x + c0 * NB * A;  // this block's rows, then 32-bit offsets
-   T *yb = y + c0 * NB * A;
 
-   // Round 1: own flux, face codes, cross sections; class ids -> shape data
+   // Stage: the block's own rows (one contiguous range), each cell's class
+   // record and this thread's upwind runs, all in flight at once. Per face
+   // 4 bits of fcode: 8 for an interior face, else the boundary side.
+   unsigned fcode = 0;
+   {
+      const int nu = kc * NB * A * (int)sizeof(T) / CU;
+      const unsigned char *src = reinterpret_cast<const unsigned char *>(x + c0 * NB * A);
+      for (int u = t; u < nu; u += blockDim.x) CpAsync<CU>(reinterpret_cast<unsigned char *>(xs) + u * CU, src + u * CU);
+   }
    if (live) {
+      const T *rec = g.rec + (int64_t)g.cls[c] * L.size;
+      for (int u = q; u < RU; u += QA) CpAsync<16>(recs + k * L.size + u * (16 / (int)sizeof(T)), rec + u * (16 / (int)sizeof(T)));
 #pragma unroll
-      for (int j = 0; j < NB; j++) xs[(k * NB + j) * A + a] = xb[(k * NB + j) * A + a];
+      for (int f = 0; f < F; f++) {
+         const int32_t cf = g.code[c * F + f];
+         if (FaceInterior(cf)) {
+            fcode |= 8u << (4 * f);
+#pragma unroll
+            for (int j = 0; j < NB; j++)
+               CpAsync<CU>(xup + ((t * F + f) * NB + j) * AP, x + ((int64_t)cf * NB + j) * A + a0);
+         } else {
+            fcode |= (unsigned)FaceSide(cf) << (4 * f);
+         }
+      }
    }
-   for (int e = t; e < kc * F; e += blockDim.x) codes[e] = g.code[c0 * F + e];
-   for (int e = t; e < kc; e += blockDim.x) {
-      sig[2 * e] = g.sigma_t[c0 + e];
-      sig[2 * e + 1] = SCATTER ? g.sigma_s[c0 + e] * g.inv_sum_weights : T(0);
+   T om[3 * AP];
+   T sig_t = T(0);
+   if (live) {
+      LoadRun<T, 3 * AP>(g.omega + 3 * a0, om);
+      sig_t = g.sigma_t[c];
+      if (SCATTER && q == 0) ssw[k] = g.sigma_s[c] * g.inv_sum_weights;
    }
-   for (int e = t; e < kc * U; e += blockDim.x) {
-      const int kk = e / U;
-      const int u = e - kk * U;
-      const int64_t cl = g.cls[c0 + kk];
-      reinterpret_cast<int4 *>(geo)[kk * U + u] = reinterpret_cast<const int4 *>(g.rec)[cl * U + u];
-   }
+   if constexpr (SCATTER)
+      for (int b = t; b < A; b += blockDim.x) ws[b] = g.w[b];
+   CpAsyncWaitAll();
    __syncthreads();
 
-   // Round 2: the upwind neighbours of this (cell, angle), loaded together
-   // and folded in at once (inflow faces: the upwind neighbour, or the
-   // mirrored angle here), so they hold no registers past this point
-   const T *gs = geo + k * L.size;
-   T ox = T(0), oy = T(0), oz = T(0);
-   T sf[F];
-   T acc[NB];
-#pragma unroll
-   for (int i = 0; i < NB; i++) acc[i] = T(0);
-   if (live) {
-      ox = g.omega[3 * a];
-      oy = g.omega[3 * a + 1];
-      oz = g.omega[3 * a + 2];
-#pragma unroll
-      for (int f = 0; f < F; f++) sf[f] = Dot3(ox, oy, oz, gs + L.nA + 3 * f);
-      // Faces in chunks of FC: every load of a chunk is in flight at once
-      constexpr int FC = (F * NB <= 9) ? F : (F % 3 == 0 ? 3 : 2);
-#pragma unroll
-      for (int f0 = 0; f0 < F; f0 += FC) {
-      T xn[FC][NB];
-#pragma unroll
-      for (int ff = 0; ff < FC; ff++) {
-         const int32_t code = codes[k * F + f0 + ff];
-         const bool up = sf[f0 + ff] < T(0) && FaceInterior(code);
-         const T *xu = x + (size_t)(up ? code : 0) * (NB * A) + a;
-#pragma unroll
-         for (int j = 0; j < NB; j++) xn[ff][j] = up ? xu[j * A] : T(0);
+   if constexpr (SCATTER) {
+      // sigma_s / W sum_b w_b x(node, b) from the staged rows: four lanes
+      // per node, each a fixed quarter of the ordinates, then two shuffles.
+      // The loop bound is the same for every thread (the shuffles need the
+      // whole warp).
+      constexpr int G = 4;
+      const int nodes = kc * NB;
+      for (int base = 0; base < nodes * G; base += blockDim.x) {
+         const int idx = base + t;
+         const int n = idx / G, part = idx - (idx / G) * G;
+         T m = T(0);
+         if (n < nodes)
+            for (int b = part; b < A; b += G) m += ws[b] * xs[n * A + b];
+         m += __shfl_xor_sync(0xffffffffu, m, 1);
+         m += __shfl_xor_sync(0xffffffffu, m, 2);
+         if (part == 0 && n < nodes) mom[n] = m * ssw[n / NB];
       }
+   }
+
+   T acc[AP][NB];
+   if (live) {
+      const T *r = recs + k * L.size;
+      const T *xk = xs + k * NB * A;
+      constexpr int TS = L.size - L.tail;  // grad phi and 1 / V
+      T tl[TS];
+      LoadShared<T, TS>(r + L.tail, tl);
+      T xo[AP][NB];
 #pragma unroll
-      for (int ff = 0; ff < FC; ff++) {
-         const int f = f0 + ff;
-         if (!(sf[f] < T(0))) continue;
-         const int32_t code = codes[k * F + f];
-         if (!FaceInterior(code)) {
-            const int side = FaceSide(code);
-            if (g.side_bc[side] != UBOLT_BC_REFLECT) continue;
-            const int ar = g.refl[(side >> 1) * A + a];
+      for (int j = 0; j < NB; j++) {
+         T v[AP];
+         LoadShared<T, AP>(xk + j * A + a0, v);
 #pragma unroll
-            for (int j = 0; j < NB; j++) xn[ff][j] = xs[(k * NB + j) * A + ar];
+         for (int p = 0; p < AP; p++) xo[p][j] = v[p];
+      }
+      // Removal, and the volume term -(Omega . grad phi_i) x(c, 0, a) for i > 0
+#pragma unroll
+      for (int p = 0; p < AP; p++)
+#pragma unroll
+         for (int i = 0; i < NB; i++) acc[p][i] = sig_t * xo[p][i];
+      if constexpr (NB > 1) {
+#pragma unroll
+         for (int i = 1; i < NB; i++)
+#pragma unroll
+            for (int p = 0; p < AP; p++) acc[p][i] -= Dot3(om + 3 * p, tl + 3 * i) * xo[p][0];
+      }
+      // Each face without a branch on the sign of s = Omega . nA: outflow
+      // max(s, 0) face_own x, inflow min(s, 0) face_up x_up, x_up the
+      // neighbour, this cell's mirrored ordinate on a reflective side, zero
+      // on a vacuum side (DG0: the same with 1 / V for both matrices). The
+      // faces one at a time: unrolled, their reads would be hoisted together
+      // and spill
+#pragma unroll 1
+      for (int f = 0; f < F; f++) {
+         const unsigned fc = (fcode >> (4 * f)) & 15u;
+         T na[4];
+         LoadShared<T, 4>(r + L.nA(f), na);
+         T xn[AP][NB];
+         if (fc & 8u) {
+#pragma unroll
+            for (int j = 0; j < NB; j++) {
+               T v[AP];
+               LoadShared<T, AP>(xup + ((t * F + f) * NB + j) * AP, v);
+#pragma unroll
+               for (int p = 0; p < AP; p++) xn[p][j] = v[p];
+            }
+         } else {
+            const int side = (int)fc;
+            const bool refl = g.side_bc[side] == UBOLT_BC_REFLECT;
+#pragma unroll
+            for (int p = 0; p < AP; p++) {
+               const int ar = refl ? g.refl[(side >> 1) * A + a0 + p] : 0;
+#pragma unroll
+               for (int j = 0; j < NB; j++) xn[p][j] = refl ? xk[j * A + ar] : T(0);
+            }
+         }
+         T sp[AP], sm[AP];
+#pragma unroll
+         for (int p = 0; p < AP; p++) {
+            const T s = Dot3(om + 3 * p, na);
+            sp[p] = fmax(s, T(0));
+            sm[p] = fmin(s, T(0));
          }
          if constexpr (NB == 1) {
-            acc[0] += sf[f] * gs[L.ivol] * xn[ff][0];
+#pragma unroll
+            for (int p = 0; p < AP; p++) acc[p][0] += (sp[p] * xo[p][0] + sm[p] * xn[p][0]) * tl[0];
          } else {
-            const T *M = gs + L.fup + f * NB * NB;
+            {
+               T m[L.fm];
+               LoadShared<T, L.fm>(r + L.fown(f), m);
 #pragma unroll
-            for (int i = 0; i < NB; i++) {
-               T u = T(0);
+               for (int p = 0; p < AP; p++)
 #pragma unroll
-               for (int j = 0; j < NB; j++) u += M[i * NB + j] * xn[ff][j];
-               acc[i] += sf[f] * u;
+                  for (int i = 0; i < NB; i++) {
+                     T u = T(0);
+#pragma unroll
+                     for (int j = 0; j < NB; j++) u += m[i * NB + j] * xo[p][j];
+                     acc[p][i] += sp[p] * u;
+                  }
+            }
+            {
+               T m[L.fm];
+               LoadShared<T, L.fm>(r + L.fup(f), m);
+#pragma unroll
+               for (int p = 0; p < AP; p++)
+#pragma unroll
+                  for (int i = 0; i < NB; i++) {
+                     T v = T(0);
+#pragma unroll
+                     for (int j = 0; j < NB; j++) v += m[i * NB + j] * xn[p][j];
+                     acc[p][i] += sm[p] * v;
+                  }
             }
          }
       }
-      }
    }
    if constexpr (SCATTER) {
-      // Per node: sigma_s / W sum_b w_b x(node, b)
-      const int warp = t >> 5, lane = t & 31, n_warps = blockDim.x >> 5;
-      for (int n = warp; n < kc * NB; n += n_warps) {
-         T s = T(0);
-         for (int b = lane; b < A; b += 32) s += g.w[b] * xs[n * A + b];
-         s = WarpSum(s);
-         if (lane == 0) mom[n] = s * sig[2 * (n / NB) + 1];
-      }
       __syncthreads();
+      if (live) {
+#pragma unroll
+         for (int p = 0; p < AP; p++)
+#pragma unroll
+            for (int i = 0; i < NB; i++) acc[p][i] -= mom[k * NB + i];
+      }
    }
    if (!live) return;
-
-   // Own block: outflow faces, volume term, removal
-   if constexpr (NB == 1) {
-      T out = T(0);
 #pragma unroll
-      for (int f = 0; f < F; f++)
-         if (sf[f] > T(0)) out += sf[f];
-      acc[0] += (out * gs[L.ivol] + sig[2 * k]) * xs[k * A + a];
-   } else {
-      T B[NB][NB];
+   for (int i = 0; i < NB; i++) {
+      T v[AP];
 #pragma unroll
-      for (int i = 0; i < NB; i++)
-#pragma unroll
-         for (int j = 0; j < NB; j++) B[i][j] = T(0);
-#pragma unroll
-      for (int f = 0; f < F; f++) {
-         if (sf[f] > T(0)) {
-            const T *M = gs + L.fown + f * NB * NB;
-#pragma unroll
-            for (int i = 0; i < NB; i++)
-#pragma unroll
-               for (int j = 0; j < NB; j++) B[i][j] += sf[f] * M[i * NB + j];
-         }
-      }
-#pragma unroll
-      for (int i = 1; i < NB; i++) B[i][0] -= Dot3(ox, oy, oz, gs + L.bgrad + 3 * i);
-#pragma unroll
-      for (int i = 0; i < NB; i++) B[i][i] += sig[2 * k];
-      T xo[NB];
-#pragma unroll
-      for (int j = 0; j < NB; j++) xo[j] = xs[(k * NB + j) * A + a];
-#pragma unroll
-      for (int i = 0; i < NB; i++) {
-         T u = T(0);
-#pragma unroll
-         for (int j = 0; j < NB; j++) u += B[i][j] * xo[j];
-         acc[i] += u;
-      }
+      for (int p = 0; p < AP; p++) v[p] = acc[p][i];
+      StoreRun<T, AP>(y + (c * NB + i) * A + a0, v);
    }
-   if constexpr (SCATTER) {
-#pragma unroll
-      for (int i = 0; i < NB; i++) acc[i] -= mom[k * NB + i];
-   }
-#pragma unroll
-   for (int i = 0; i < NB; i++) yb[(k * NB + i) * A + a] = acc[i];
 }
 
 // Column (c, j, a) of L - S: the own block transposed, the scatter's
@@ -323,6 +436,56 @@ __global__ void DiagonalKernel(const DevGeom<T> g, T *__restrict__ d)
    for (int i = 0; i < NB; i++) d[(c * NB + i) * g.A + a] = B[i][i];
 }
 
+// Cells per block for QA threads per cell: the most live threads resident
+// per SM for this kernel (registers and shared memory), then the fewest idle
+// lanes, then the block nearest 256 threads. Cached per kernel and QA.
+template <typename Kern, typename Smem>
+static int ApplyCells(Kern kern, int QA, Smem smem_of)
+{
+   static std::mutex mu;
+   static std::map<std::pair<const void *, int>, int> memo;
+   const auto key = std::make_pair(reinterpret_cast<const void *>(kern), QA);
+   {
+      std::lock_guard<std::mutex> lk(mu);
+      auto it = memo.find(key);
+      if (it != memo.end()) return it->second;
+   }
+   int dev = 0, smem_max = 48 * 1024;
+   cudaGetDevice(&dev);
+   cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+   int best = 1;
+   long best_live = -1;
+   double best_idle = 2.0, best_dist = 1e9;
+   for (int K = 1; K * QA <= 256; K++) {
+      const int thr = (K * QA + 31) / 32 * 32;
+      const size_t smem = smem_of(K, thr);
+      if (smem > (size_t)smem_max) break;  // grows with K
+      int per_sm = 0;
+      if (smem > 48 * 1024 &&
+          cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+         cudaGetLastError();
+         break;
+      }
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, thr, smem) != cudaSuccess) {
+         cudaGetLastError();
+         per_sm = 0;
+      }
+      const long live = (long)per_sm * K * QA;
+      const double idle = (double)(thr - K * QA) / thr;
+      const double dist = std::abs(thr - 256);
+      if (live > best_live || (live == best_live && (idle < best_idle - 1e-9 ||
+                                                     (idle < best_idle + 1e-9 && dist < best_dist)))) {
+         best = K;
+         best_live = live;
+         best_idle = idle;
+         best_dist = dist;
+      }
+   }
+   std::lock_guard<std::mutex> lk(mu);
+   memo[key] = best;
+   return best;
+}
+
 template <typename T, int NB, int F>
 int LaunchApply(const ubolt_ctx *ctx, const DevGeom<T> &g, const T *x, T *y, int mode, cudaStream_t s)
 {
@@ -333,12 +496,32 @@ int LaunchApply(const ubolt_ctx *ctx, const DevGeom<T> &g, const T *x, T *y, int
       const size_t smem = sizeof(T) * (size_t)(K * NB * g.A + K * NB);
       AdjointApplyKernel<T, NB, F><<<blocks, threads, smem, s>>>(g, x, y, K);
    } else {
-      const size_t smem = sizeof(T) * (size_t)K * (RecordLayout(NB, F, (int)sizeof(T)).size + NB * g.A + NB + 2) +
-                          sizeof(int32_t) * K * F;
-      auto kern = mode == kFull ? ApplyKernel<T, NB, F, true> : ApplyKernel<T, NB, F, false>;
-      // Few ordinates mean many cells per block (DG1 hexes at S2: 32 cells, 67 KB)
-      if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      kern<<<blocks, threads, smem, s>>>(g, x, y, K);
+      // AP ordinates per thread as one 16-byte run where they fit evenly and
+      // both vectors are 16-byte aligned
+      constexpr int AV = 16 / (int)sizeof(T);
+      const bool vec = g.A % AV == 0 && (reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) % 16 == 0;
+      const int AP = vec ? AV : 1;
+      const int QA = g.A / AP;
+      if (QA > 256) return SetError(UBOLT_ERR_ARG, "apply: %d ordinates need 16-byte aligned vectors", g.A);
+      auto kern = vec ? (mode == kFull ? ApplyKernel<T, NB, F, AV, true> : ApplyKernel<T, NB, F, AV, false>)
+                      : (mode == kFull ? ApplyKernel<T, NB, F, 1, true> : ApplyKernel<T, NB, F, 1, false>);
+      const int A = g.A;
+      auto smem_of = [vec, A](int K, int thr) {
+         return sizeof(T) * (vec ? ApplySmemElems<T, NB, F, AV>(K, thr, A) : ApplySmemElems<T, NB, F, 1>(K, thr, A));
+      };
+      const int Kt = ApplyCells(kern, QA, smem_of);
+      const int64_t nblk = (g.n_cells + Kt - 1) / Kt;
+      const int nthr = (Kt * QA + 31) / 32 * 32;
+      const size_t smem = smem_of(Kt, nthr);
+      if (smem > 48 * 1024) {
+         const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+         if (e != cudaSuccess) {
+            cudaGetLastError();
+            return SetError(UBOLT_ERR_ARG, "apply: %zu bytes of shared memory for %d ordinates: %s", smem, g.A,
+                            cudaGetErrorString(e));
+         }
+      }
+      kern<<<nblk, nthr, smem, s>>>(g, x, y, Kt);
    }
    return CheckLaunch("apply");
 }

@@ -250,22 +250,29 @@ extern "C" int ubolt_ctx_create(const ubolt_dg_geometry *geom, const ubolt_quadr
       if ((rc = Upload(ctx, fbv, &g.fbv)) || (rc = Upload(ctx, ToF32(fbv), &h.fbv))) return fail(rc);
    }
    {
-      // Packed records, one per class, for kernels that stage a cell's shape data whole
+      // Packed records, one per class, for kernels that read a cell's shape data whole
       const RecordLayout L64(nb, F, 8), L32(nb, F, 4);
       std::vector<double> r64((size_t)ncls * L64.size, 0.0);
       std::vector<float> r32((size_t)ncls * L32.size, 0.0f);
       for (int64_t q = 0; q < ncls; q++) {
-         auto put = [&](int off, double v) {
-            r64[(size_t)q * L64.size + off] = v;
-            r32[(size_t)q * L32.size + off] = (float)v;
+         double *d64 = &r64[(size_t)q * L64.size];
+         float *d32 = &r32[(size_t)q * L32.size];
+         // Offsets differ between the two: each part is padded to 16 bytes
+         auto put = [&](int o64, int o32, double v) {
+            d64[o64] = v;
+            d32[o32] = (float)v;
          };
-         for (int k = 0; k < s_nA; k++) put(L64.nA + k, nA[q * s_nA + k]);
-         if (nb > 1) {
-            for (int k = 0; k < s_m; k++) put(L64.fown + k, fown[q * s_m + k]);
-            for (int k = 0; k < s_m; k++) put(L64.fup + k, fup[q * s_m + k]);
-            for (int k = 0; k < s_g; k++) put(L64.bgrad + k, bgrad[q * s_g + k]);
+         for (int f = 0; f < F; f++) {
+            for (int d = 0; d < 3; d++) put(L64.nA(f) + d, L32.nA(f) + d, nA[q * s_nA + f * 3 + d]);
+            if (nb > 1)
+               for (int k = 0; k < nb * nb; k++) {
+                  put(L64.fown(f) + k, L32.fown(f) + k, fown[q * s_m + f * nb * nb + k]);
+                  put(L64.fup(f) + k, L32.fup(f) + k, fup[q * s_m + f * nb * nb + k]);
+               }
          }
-         put(L64.ivol, inv_vol[q]);
+         if (nb > 1)
+            for (int k = 0; k < (int)s_g; k++) put(L64.bgrad() + k, L32.bgrad() + k, bgrad[q * s_g + k]);
+         put(L64.ivol(), L32.ivol(), inv_vol[q]);
       }
       if ((rc = Upload(ctx, r64, &g.rec)) || (rc = Upload(ctx, r32, &h.rec))) return fail(rc);
    }

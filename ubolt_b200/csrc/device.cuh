@@ -24,18 +24,27 @@ constexpr int kMaxFaces = 6;
 __host__ __device__ inline bool FaceInterior(int32_t code) { return code >= 0; }
 __host__ __device__ inline int FaceSide(int32_t code) { return -1 - code; }
 
-// A geometry class packed as one record: [nA F x 3][face_own F x nb x nb]
-// [face_up F x nb x nb][grad phi nb x 3][1 / V], padded to 16 bytes (the
-// matrices and gradients only for nb > 1). Offsets in elements of `elem` bytes.
+// n elements of `elem` bytes rounded up to a whole number of 16-byte units
+__host__ __device__ constexpr int Pad16(int n, int elem) { return (n + 16 / elem - 1) / (16 / elem) * (16 / elem); }
+
+// A geometry class packed as one record of 16-byte units, so a thread reads
+// a face's parts with a few vector loads: per face f a slab [nA_f (3, padded
+// to 4) | face_own_f (nb x nb) | face_up_f (nb x nb)], then [grad phi (nb x
+// 3) | 1 / V] (the matrices and gradients only for nb > 1), each part padded
+// to 16 bytes. Offsets in elements of `elem` bytes.
 struct RecordLayout {
-   int nA, fown, fup, bgrad, ivol, raw, size;
-   __host__ __device__ constexpr RecordLayout(int nb, int F, int elem)
-       : nA(0), fown(F * 3), fup(F * 3 + (nb > 1 ? F * nb * nb : 0)),
-         bgrad(F * 3 + (nb > 1 ? 2 * F * nb * nb : 0)), ivol(F * 3 + (nb > 1 ? 2 * F * nb * nb + nb * 3 : 0)),
-         raw(F * 3 + (nb > 1 ? 2 * F * nb * nb + nb * 3 : 0) + 1),
-         size((F * 3 + (nb > 1 ? 2 * F * nb * nb + nb * 3 : 0) + 1 + 16 / elem - 1) / (16 / elem) * (16 / elem))
+   int nb, fm, fs, tail, size;
+   __host__ __device__ constexpr RecordLayout(int nb_, int F, int elem)
+       : nb(nb_), fm(nb_ > 1 ? Pad16(nb_ * nb_, elem) : 0), fs(4 + 2 * (nb_ > 1 ? Pad16(nb_ * nb_, elem) : 0)),
+         tail(F * (4 + 2 * (nb_ > 1 ? Pad16(nb_ * nb_, elem) : 0))),
+         size(F * (4 + 2 * (nb_ > 1 ? Pad16(nb_ * nb_, elem) : 0)) + Pad16((nb_ > 1 ? 3 * nb_ : 0) + 1, elem))
    {
    }
+   __host__ __device__ constexpr int nA(int f) const { return f * fs; }
+   __host__ __device__ constexpr int fown(int f) const { return f * fs + 4; }
+   __host__ __device__ constexpr int fup(int f) const { return f * fs + 4 + fm; }
+   __host__ __device__ constexpr int bgrad() const { return tail; }
+   __host__ __device__ constexpr int ivol() const { return tail + (nb > 1 ? 3 * nb : 0); }
 };
 
 template <typename T>
@@ -65,6 +74,16 @@ struct DevGeom {
    const T *sigma_t;
    const T *sigma_s;
 };
+
+// An asynchronous global -> shared copy of one 4-, 8- or 16-byte word, both
+// addresses aligned to its size
+template <int BYTES>
+__device__ __forceinline__ void CpAsync(void *smem_dst, const void *src)
+{
+   const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+   asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(d), "l"(src), "n"(BYTES) : "memory");
+}
+__device__ __forceinline__ void CpAsyncWaitAll() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 template <typename T>
 __device__ __forceinline__ T Dot3(const T *__restrict__ om, const T *__restrict__ n)

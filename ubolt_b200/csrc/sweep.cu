@@ -200,15 +200,6 @@ __device__ __forceinline__ void PollUpwind(const T *p, int stride, const SweepDe
    }
 }
 
-// An asynchronous global -> shared copy of one 4- or 8-byte word
-template <int BYTES>
-__device__ __forceinline__ void CpAsync(void *smem_dst, const void *src)
-{
-   const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
-   asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(d), "l"(src), "n"(BYTES) : "memory");
-}
-__device__ __forceinline__ void CpAsyncWaitAll() { asm volatile("cp.async.wait_all;" ::: "memory"); }
-
 // y -= G x for one nb x nb coupling held in shared memory (16-byte aligned,
 // GStride elements), read with 16-byte loads
 template <typename T, int NB>
