@@ -295,27 +295,43 @@ typedef struct {
    double consistent_power;  /* DG0 consistent-D blend power p (default 1.5) */
    int32_t consistent_d;     /* DG0: blend the upwind numerical diffusion in (default 1) */
    int32_t inner_iterations; /* block-Jacobi PCG iterations of the inner solve (default 30) */
+   double void_sigma_t;      /* a cell with sigma_t <= this is void (-dsa_void_sigma_t, default 0) */
+   double void_d;            /* D in a bridged void; 0: from the voids' mean chord (-dsa_void_d, default 0) */
+   int32_t void_bridge;      /* bridge the voids where the operator allows (-dsa_void_bridge, default 1) */
+   int32_t pad_;
 } ubolt_dsa_options;
 
 void ubolt_dsa_defaults(ubolt_dsa_options *opts);
 /* Keep the host geometry the diffusion operator is built from and allocate
  * its device storage (DSAPrecon::create on an UnstructuredDG,
  * src/dsak.kokkos.cxx:113-121, src/dsa_plexk.kokkos.cxx:68-209). The
- * geometry must be the context's. No voids: every sigma_t must be > 0. */
+ * geometry must be the context's. */
 int ubolt_dsa_setup(ubolt_ctx *ctx, const ubolt_dg_geometry *geom, const ubolt_dsa_options *opts);
 /* Refill the diffusion matrix for the context's current group - host
  * assembly, then upload (DSAPrecon::set_group, src/dsak.kokkos.cxx:216-226:
  * MIP at DG1, dsa_plexk.kokkos.cxx:365-475; two-point flux with the
- * consistent-D blend at DG0, :288-348). Synchronises `stream`. */
+ * consistent-D blend at DG0, :288-348), after the void policy
+ * (DSAPrecon::assemble, src/dsak.kokkos.cxx:233-345): void cells are bridged
+ * (D from their mean chord, or the fixed void D) or, where bridging is off or
+ * would leave the operator singular, masked (V times the identity, no
+ * coupling, vacuum faces onto them, R and P skip them). UBOLT_ERR_ARG where
+ * the operator is singular (every face reflective, no void, no absorption).
+ * Synchronises `stream`. */
 int ubolt_dsa_set_group(ubolt_ctx *ctx, void *stream);
+/* The void policy's outcome for the current group: the number of void cells,
+ * whether they are bridged, and their mean chord 4 V / S (0 unless bridged)
+ * (DSAPrecon::assemble, src/dsak.kokkos.cxx:255-296). Any pointer may be NULL. */
+int ubolt_dsa_void_info(ubolt_ctx *ctx, int64_t *n_void, int32_t *bridged, double *chord);
 /* y = P D^{-1} R x (DSAPrecon::apply, src/dsak.kokkos.cxx:350-391), the
  * inner solve a fixed count of FP64 block-Jacobi PCG iterations on device. */
 int ubolt_dsa_apply(ubolt_ctx *ctx, const double *x, double *y, void *stream);
 /* v = D u over the nodes (n_cells * n_basis): the diffusion SpMV. */
 int ubolt_dsa_spmv(ubolt_ctx *ctx, const double *u, double *v, void *stream);
-/* rhs(node) = V_c sum_a w_a x(node, a) (RestrictKernel, src/dsak.kokkos.cxx:20-44). */
+/* rhs(node) = V_c sum_a w_a x(node, a) (RestrictKernel, src/dsak.kokkos.cxx:20-44);
+ * zero on a masked void's nodes once a group is filled. */
 int ubolt_dsa_restrict(ubolt_ctx *ctx, const double *x, double *rhs, void *stream);
-/* y(node, a) = u(node) / W (ProlongKernel, src/dsak.kokkos.cxx:51-62). */
+/* y(node, a) = u(node) / W (ProlongKernel, src/dsak.kokkos.cxx:51-62); zero
+ * on a masked void's rows once a group is filled. */
 int ubolt_dsa_prolong(ubolt_ctx *ctx, const double *u, double *y, void *stream);
 /* y = P D^{-1} R x exactly as ubolt_dsa_apply computes it, but with every
  * scratch vector of the inner solve in one fixed device array built into

@@ -184,43 +184,74 @@ def threads():
     return _lib.oracle_threads()
 
 
+u8p = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
+_sig("oracle_dsa_void_policy", C.c_int, C.c_int, C.c_int64, dp, i64p, i32p, dp, dp, dp, C.c_double, C.c_int,
+     C.c_double, u8p, u8p, dp, dp)
 _sig("oracle_dsa_mip", C.c_int64, C.c_int, C.c_int, C.c_int64, dp, i64p, i32p, dp, dp, dp, dp, dp, dp, dp, dp,
-     C.c_double, i64p, i64p, dp)
+     C.c_double, dp, u8p, u8p, C.c_int, i64p, i64p, dp)
 _sig("oracle_dsa_dg0", C.c_int64, C.c_int, C.c_int64, C.c_int, dp, i64p, i32p, dp, dp, dp, dp, C.c_double, dp, dp,
-     C.c_int, C.c_double, i64p, i64p, dp)
-_sig("oracle_dsa_restrict", None, C.c_int64, C.c_int, C.c_int, dp, dp, dp, dp)
-_sig("oracle_dsa_prolong", None, C.c_int64, C.c_int, C.c_int, C.c_double, dp, dp)
+     C.c_int, C.c_double, dp, u8p, i64p, i64p, dp)
+_sig("oracle_dsa_restrict", None, C.c_int64, C.c_int, C.c_int, dp, dp, dp, C.c_void_p, dp)
+_sig("oracle_dsa_prolong", None, C.c_int64, C.c_int, C.c_int, C.c_double, dp, C.c_void_p, dp)
 
 
-def dsa_matrix(geometry, quad, sigma_t, sigma_s, penalty=4.0, consistent=True, power=1.5):
-    """The DSA diffusion matrix (MIP at DG1, two-point flux at DG0) as SciPy CSR."""
+class VoidPolicy:
+    """The DSA void policy for one group (DSAPrecon::assemble,
+    src/dsak.kokkos.cxx:233-345): per cell is_void, masked and D, the bridge
+    decision, the voids' mean chord and their count; singular is True where
+    the diffusion operator would be singular."""
+
+    def __init__(self, geometry, sigma_t, sigma_s, void_sigma_t=0.0, bridge=True, void_d=0.0):
+        g = geometry
+        nc = g.n_cells
+        self.is_void = np.zeros(nc, dtype=np.uint8)
+        self.masked = np.zeros(nc, dtype=np.uint8)
+        self.d = np.zeros(nc)
+        out = np.zeros(3)
+        st = np.ascontiguousarray(sigma_t, dtype=np.float64)
+        ss = np.ascontiguousarray(sigma_s, dtype=np.float64)
+        self.singular = bool(_lib.oracle_dsa_void_policy(g.faces_per_cell, nc, g.face_nA, g.face_neighbour,
+                                                         g.face_bc, g.volume, st, ss, void_sigma_t, int(bridge),
+                                                         void_d, self.is_void, self.masked, self.d, out))
+        self.bridged = bool(out[0])
+        self.chord = float(out[1])
+        self.n_void = int(out[2])
+
+
+def dsa_matrix(geometry, quad, sigma_t, sigma_s, penalty=4.0, consistent=True, power=1.5, policy=None):
+    """The DSA diffusion matrix (MIP at DG1, two-point flux at DG0) as SciPy
+    CSR, with D and the masks of `policy` (default: the void policy's defaults)."""
     g = geometry
     nc, F, nb = g.n_cells, g.faces_per_cell, g.n_basis
     cap = nc * (F + 1) * nb * nb
     ri, ci, v = np.zeros(cap, dtype=np.int64), np.zeros(cap, dtype=np.int64), np.zeros(cap)
     st = np.ascontiguousarray(sigma_t, dtype=np.float64)
     ss = np.ascontiguousarray(sigma_s, dtype=np.float64)
+    pol = policy if policy is not None else VoidPolicy(g, st, ss)
     if nb > 1:
         e = _lib.oracle_dsa_mip(nb, F, nc, g.face_nA, g.face_neighbour, g.face_bc, g.face_distance, g.volume,
-                                g.face_own, g.face_up, g.basis_grad, g.face_neighbour_grad, st, ss, penalty, ri, ci, v)
+                                g.face_own, g.face_up, g.basis_grad, g.face_neighbour_grad, st, ss, penalty,
+                                pol.d, pol.is_void, pol.masked, int(pol.bridged), ri, ci, v)
     else:
         e = _lib.oracle_dsa_dg0(F, nc, quad.n_angles, g.face_nA, g.face_neighbour, g.face_bc, g.face_distance,
                                 g.volume, quad.omega.ravel(), quad.w, quad.sum_weights, st, ss, int(consistent), power,
-                                ri, ci, v)
+                                pol.d, pol.masked, ri, ci, v)
     return sp.csr_matrix((v[:e], (ri[:e], ci[:e])), shape=(nc * nb, nc * nb))
 
 
-def dsa_restrict(x, geometry, quad):
+def dsa_restrict(x, geometry, quad, masked=None):
     g = geometry
     rhs = np.empty(g.n_cells * g.n_basis)
+    m = None if masked is None else np.ascontiguousarray(masked, dtype=np.uint8)
     _lib.oracle_dsa_restrict(g.n_cells, g.n_basis, quad.n_angles, quad.w, g.volume,
-                             np.ascontiguousarray(x, dtype=np.float64), rhs)
+                             np.ascontiguousarray(x, dtype=np.float64), None if m is None else m.ctypes.data, rhs)
     return rhs
 
 
-def dsa_prolong(u, geometry, quad):
+def dsa_prolong(u, geometry, quad, masked=None):
     g = geometry
     y = np.empty(g.n_cells * g.n_basis * quad.n_angles)
+    m = None if masked is None else np.ascontiguousarray(masked, dtype=np.uint8)
     _lib.oracle_dsa_prolong(g.n_cells, g.n_basis, quad.n_angles, quad.sum_weights,
-                            np.ascontiguousarray(u, dtype=np.float64), y)
+                            np.ascontiguousarray(u, dtype=np.float64), None if m is None else m.ctypes.data, y)
     return y

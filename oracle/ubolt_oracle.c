@@ -655,10 +655,73 @@ int oracle_threads(void)
 }
 
 /* ~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~
- * DSA diffusion operators (DSAPlex, src/dsa_plexk.kokkos.cxx), no voids:
- * D = 1/(3 sigma_t), sigma_a = sigma_t - sigma_s, VOLUME-weighted rows.
- * Output as COO (row, col, val) with the reference's entry order per row.
+ * DSA diffusion operators (DSAPlex, src/dsa_plexk.kokkos.cxx): D per cell
+ * from the void policy (1/(3 sigma_t) outside voids), sigma_a = sigma_t -
+ * sigma_s, VOLUME-weighted rows. Output as COO (row, col, val) with the
+ * reference's entry order per row; a masked void's zeroed couplings are left
+ * out.
  * ~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~ */
+
+/* The void policy of DSAPrecon::assemble (src/dsak.kokkos.cxx:233-345) with
+ * DSAPlex::void_volume_surface (src/dsa_plexk.kokkos.cxx:243-262), one rank,
+ * a backend that can mask. A cell is void when sigma_t <= void_sigma_t. With
+ * bridging asked for and some void, some non-void, and a vacuum face or some
+ * absorption anywhere, the voids are bridged when their mean chord 4 V / S
+ * is positive (S: the void cells' faces onto non-void cells or vacuum
+ * sides). D = 1/(3 sigma_t) outside voids; in a bridged void void_d if > 0,
+ * else 1/(3 (max(sigma_t, 0) + 1/chord)); 0 in an unbridged void, which is
+ * masked. Fills is_void, masked, d; out[0] = bridged, out[1] = chord,
+ * out[2] = number of void cells. Returns 1 where the operator would be
+ * singular (every face reflective, no void and no absorption), else 0. */
+int oracle_dsa_void_policy(int F, int64_t n_cells, const double *face_nA, const int64_t *face_nbr,
+                           const int32_t *face_bc, const double *volume, const double *sigma_t,
+                           const double *sigma_s, double void_sigma_t, int bridge, double void_d,
+                           uint8_t *is_void, uint8_t *masked, double *d, double *out)
+{
+   int64_t n_void = 0;
+   double max_sa_all = 0.0, max_sa_solid = 0.0;
+   int any_vacuum = 0;
+   for (int64_t k = 0; k < n_cells * F; k++)
+      if (face_nbr[k] < 0 && face_bc[k] == BC_VACUUM) any_vacuum = 1;
+   for (int64_t c = 0; c < n_cells; c++) {
+      const double sa = sigma_t[c] - sigma_s[c];
+      is_void[c] = sigma_t[c] <= void_sigma_t;
+      if (is_void[c]) n_void++;
+      else if (sa > max_sa_solid) max_sa_solid = sa;
+      if (sa > max_sa_all) max_sa_all = sa;
+   }
+   int bridged = 0;
+   double chord = 0.0;
+   if (bridge && n_void > 0 && n_void < n_cells && (any_vacuum || max_sa_all > 0.0)) {
+      double vs0 = 0.0, vs1 = 0.0;
+      for (int64_t c = 0; c < n_cells; c++) {
+         if (!is_void[c]) continue;
+         vs0 += volume[c];
+         for (int f = 0; f < F; f++) {
+            const int64_t k = c * F + f;
+            const int64_t n = face_nbr[k];
+            if (n >= 0 ? !is_void[n] : face_bc[k] == BC_VACUUM) {
+               double area = 0.0;
+               for (int dd = 0; dd < 3; dd++) area += face_nA[3 * k + dd] * face_nA[3 * k + dd];
+               vs1 += sqrt(area);
+            }
+         }
+      }
+      chord = vs1 > 0.0 ? 4.0 * vs0 / vs1 : 0.0;
+      bridged = chord > 0.0;
+   }
+   for (int64_t c = 0; c < n_cells; c++) {
+      if (!is_void[c]) d[c] = 1.0 / (3.0 * sigma_t[c]);
+      else if (bridged) d[c] = void_d > 0.0 ? void_d : 1.0 / (3.0 * ((sigma_t[c] > 0.0 ? sigma_t[c] : 0.0) + 1.0 / chord));
+      else d[c] = 0.0;
+      masked[c] = is_void[c] && !bridged;
+   }
+   out[0] = bridged;
+   out[1] = chord;
+   out[2] = (double)n_void;
+   const double sa = bridged ? max_sa_all : max_sa_solid;
+   return (any_vacuum || n_void > 0 || sa > 0.0) ? 0 : 1;
+}
 
 /* The MIP interior-penalty form at DG1 (assemble_dg1, :365-475); penalty C.
  * Returns the number of entries written. */
@@ -666,12 +729,23 @@ int64_t oracle_dsa_mip(int nb, int F, int64_t n_cells, const double *face_nA, co
                        const int32_t *face_bc, const double *face_distance, const double *volume,
                        const double *face_own, const double *face_up, const double *basis_grad,
                        const double *face_nb_grad, const double *sigma_t, const double *sigma_s, double penalty,
+                       const double *d_cell, const uint8_t *is_void, const uint8_t *masked, int bridged,
                        int64_t *ri, int64_t *ci, double *v)
 {
    int64_t e = 0;
    for (int64_t c = 0; c < n_cells; c++) {
       const double vol = volume[c];
-      const double d_c = 1.0 / (3.0 * sigma_t[c]);
+      if (masked[c]) {
+         /* A masked void: V times the identity block, every coupling zero */
+         for (int i = 0; i < nb; i++)
+            for (int j = 0; j < nb; j++) {
+               ri[e] = c * nb + i;
+               ci[e] = c * nb + j;
+               v[e++] = i == j ? vol : 0.0;
+            }
+         continue;
+      }
+      const double d_c = d_cell[c];
       const double sigma_a = sigma_t[c] - sigma_s[c];
       double own[MAXB][MAXB];
       for (int i = 0; i < nb; i++)
@@ -682,8 +756,10 @@ int64_t oracle_dsa_mip(int nb, int F, int64_t n_cells, const double *face_nA, co
          }
       for (int k = 0; k < F; k++) {
          const int64_t kf = c * F + k;
-         const int interior = face_nbr[kf] >= 0;
-         if (!interior && face_bc[kf] != BC_VACUUM) continue;
+         /* A face into a masked void is a vacuum face, as if the mesh stopped there */
+         const int has_nb = face_nbr[kf] >= 0;
+         const int interior = has_nb && !masked[face_nbr[kf]];
+         if (!has_nb && face_bc[kf] != BC_VACUUM) continue;
          double area = 0.0, nrm[3];
          for (int d = 0; d < 3; d++) area += face_nA[3 * kf + d] * face_nA[3 * kf + d];
          area = sqrt(area);
@@ -702,17 +778,22 @@ int64_t oracle_dsa_mip(int nb, int F, int64_t n_cells, const double *face_nA, co
          const double h_c = 2.0 * face_distance[2 * kf];
          if (interior) {
             const int64_t n = face_nbr[kf];
-            const double d_n = 1.0 / (3.0 * sigma_t[n]);
             const double h_n = 2.0 * face_distance[2 * kf + 1];
-            double kappa = 0.5 * penalty * (d_c / h_c + d_n / h_n);
+            /* A face touching a bridged void: both sides take the face's harmonic D */
+            double dc_f = d_c, dn_f = d_cell[n];
+            if (bridged && (is_void[c] || is_void[n])) {
+               dc_f = 2.0 * d_c * d_cell[n] / (d_c + d_cell[n]);
+               dn_f = dc_f;
+            }
+            double kappa = 0.5 * penalty * (dc_f / h_c + dn_f / h_n);
             if (kappa < 0.25) kappa = 0.25;
             for (int i = 0; i < nb; i++) {
                const double m_i = scale * fo[i * nb];
                for (int j = 0; j < nb; j++) {
-                  own[i][j] += kappa * scale * fo[i * nb + j] - 0.5 * d_c * gc[j] * m_i - 0.5 * d_c * gc[i] * scale * fo[j];
+                  own[i][j] += kappa * scale * fo[i * nb + j] - 0.5 * dc_f * gc[j] * m_i - 0.5 * dc_f * gc[i] * scale * fo[j];
                   ri[e] = c * nb + i;
                   ci[e] = n * nb + j;
-                  v[e++] = -kappa * scale * fu[i * nb + j] - 0.5 * d_n * gn[j] * m_i + 0.5 * d_c * gc[i] * scale * fu[j];
+                  v[e++] = -kappa * scale * fu[i * nb + j] - 0.5 * dn_f * gn[j] * m_i + 0.5 * dc_f * gc[i] * scale * fu[j];
                }
             }
          } else {
@@ -761,11 +842,19 @@ static double blend_d(double d, double m, double p)
 int64_t oracle_dsa_dg0(int F, int64_t n_cells, int A, const double *face_nA, const int64_t *face_nbr,
                        const int32_t *face_bc, const double *face_distance, const double *volume,
                        const double *omega, const double *w, double sum_weights, const double *sigma_t,
-                       const double *sigma_s, int consistent, double power, int64_t *ri, int64_t *ci, double *v)
+                       const double *sigma_s, int consistent, double power, const double *d_cell,
+                       const uint8_t *masked, int64_t *ri, int64_t *ci, double *v)
 {
    int64_t e = 0;
    for (int64_t c = 0; c < n_cells; c++) {
-      const double d_c = 1.0 / (3.0 * sigma_t[c]);
+      if (masked[c]) {
+         /* A masked void: V on the diagonal, couplings zero */
+         ri[e] = c;
+         ci[e] = c;
+         v[e++] = volume[c];
+         continue;
+      }
+      const double d_c = d_cell[c];
       double diag = volume[c] * (sigma_t[c] - sigma_s[c]);
       for (int k = 0; k < F; k++) {
          const int64_t kf = c * F + k;
@@ -774,9 +863,13 @@ int64_t oracle_dsa_dg0(int F, int64_t n_cells, int A, const double *face_nA, con
          area = sqrt(area);
          const double hr = half_range(A, omega, w, sum_weights, face_nA, kf, area);
          const double d_own = face_distance[2 * kf];
-         if (face_nbr[kf] >= 0) {
+         if (face_nbr[kf] >= 0 && masked[face_nbr[kf]]) {
+            /* A face into a masked void: no coupling, the vacuum face's Marshak term */
+            const double d_b = consistent ? blend_d(d_c, 2.0 * d_own * hr, power) : d_c;
+            diag += area / (2.0 + d_own / d_b);
+         } else if (face_nbr[kf] >= 0) {
             const int64_t n = face_nbr[kf];
-            const double d_n = 1.0 / (3.0 * sigma_t[n]);
+            const double d_n = d_cell[n];
             double t_f = area / (d_own / d_c + face_distance[2 * kf + 1] / d_n);
             if (consistent) {
                const double len = d_own + face_distance[2 * kf + 1];
@@ -799,19 +892,22 @@ int64_t oracle_dsa_dg0(int F, int64_t n_cells, int A, const double *face_nA, con
 }
 
 /* R: rhs(node) = V_c sum_a w_a x(node, a); P: y(node, a) = u(node) / W
- * (RestrictKernel / ProlongKernel, src/dsak.kokkos.cxx:20-62, no BC rows) */
+ * (RestrictKernel / ProlongKernel, src/dsak.kokkos.cxx:20-62, no BC rows).
+ * A masked void's nodes restrict to zero and its rows prolong to zero;
+ * masked may be NULL (no voids). */
 void oracle_dsa_restrict(int64_t n_cells, int nb, int A, const double *w, const double *volume, const double *x,
-                         double *rhs)
+                         const uint8_t *masked, double *rhs)
 {
    for (int64_t n = 0; n < n_cells * nb; n++) {
       double s = 0.0;
       for (int a = 0; a < A; a++) s += w[a] * x[n * A + a];
-      rhs[n] = s * volume[n / nb];
+      rhs[n] = (masked && masked[n / nb]) ? 0.0 : s * volume[n / nb];
    }
 }
 
-void oracle_dsa_prolong(int64_t n_cells, int nb, int A, double sum_weights, const double *u, double *y)
+void oracle_dsa_prolong(int64_t n_cells, int nb, int A, double sum_weights, const double *u, const uint8_t *masked,
+                        double *y)
 {
    for (int64_t n = 0; n < n_cells * nb; n++)
-      for (int a = 0; a < A; a++) y[n * A + a] = u[n] / sum_weights;
+      for (int a = 0; a < A; a++) y[n * A + a] = (masked && masked[n / nb]) ? 0.0 : u[n] / sum_weights;
 }

@@ -164,12 +164,14 @@ _sig("ubolt_gradient", C.c_int, vp, vp, vp, vp, vp, vp)
 
 class DsaOptions(C.Structure):
     _fields_ = [("penalty", C.c_double), ("consistent_power", C.c_double), ("consistent_d", C.c_int32),
-                ("inner_iterations", C.c_int32)]
+                ("inner_iterations", C.c_int32), ("void_sigma_t", C.c_double), ("void_d", C.c_double),
+                ("void_bridge", C.c_int32), ("pad_", C.c_int32)]
 
 
 _sig("ubolt_dsa_defaults", None, C.POINTER(DsaOptions))
 _sig("ubolt_dsa_setup", C.c_int, vp, C.POINTER(DGGeometry), C.POINTER(DsaOptions))
 _sig("ubolt_dsa_set_group", C.c_int, vp, vp)
+_sig("ubolt_dsa_void_info", C.c_int, vp, i64p, C.POINTER(C.c_int32), dp)
 _sig("ubolt_dsa_apply", C.c_int, vp, vp, vp, vp)
 _sig("ubolt_dsa_apply_static", C.c_int, vp, vp, vp, vp)
 _sig("ubolt_dsa_spmv", C.c_int, vp, vp, vp, vp)

@@ -9,9 +9,13 @@
 //           floor 1/4 (DSAPlex::assemble_dg1, dsa_plexk.kokkos.cxx:365-475);
 //      DG0: the two-point flux with the consistent-D blend
 //           (D^p + (m h)^p)^(1/p), p = 1.5 (assemble_dg0, :288-348).
-// Voids (sigma_t <= 0) are refused: none of the workloads has one, and the
-// bridge/mask policy of DSAPrecon::assemble (dsak.kokkos.cxx:233-345) is
-// not restated.
+// Voids follow DSAPrecon::assemble's policy (dsak.kokkos.cxx:233-345), on
+// one rank of a backend that can mask: a cell with sigma_t <= void_sigma_t
+// is void; the voids are bridged (D = 1/(3 (sigma_t + 1/L)), L their mean
+// chord 4 V / S, or a fixed void D) when that is asked for and leaves the
+// operator nonsingular, else masked: V times the identity, no coupling, a
+// face into one is a vacuum face, and R and P skip its nodes
+// (dsa_plexk.kokkos.cxx:288-475, RestrictKernel/ProlongKernel).
 //
 // As in the reference the matrix is refilled on the host per group (a host
 // loop) and uploaded; here into a block-ELL layout - per cell its F neighbour
@@ -33,6 +37,16 @@ struct ubolt_dsa {
    double penalty = 4.0, power = 1.5;
    int consistent = 1, inner_its = 30;
    bool assembled = false;
+   // The void policy: options, the boundary's vacuum faces, and this group's outcome
+   double void_sigma_t = 0.0, void_d = 0.0;
+   int void_bridge = 1;
+   bool any_vacuum = false;
+   int64_t n_void = 0;
+   int bridged = 0;
+   double chord = 0.0;
+   std::vector<uint8_t> h_void, h_mask;
+   std::vector<double> h_d;
+   uint8_t *mask = nullptr;  // device, per cell: a masked void
    // Host geometry (the backend data DSAPlex::create keeps)
    std::vector<double> area, nrm, dist, volume, fown, fup, bgrad, nbgrad, half_range;
    std::vector<int64_t> nbr;
@@ -75,10 +89,12 @@ __global__ void DsaSpmvKernel(int64_t n_nodes, int nb, int F, const int32_t *__r
 }
 
 // rhs(node) = V_c sum_a w_a (x(node, a) - ax(node, a)); ax may be NULL. Warp per node.
+// A masked void's nodes restrict to zero (mask may be NULL: none).
 template <typename T>
 __global__ void DsaRestrictKernel(int64_t n_nodes, int nb, int A, const double *__restrict__ w,
                                   const double *__restrict__ volume, const T *__restrict__ x,
-                                  const T *__restrict__ ax, double *__restrict__ rhs)
+                                  const T *__restrict__ ax, const uint8_t *__restrict__ mask,
+                                  double *__restrict__ rhs)
 {
    const int64_t node = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
    const int lane = threadIdx.x & 31;
@@ -91,17 +107,17 @@ __global__ void DsaRestrictKernel(int64_t n_nodes, int nb, int A, const double *
    }
 #pragma unroll
    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-   if (lane == 0) rhs[node] = s * volume[node / nb];
+   if (lane == 0) rhs[node] = (mask && mask[node / nb]) ? 0.0 : s * volume[node / nb];
 }
 
-// y(node, a) (+)= u(node) / W
+// y(node, a) (+)= u(node) / W; a masked void's rows get zero (mask may be NULL)
 template <typename T>
-__global__ void DsaProlongKernel(int64_t n_rows, int A, double inv_w, const double *__restrict__ u, T *__restrict__ y,
-                                 int add)
+__global__ void DsaProlongKernel(int64_t n_rows, int nb, int A, double inv_w, const double *__restrict__ u,
+                                 const uint8_t *__restrict__ mask, T *__restrict__ y, int add)
 {
    const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
    if (r >= n_rows) return;
-   const double v = u[r / A] * inv_w;
+   const double v = (mask && mask[r / ((int64_t)nb * A)]) ? 0.0 : u[r / A] * inv_w;
    y[r] = add ? (T)((double)y[r] + v) : (T)v;
 }
 
@@ -218,33 +234,97 @@ static double BlendD(double d, double m, double p)
    return std::pow(std::pow(d, p) + std::pow(m, p), 1.0 / p);
 }
 
+// The void policy for one group (DSAPrecon::assemble, dsak.kokkos.cxx:233-345,
+// with DSAPlex::void_volume_surface, dsa_plexk.kokkos.cxx:243-262): the
+// census, the bridge decision and the voids' mean chord, D per cell and the
+// mask, and the guard against a singular operator.
+static int VoidPolicy(ubolt_dsa *ds, const double *st, const double *ss)
+{
+   const int F = ds->F;
+   const int64_t nc = ds->nc;
+   ds->h_void.assign(nc, 0);
+   ds->h_mask.assign(nc, 0);
+   ds->h_d.assign(nc, 0.0);
+   int64_t n_void = 0;
+   // The largest sigma_a anywhere, and outside the voids
+   double max_sa_all = 0.0, max_sa_solid = 0.0;
+   for (int64_t c = 0; c < nc; c++) {
+      const double sa = st[c] - ss[c];
+      ds->h_void[c] = st[c] <= ds->void_sigma_t;
+      if (ds->h_void[c]) n_void++;
+      else max_sa_solid = std::max(max_sa_solid, sa);
+      max_sa_all = std::max(max_sa_all, sa);
+   }
+   // Bridge when asked, some cell is void and some is not, and a vacuum face
+   // or some absorption holds the bridged operator; bridged iff a face ends
+   // a flight through the voids (their chord is positive)
+   ds->bridged = 0;
+   ds->chord = 0.0;
+   if (ds->void_bridge && n_void > 0 && n_void < nc && (ds->any_vacuum || max_sa_all > 0.0)) {
+      double vol = 0.0, surf = 0.0;
+      for (int64_t c = 0; c < nc; c++) {
+         if (!ds->h_void[c]) continue;
+         vol += ds->volume[c];
+         for (int f = 0; f < F; f++) {
+            const int64_t k = c * F + f;
+            const int64_t n = ds->nbr[k];
+            if (n >= 0 ? !ds->h_void[n] : ds->bc[k] == UBOLT_BC_VACUUM) surf += ds->area[k];
+         }
+      }
+      ds->chord = surf > 0.0 ? 4.0 * vol / surf : 0.0;
+      ds->bridged = ds->chord > 0.0;
+   }
+   // D: 1/(3 sigma_t); in a bridged void 1/3 of the flight 1/(sigma_t + 1/L)
+   // unless a void D is fixed; 0 in an unbridged void, which is masked
+   for (int64_t c = 0; c < nc; c++) {
+      if (!ds->h_void[c]) ds->h_d[c] = 1.0 / (3.0 * st[c]);
+      else if (ds->bridged)
+         ds->h_d[c] = ds->void_d > 0.0 ? ds->void_d : 1.0 / (3.0 * (std::max(st[c], 0.0) + 1.0 / ds->chord));
+      ds->h_mask[c] = ds->h_void[c] && !ds->bridged;
+   }
+   ds->n_void = n_void;
+   // Every face reflective (pure Neumann): only absorption, or a masked void
+   // (whose faces are Marshak faces), keeps the operator nonsingular
+   const double sa = ds->bridged ? max_sa_all : max_sa_solid;
+   if (!(ds->any_vacuum || n_void > 0 || sa > 0.0))
+      return SetError(UBOLT_ERR_ARG,
+                      "the DSA diffusion operator is singular: every face is reflective, there is no void, and "
+                      "sigma_a = sigma_t - sigma_s is zero everywhere in this group");
+   return UBOLT_OK;
+}
+
 // Fill the block-ELL values and the block-Jacobi inverses for one group.
 static int Assemble(ubolt_dsa *ds, const double *st, const double *ss)
 {
    const int nb = ds->nb, F = ds->F;
    const int64_t nc = ds->nc;
    const size_t bs = (size_t)nb * nb;
+   int rc = VoidPolicy(ds, st, ss);
+   if (rc) return rc;
    ds->h_val.assign(nc * (F + 1) * bs, 0.0);
    ds->h_jinv.assign(nc * bs, 0.0);
-   int bad = 0;
+   const double *dcell = ds->h_d.data();
+   const uint8_t *masked = ds->h_mask.data(), *is_void = ds->h_void.data();
 #pragma omp parallel for schedule(static)
    for (int64_t c = 0; c < nc; c++) {
-      if (!(st[c] > 0.0)) {
-         bad = 1;
-         continue;
-      }
       double *blk = &ds->h_val[c * (F + 1) * bs];
       double *own = blk + F * bs;
       const double vol = ds->volume[c];
-      const double d_c = 1.0 / (3.0 * st[c]);
+      if (masked[c]) {
+         // A masked void: V times the identity, every coupling zero
+         for (int i = 0; i < nb; i++) own[i * nb + i] = vol;
+         InvertSmall(nb, own, &ds->h_jinv[c * bs]);
+         continue;
+      }
+      const double d_c = dcell[c];
       if (nb == 1) {
          double diag = vol * (st[c] - ss[c]);
          for (int f = 0; f < F; f++) {
             const int64_t k = c * F + f;
             const double d_own = ds->dist[2 * k];
-            if (ds->nbr[k] >= 0) {
-               const int64_t n = ds->nbr[k];
-               const double d_n = 1.0 / (3.0 * st[n]);
+            const int64_t n = ds->nbr[k];
+            if (n >= 0 && !masked[n]) {
+               const double d_n = dcell[n];
                double t_f = ds->area[k] / (d_own / d_c + ds->dist[2 * k + 1] / d_n);
                if (ds->consistent) {
                   const double len = d_own + ds->dist[2 * k + 1];
@@ -252,7 +332,8 @@ static int Assemble(ubolt_dsa *ds, const double *st, const double *ss)
                }
                blk[f] = -t_f;
                diag += t_f;
-            } else if (ds->bc[k] == UBOLT_BC_VACUUM) {
+            } else if (n >= 0 || ds->bc[k] == UBOLT_BC_VACUUM) {
+               // A vacuum side, or a face into a masked void: Marshak
                const double d_b = ds->consistent ? BlendD(d_c, 2.0 * d_own * ds->half_range[k], ds->power) : d_c;
                diag += ds->area[k] / (2.0 + d_own / d_b);
             }
@@ -268,8 +349,10 @@ static int Assemble(ubolt_dsa *ds, const double *st, const double *ss)
             }
          for (int f = 0; f < F; f++) {
             const int64_t k = c * F + f;
-            const bool interior = ds->nbr[k] >= 0;
-            if (!interior && ds->bc[k] != UBOLT_BC_VACUUM) continue;
+            const int64_t n = ds->nbr[k];
+            // A face into a masked void is a vacuum face, as if the mesh stopped there
+            const bool interior = n >= 0 && !masked[n];
+            if (n < 0 && ds->bc[k] != UBOLT_BC_VACUUM) continue;
             const double scale = vol * ds->area[k];
             const double *fo = &ds->fown[k * bs], *fu = &ds->fup[k * bs];
             double gc[4], gn[4];
@@ -282,17 +365,23 @@ static int Assemble(ubolt_dsa *ds, const double *st, const double *ss)
             }
             const double h_c = 2.0 * ds->dist[2 * k];
             if (interior) {
-               const double d_n = 1.0 / (3.0 * st[ds->nbr[k]]);
                const double h_n = 2.0 * ds->dist[2 * k + 1];
-               const double kappa = std::max(0.5 * ds->penalty * (d_c / h_c + d_n / h_n), 0.25);
+               // A face touching a bridged void: both sides take the face's
+               // harmonic D, in the averages and in kappa
+               double dc_f = d_c, dn_f = dcell[n];
+               if (ds->bridged && (is_void[c] || is_void[n])) {
+                  dc_f = 2.0 * d_c * dcell[n] / (d_c + dcell[n]);
+                  dn_f = dc_f;
+               }
+               const double kappa = std::max(0.5 * ds->penalty * (dc_f / h_c + dn_f / h_n), 0.25);
                double *nbb = blk + f * bs;
                for (int i = 0; i < nb; i++) {
                   const double m_i = scale * fo[i * nb];
                   for (int j = 0; j < nb; j++) {
-                     own[i * nb + j] += kappa * scale * fo[i * nb + j] - 0.5 * d_c * gc[j] * m_i -
-                                        0.5 * d_c * gc[i] * scale * fo[j];
-                     nbb[i * nb + j] = -kappa * scale * fu[i * nb + j] - 0.5 * d_n * gn[j] * m_i +
-                                       0.5 * d_c * gc[i] * scale * fu[j];
+                     own[i * nb + j] += kappa * scale * fo[i * nb + j] - 0.5 * dc_f * gc[j] * m_i -
+                                        0.5 * dc_f * gc[i] * scale * fo[j];
+                     nbb[i * nb + j] = -kappa * scale * fu[i * nb + j] - 0.5 * dn_f * gn[j] * m_i +
+                                       0.5 * dc_f * gc[i] * scale * fu[j];
                   }
                }
             } else {
@@ -308,7 +397,6 @@ static int Assemble(ubolt_dsa *ds, const double *st, const double *ss)
       }
       InvertSmall(nb, own, &ds->h_jinv[c * bs]);
    }
-   if (bad) return SetError(UBOLT_ERR_ARG, "DSA: a cell has sigma_t <= 0 (voids are not supported)");
    return UBOLT_OK;
 }
 
@@ -330,6 +418,12 @@ int DsaSolveOnDevice(ubolt_ctx *ctx, cudaStream_t s)
       CountLaunch(5);
    }
    return CheckLaunch("dsa solve");
+}
+
+// The per-cell void mask of the current group, or NULL (no DSA filled, or no masked void)
+static const uint8_t *DsaMask(const ubolt_ctx *ctx)
+{
+   return (ctx->dsa && ctx->dsa->assembled) ? ctx->dsa->mask : nullptr;
 }
 
 static int CheckDsa(ubolt_ctx *ctx)
@@ -355,11 +449,11 @@ int DsaCorrect(ubolt_ctx *ctx, const T *r, T *y, T *tmp, void *stream)
    if ((rc = OperatorApply<T>(ctx, false, y, tmp, stream))) return rc;
    const int64_t threads = ds->n_nodes * 32;
    DsaRestrictKernel<T><<<(threads + 255) / 256, 256, 0, s>>>(ds->n_nodes, ds->nb, ctx->A, ctx->g64.w, ctx->d_volume,
-                                                              r, tmp, ds->rhs);
+                                                              r, tmp, ds->mask, ds->rhs);
    CountLaunch();
    if ((rc = DsaSolveOnDevice(ctx, s))) return rc;
-   DsaProlongKernel<T><<<(ctx->n_rows + 255) / 256, 256, 0, s>>>(ctx->n_rows, ctx->A, 1.0 / ctx->sum_weights, ds->u,
-                                                                  y, 1);
+   DsaProlongKernel<T><<<(ctx->n_rows + 255) / 256, 256, 0, s>>>(ctx->n_rows, ds->nb, ctx->A, 1.0 / ctx->sum_weights,
+                                                                  ds->u, ds->mask, y, 1);
    return CheckLaunch("dsa correct");
 }
 template int DsaCorrect<double>(ubolt_ctx *, const double *, double *, double *, void *);
@@ -374,7 +468,7 @@ void UboltDsaFree(ubolt_ctx *ctx)
    ubolt_dsa *ds = ctx->dsa;
    if (!ds) return;
    for (void *p : {(void *)ds->val, (void *)ds->jinv, (void *)ds->rhs, (void *)ds->u, (void *)ds->r, (void *)ds->z,
-                   (void *)ds->p, (void *)ds->q, (void *)ds->scal})
+                   (void *)ds->p, (void *)ds->q, (void *)ds->scal, (void *)ds->mask})
       if (p) cudaFree(p);
    delete ds;
    ctx->dsa = nullptr;
@@ -387,6 +481,10 @@ extern "C" void ubolt_dsa_defaults(ubolt_dsa_options *o)
    o->consistent_power = 1.5;
    o->consistent_d = 1;
    o->inner_iterations = 30;
+   o->void_sigma_t = 0.0;
+   o->void_d = 0.0;
+   o->void_bridge = 1;
+   o->pad_ = 0;
 }
 
 extern "C" int ubolt_dsa_setup(ubolt_ctx *ctx, const ubolt_dg_geometry *g, const ubolt_dsa_options *opts)
@@ -405,6 +503,7 @@ extern "C" int ubolt_dsa_setup(ubolt_ctx *ctx, const ubolt_dg_geometry *g, const
    if (!(o.penalty > 0.0)) return SetError(UBOLT_ERR_ARG, "dsa penalty must be positive, got %g", o.penalty);
    if (!(o.consistent_power >= 1.0)) return SetError(UBOLT_ERR_ARG, "consistent-D power must be >= 1");
    if (o.inner_iterations < 1 || o.inner_iterations > 10000) return SetError(UBOLT_ERR_ARG, "inner iterations");
+   if (!(o.void_d >= 0.0)) return SetError(UBOLT_ERR_ARG, "void D must be >= 0 (0: from the voids' chord)");
    UboltDsaFree(ctx);
    auto ds = new ubolt_dsa();
    ctx->dsa = ds;
@@ -418,10 +517,15 @@ extern "C" int ubolt_dsa_setup(ubolt_ctx *ctx, const ubolt_dg_geometry *g, const
    ds->consistent = o.consistent_d;
    ds->power = o.consistent_power;
    ds->inner_its = o.inner_iterations;
+   ds->void_sigma_t = o.void_sigma_t;
+   ds->void_d = o.void_d;
+   ds->void_bridge = o.void_bridge != 0;
    ds->volume.assign(g->volume, g->volume + nc);
    ds->nbr.assign(g->face_neighbour, g->face_neighbour + ns);
    ds->bc.assign(g->face_bc, g->face_bc + ns);
    ds->dist.assign(g->face_distance, g->face_distance + 2 * ns);
+   for (int64_t k = 0; k < ns; k++)
+      if (ds->nbr[k] < 0 && ds->bc[k] == UBOLT_BC_VACUUM) ds->any_vacuum = true;
    ds->area.resize(ns);
    ds->nrm.resize(3 * ns);
    for (int64_t k = 0; k < ns; k++) {
@@ -464,6 +568,12 @@ extern "C" int ubolt_dsa_setup(ubolt_ctx *ctx, const ubolt_dg_geometry *g, const
       UboltDsaFree(ctx);
       return rc;
    }
+   if (cudaMalloc((void **)&ds->mask, std::max<int64_t>(nc, 1)) != cudaSuccess) {
+      cudaGetLastError();
+      ds->mask = nullptr;
+      UboltDsaFree(ctx);
+      return SetError(UBOLT_ERR_NOMEM, "DSA void mask");
+   }
    return UBOLT_OK;
 }
 
@@ -482,8 +592,19 @@ extern "C" int ubolt_dsa_set_group(ubolt_ctx *ctx, void *stream)
    if ((rc = Assemble(ds, st.data(), ss.data()))) return rc;
    cudaMemcpyAsync(ds->val, ds->h_val.data(), ds->h_val.size() * 8, cudaMemcpyHostToDevice, s);
    cudaMemcpyAsync(ds->jinv, ds->h_jinv.data(), ds->h_jinv.size() * 8, cudaMemcpyHostToDevice, s);
+   cudaMemcpyAsync(ds->mask, ds->h_mask.data(), ds->nc, cudaMemcpyHostToDevice, s);
    if ((rc = CudaCheck(cudaStreamSynchronize(s), "dsa upload"))) return rc;
    ds->assembled = true;
+   return UBOLT_OK;
+}
+
+extern "C" int ubolt_dsa_void_info(ubolt_ctx *ctx, int64_t *n_void, int32_t *bridged, double *chord)
+{
+   int rc = CheckReady(ctx, false);
+   if (rc || (rc = CheckDsa(ctx))) return rc;
+   if (n_void) *n_void = ctx->dsa->n_void;
+   if (bridged) *bridged = ctx->dsa->bridged;
+   if (chord) *chord = ctx->dsa->chord;
    return UBOLT_OK;
 }
 
@@ -506,7 +627,7 @@ extern "C" int ubolt_dsa_restrict(ubolt_ctx *ctx, const double *x, double *rhs, 
    if (!x || !rhs) return SetError(UBOLT_ERR_ARG, "dsa_restrict: NULL array");
    const int64_t threads = ctx->n_nodes * 32;
    DsaRestrictKernel<double><<<(threads + 255) / 256, 256, 0, (cudaStream_t)stream>>>(
-      ctx->n_nodes, ctx->nb, ctx->A, ctx->g64.w, ctx->d_volume, x, nullptr, rhs);
+      ctx->n_nodes, ctx->nb, ctx->A, ctx->g64.w, ctx->d_volume, x, nullptr, DsaMask(ctx), rhs);
    return CheckLaunch("dsa_restrict");
 }
 
@@ -516,7 +637,7 @@ extern "C" int ubolt_dsa_prolong(ubolt_ctx *ctx, const double *u, double *y, voi
    if (rc) return rc;
    if (!u || !y) return SetError(UBOLT_ERR_ARG, "dsa_prolong: NULL array");
    DsaProlongKernel<double><<<(ctx->n_rows + 255) / 256, 256, 0, (cudaStream_t)stream>>>(
-      ctx->n_rows, ctx->A, 1.0 / ctx->sum_weights, u, y, 0);
+      ctx->n_rows, ctx->nb, ctx->A, 1.0 / ctx->sum_weights, u, DsaMask(ctx), y, 0);
    return CheckLaunch("dsa_prolong");
 }
 
@@ -529,11 +650,11 @@ extern "C" int ubolt_dsa_apply(ubolt_ctx *ctx, const double *x, double *y, void 
    ubolt_dsa *ds = ctx->dsa;
    const int64_t threads = ds->n_nodes * 32;
    DsaRestrictKernel<double><<<(threads + 255) / 256, 256, 0, s>>>(ds->n_nodes, ds->nb, ctx->A, ctx->g64.w,
-                                                                   ctx->d_volume, x, nullptr, ds->rhs);
+                                                                   ctx->d_volume, x, nullptr, ds->mask, ds->rhs);
    CountLaunch();
    if ((rc = DsaSolveOnDevice(ctx, s))) return rc;
-   DsaProlongKernel<double><<<(ctx->n_rows + 255) / 256, 256, 0, s>>>(ctx->n_rows, ctx->A, 1.0 / ctx->sum_weights,
-                                                                      ds->u, y, 0);
+   DsaProlongKernel<double><<<(ctx->n_rows + 255) / 256, 256, 0, s>>>(ctx->n_rows, ds->nb, ctx->A,
+                                                                      1.0 / ctx->sum_weights, ds->u, ds->mask, y, 0);
    return CheckLaunch("dsa_apply");
 }
 
@@ -606,7 +727,7 @@ extern "C" int ubolt_dsa_apply_static(ubolt_ctx *ctx, const double *x, double *y
    cudaStream_t s = (cudaStream_t)stream;
    const int64_t threads = ds->n_nodes * 32;
    DsaRestrictKernel<double><<<(threads + 255) / 256, 256, 0, s>>>(ds->n_nodes, ds->nb, ctx->A, ctx->g64.w,
-                                                                   ctx->d_volume, x, nullptr, rhs);
+                                                                   ctx->d_volume, x, nullptr, ds->mask, rhs);
    CountLaunch();
    // The same fixed-count block-Jacobi PCG as the workspace path; the
    // scalars are cleared here, every vector is written before it is read
@@ -623,7 +744,7 @@ extern "C" int ubolt_dsa_apply_static(ubolt_ctx *ctx, const double *x, double *y
       CgRotateScalars<<<1, 1, 0, s>>>(scal);
       CountLaunch(5);
    }
-   DsaProlongKernel<double><<<(ctx->n_rows + 255) / 256, 256, 0, s>>>(ctx->n_rows, ctx->A, 1.0 / ctx->sum_weights, u,
-                                                                      y, 0);
+   DsaProlongKernel<double><<<(ctx->n_rows + 255) / 256, 256, 0, s>>>(ctx->n_rows, ds->nb, ctx->A,
+                                                                      1.0 / ctx->sum_weights, u, ds->mask, y, 0);
    return CheckLaunch("dsa_apply_static");
 }

@@ -345,18 +345,26 @@ def solve_groups(ctx, sigma_t, sigma_s, source, side_inflow=None, dsa=None, keep
 class DSAPrecon:
     """The diffusion correction y = P D^{-1} R x (include/ubolt/dsa.hpp)."""
 
-    def __init__(self, ctx, penalty=4.0, consistent_d=True, consistent_power=1.5, inner_iterations=30):
+    def __init__(self, ctx, penalty=4.0, consistent_d=True, consistent_power=1.5, inner_iterations=30,
+                 void_sigma_t=0.0, void_bridge=True, void_d=0.0):
         self.ctx = ctx
         o = _lib.DsaOptions()
         lib.ubolt_dsa_defaults(C.byref(o))
         o.penalty, o.consistent_d, o.consistent_power = penalty, int(consistent_d), consistent_power
         o.inner_iterations = inner_iterations
+        o.void_sigma_t, o.void_bridge, o.void_d = void_sigma_t, int(void_bridge), void_d
         gs = ctx.geometry.struct()
         check(lib.ubolt_dsa_setup(ctx.handle, C.byref(gs), C.byref(o)))
 
     def set_group(self, stream=None):
         """Refill D for the context's current group (call after Context.set_group)."""
         check(lib.ubolt_dsa_set_group(self.ctx.handle, _stream(stream)))
+
+    def void_info(self):
+        """The void policy's outcome for the current group: (void cells, bridged, mean chord)."""
+        n, br, ch = C.c_int64(0), C.c_int32(0), C.c_double(0.0)
+        check(lib.ubolt_dsa_void_info(self.ctx.handle, C.byref(n), C.byref(br), C.byref(ch)))
+        return n.value, bool(br.value), ch.value
 
     def apply(self, x, y=None, stream=None):
         y = torch.empty_like(x) if y is None else y
