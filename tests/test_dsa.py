@@ -145,3 +145,16 @@ def test_gpu_sweep_dsa_solve_is_the_same_answer_in_fewer_iterations():
     assert (x1 - x0).abs().max().item() <= 1e-7 * x0.abs().max().item()
     assert s1["iterations"] < s0["iterations"], (s0["iterations"], s1["iterations"])
     ctx.close()
+
+
+@pytest.mark.gpu
+def test_gpu_dsa_apply_is_deterministic():
+    """The inner PCG's dot products are fixed-order grid sums: two applies of
+    the same input agree bit for bit."""
+    import torch
+    ctx, keep, dsa, g, q, st, ss = _gpu(CASES[0])
+    x = torch.tensor(np.random.default_rng(11).standard_normal(g.n_cells * g.n_basis * q.n_angles), device="cuda")
+    y1 = dsa.apply(x).clone()
+    for _ in range(3):
+        assert torch.equal(dsa.apply(x), y1)
+    ctx.close()

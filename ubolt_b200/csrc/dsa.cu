@@ -55,15 +55,62 @@ struct ubolt_dsa {
    // Device
    double *val = nullptr, *jinv = nullptr;          // [nc][F+1][nb][nb], [nc][nb][nb]
    double *rhs = nullptr, *u = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *q = nullptr;
-   double *scal = nullptr;                         // [0] rho, [1] rho_new, [2] pq
+   // [0] rho, [1] rho_new, [2] pq, [3] the grid sums' block counter (an
+   // unsigned int in a double's slot), then one partial per block
+   double *scal = nullptr;
 };
 
 namespace ubolt {
 
+constexpr int kDsaThreads = 256;
+
+// Scalar slots ahead of the per-block partials
+constexpr int kDsaScalars = 4;
+
+// Deterministic sum of d over the grid into *out: each block's total goes to
+// part[blockIdx.x]; the last block to finish (an integer counter) adds the
+// totals in block order, writes *out and resets the counter. No block waits
+// on another. Every thread of the block must call it.
+__device__ __forceinline__ void GridSum(double d, double *part, unsigned *count, double *out)
+{
+   __shared__ double red[kDsaThreads / 32];
+   __shared__ bool last;
+   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+   for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
+   if (lane == 0) red[warp] = d;
+   __syncthreads();
+   if (threadIdx.x == 0) {
+      double s = 0.0;
+      for (int w = 0; w < nw; w++) s += red[w];
+      part[blockIdx.x] = s;
+      __threadfence();
+      last = atomicAdd(count, 1u) == gridDim.x - 1;
+   }
+   __syncthreads();
+   if (!last) return;
+   __threadfence();
+   double s = 0.0;
+   for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) s += __ldcg(&part[b]);
+#pragma unroll
+   for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+   __syncthreads();
+   if (lane == 0) red[warp] = s;
+   __syncthreads();
+   if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < nw; w++) t += red[w];
+      *out = t;
+      *count = 0;
+   }
+}
+
+__device__ __forceinline__ unsigned *GridCount(double *scal) { return reinterpret_cast<unsigned *>(scal + 3); }
+
 // v = D u over the block-ELL rows, one thread per node
 __global__ void DsaSpmvKernel(int64_t n_nodes, int nb, int F, const int32_t *__restrict__ code,
                               const double *__restrict__ val, const double *__restrict__ u, double *__restrict__ v,
-                              const double *__restrict__ dotw, double *dot_out)
+                              const double *__restrict__ dotw, double *scal)
 {
    const int64_t node = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
    double d = 0.0;
@@ -81,11 +128,8 @@ __global__ void DsaSpmvKernel(int64_t n_nodes, int nb, int F, const int32_t *__r
       v[node] = s;
       if (dotw) d = dotw[node] * s;
    }
-   if (dot_out) {
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
-      if ((threadIdx.x & 31) == 0 && d != 0.0) atomicAdd(dot_out, d);
-   }
+   // scal[2] = (dotw, v), when asked
+   if (scal) GridSum(d, scal + kDsaScalars, GridCount(scal), &scal[2]);
 }
 
 // rhs(node) = V_c sum_a w_a (x(node, a) - ax(node, a)); ax may be NULL. Warp per node.
@@ -141,9 +185,7 @@ __global__ void CgStartKernel(int64_t n_nodes, int nb, const double *__restrict_
       p[node] = zz;
       d = rhs[node] * zz;
    }
-#pragma unroll
-   for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
-   if ((threadIdx.x & 31) == 0 && d != 0.0) atomicAdd(&scal[0], d);
+   GridSum(d, scal + kDsaScalars, GridCount(scal), &scal[0]);
 }
 
 // alpha = rho / pq; u += alpha p; r -= alpha q
@@ -158,7 +200,7 @@ __global__ void CgUpdateKernel(int64_t n_nodes, const double *__restrict__ p, co
    r[node] -= alpha * q[node];
 }
 
-// z = J r; scal[1] += (r, z)
+// z = J r; scal[1] = (r, z)
 __global__ void CgPrecondKernel(int64_t n_nodes, int nb, const double *__restrict__ jinv, const double *__restrict__ r,
                                 double *__restrict__ z, double *scal)
 {
@@ -172,9 +214,7 @@ __global__ void CgPrecondKernel(int64_t n_nodes, int nb, const double *__restric
       z[node] = zz;
       d = r[node] * zz;
    }
-#pragma unroll
-   for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
-   if ((threadIdx.x & 31) == 0 && d != 0.0) atomicAdd(&scal[1], d);
+   GridSum(d, scal + kDsaScalars, GridCount(scal), &scal[1]);
 }
 
 // beta = rho_new / rho; p = z + beta p; rho = rho_new; clear rho_new and pq (one thread does the scalars)
@@ -404,13 +444,13 @@ int DsaSolveOnDevice(ubolt_ctx *ctx, cudaStream_t s)
 {
    ubolt_dsa *ds = ctx->dsa;
    const int64_t nn = ds->n_nodes;
-   const int bl = 256;
+   const int bl = kDsaThreads;
    const int64_t grid = (nn + bl - 1) / bl;
-   cudaMemsetAsync(ds->scal, 0, 4 * sizeof(double), s);
+   cudaMemsetAsync(ds->scal, 0, kDsaScalars * sizeof(double), s);
    CgStartKernel<<<grid, bl, 0, s>>>(nn, ds->nb, ds->jinv, ds->rhs, ds->u, ds->r, ds->z, ds->p, ds->scal);
    CountLaunch();
    for (int it = 0; it < ds->inner_its; it++) {
-      DsaSpmvKernel<<<grid, bl, 0, s>>>(nn, ds->nb, ds->F, ctx->g64.code, ds->val, ds->p, ds->q, ds->p, &ds->scal[2]);
+      DsaSpmvKernel<<<grid, bl, 0, s>>>(nn, ds->nb, ds->F, ctx->g64.code, ds->val, ds->p, ds->q, ds->p, ds->scal);
       CgUpdateKernel<<<grid, bl, 0, s>>>(nn, ds->p, ds->q, ds->u, ds->r, ds->scal);
       CgPrecondKernel<<<grid, bl, 0, s>>>(nn, ds->nb, ds->jinv, ds->r, ds->z, ds->scal);
       CgDirectionKernel<<<grid, bl, 0, s>>>(nn, ds->z, ds->p, ds->scal);
@@ -564,7 +604,7 @@ extern "C" int ubolt_dsa_setup(ubolt_ctx *ctx, const ubolt_dg_geometry *g, const
    const size_t bs = (size_t)nb * nb, nn = (size_t)ds->n_nodes;
    if ((rc = alloc(&ds->val, nc * (F + 1) * bs)) || (rc = alloc(&ds->jinv, nc * bs)) || (rc = alloc(&ds->rhs, nn)) ||
        (rc = alloc(&ds->u, nn)) || (rc = alloc(&ds->r, nn)) || (rc = alloc(&ds->z, nn)) || (rc = alloc(&ds->p, nn)) ||
-       (rc = alloc(&ds->q, nn)) || (rc = alloc(&ds->scal, 4))) {
+       (rc = alloc(&ds->q, nn)) || (rc = alloc(&ds->scal, kDsaScalars + (nn + kDsaThreads - 1) / kDsaThreads))) {
       UboltDsaFree(ctx);
       return rc;
    }
@@ -680,9 +720,9 @@ extern "C" int ubolt_dsa_matrix(ubolt_ctx *ctx, double *blocks)
 namespace {
 
 // Six node vectors (restricted rhs and the PCG's u, r, z, p, q) of at most
-// kStaticDsaNodes nodes each, then 4 scalars
+// kStaticDsaNodes nodes each, then the scalars and one partial sum per block
 constexpr int64_t kStaticDsaNodes = (int64_t)1 << 18;
-constexpr int64_t kStaticDsaDoubles = 6 * kStaticDsaNodes + 4;
+constexpr int64_t kStaticDsaDoubles = 6 * kStaticDsaNodes + kDsaScalars + kStaticDsaNodes / kDsaThreads;
 static __device__ __align__(256) double g_dsa_scratch[kStaticDsaDoubles];
 
 constexpr int kMaxDevices = 64;
@@ -733,11 +773,11 @@ extern "C" int ubolt_dsa_apply_static(ubolt_ctx *ctx, const double *x, double *y
    // scalars are cleared here, every vector is written before it is read
    const int64_t nodes = ds->n_nodes;
    const int64_t grid = (nodes + 255) / 256;
-   cudaMemsetAsync(scal, 0, 4 * sizeof(double), s);
+   cudaMemsetAsync(scal, 0, kDsaScalars * sizeof(double), s);
    CgStartKernel<<<grid, 256, 0, s>>>(nodes, ds->nb, ds->jinv, rhs, u, r, z, p, scal);
    CountLaunch();
    for (int it = 0; it < ds->inner_its; it++) {
-      DsaSpmvKernel<<<grid, 256, 0, s>>>(nodes, ds->nb, ds->F, ctx->g64.code, ds->val, p, q, p, &scal[2]);
+      DsaSpmvKernel<<<grid, 256, 0, s>>>(nodes, ds->nb, ds->F, ctx->g64.code, ds->val, p, q, p, scal);
       CgUpdateKernel<<<grid, 256, 0, s>>>(nodes, p, q, u, r, scal);
       CgPrecondKernel<<<grid, 256, 0, s>>>(nodes, ds->nb, ds->jinv, r, z, scal);
       CgDirectionKernel<<<grid, 256, 0, s>>>(nodes, z, p, scal);
