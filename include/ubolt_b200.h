@@ -406,6 +406,19 @@ int ubolt_solver_setup(ubolt_ctx *ctx, const ubolt_solve_options *opts);
  * Returns UBOLT_ERR_NOT_CONVERGED, with x and stats filled, at max_it. */
 int ubolt_solve(ubolt_ctx *ctx, const double *b, double *x, const ubolt_solve_options *opts,
                 ubolt_solve_stats *stats, void *stream);
+/* n solves of right-hand sides held in HOST memory, x_host[i] = A^{-1}
+ * b_host[i], each as ubolt_solve. The upload of b_host[i + 1] and the
+ * download of x_host[i - 1] run on two copy streams of the context while
+ * solve i runs, through two device buffers each for b and x kept in the
+ * solver's workspace (4 n_rows doubles). The copies overlap the solves
+ * only from page-locked host memory. The first upload waits for the work
+ * already on `stream`; on return `stream` waits for the last download, so
+ * x_host is complete once `stream` is synchronised. stats (n entries, may be
+ * NULL) per solve; every solve starts from zero. Stops at the first solve
+ * that fails, returning its status.
+ * The batched form of TransportSolver::solve over a PETSc host Vec. */
+int ubolt_solve_host_batch(ubolt_ctx *ctx, int n, const double *const *b_host, double *const *x_host,
+                           const ubolt_solve_options *opts, ubolt_solve_stats *stats, void *stream);
 
 /* ~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~
  * Adjoint and gradients. No reference counterpart (the reference has no

@@ -121,6 +121,8 @@ _sig("ubolt_sweep_set_factor_limit", C.c_int, vp, C.c_int64)
 _sig("ubolt_solve_defaults", None, C.POINTER(SolveOptions))
 _sig("ubolt_solver_setup", C.c_int, vp, C.POINTER(SolveOptions))
 _sig("ubolt_solve", C.c_int, vp, vp, vp, C.POINTER(SolveOptions), C.POINTER(SolveStats), vp)
+_sig("ubolt_solve_host_batch", C.c_int, vp, C.c_int, C.POINTER(vp), C.POINTER(vp), C.POINTER(SolveOptions),
+     C.POINTER(SolveStats), vp)
 
 
 class SweepPlanView(C.Structure):

@@ -54,6 +54,19 @@ struct ubolt_solver {
    // scalars alpha[restart + 2] and four reduction slots
    int64_t n_nodes = 0;
    double *Phi = nullptr, *rho = nullptr, *alpha = nullptr, *scal = nullptr;
+   // The solver's small host <-> device values (dot products, scalars, the
+   // update coefficients) pass through mapped page-locked memory, copied by
+   // one-block kernels, not the copy engines: a large host copy on another
+   // stream (a host-buffer batch) would hold a small copy up for its whole
+   // length. First half device -> host, second half host -> device.
+   double *mb_h = nullptr, *mb_d = nullptr;
+   int mb_half = 0;
+   // Host-buffer batches: two device buffers each for b and x, the upload
+   // and download streams, and per buffer the events that order them
+   double *hb[2] = {nullptr, nullptr}, *hx[2] = {nullptr, nullptr};
+   cudaStream_t up = nullptr, down = nullptr;
+   cudaEvent_t entry = nullptr, uploaded[2] = {nullptr, nullptr}, solved[2] = {nullptr, nullptr},
+               downloaded[2] = {nullptr, nullptr};
 };
 
 namespace ubolt {
@@ -171,15 +184,56 @@ static void MultiDot(const ubolt_solver *ws, const S *V, int nv, const S *w, int
    CountLaunch((nv + kChunk - 1) / kChunk + 1);
 }
 
+// y = x on the SMs: a device-to-device cudaMemcpy may go to a copy engine,
+// where a large host copy on another stream would hold it up
+template <typename T>
+__global__ void CopyKernel(const T *__restrict__ x, T *__restrict__ y, int64_t n)
+{
+   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+      y[k] = x[k];
+}
+
+template <typename T>
+static int DeviceCopy(T *y, const T *x, int64_t n, cudaStream_t s, const char *what)
+{
+   CopyKernel<T><<<GridFor(n), 256, 0, s>>>(x, y, n);
+   CountLaunch();
+   return CudaCheck(cudaGetLastError(), what);
+}
+
+__global__ void MailCopyKernel(const double *__restrict__ src, double *__restrict__ dst, int n)
+{
+   for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+}
+
+// Mailbox offsets (doubles) in each half
+constexpr int kMbScalars = 0, kMbH1 = 8;
+
+// n device values to the mailbox at off; read ws->mb_h[off ...] after the stream syncs
+static void ToHost(const ubolt_solver *ws, const double *dev, int off, int n, cudaStream_t s)
+{
+   MailCopyKernel<<<1, 64, 0, s>>>(dev, ws->mb_d + off, n);
+   CountLaunch();
+}
+
+// n host values to the device through the mailbox at off (the previous
+// value at that offset has been consumed: the solver syncs in between)
+static void ToDevice(const ubolt_solver *ws, const double *host, double *dev, int off, int n, cudaStream_t s)
+{
+   double *box = ws->mb_h + ws->mb_half + off;
+   for (int i = 0; i < n; i++) box[i] = host[i];
+   MailCopyKernel<<<1, 64, 0, s>>>(ws->mb_d + ws->mb_half + off, dev, n);
+   CountLaunch();
+}
+
 template <typename S>
 static double Norm(const ubolt_solver *ws, const S *x, int64_t n, cudaStream_t s, int *rc)
 {
    double *slot = ws->h + 3 * (ws->restart + 2) - 1;
    MultiDot<S>(ws, x, 1, x, n, slot, s);
-   double v = 0.0;
-   cudaMemcpyAsync(&v, slot, sizeof v, cudaMemcpyDeviceToHost, s);
+   ToHost(ws, slot, kMbScalars, 1, s);
    *rc = CudaCheck(cudaStreamSynchronize(s), "norm");
-   return std::sqrt(v);
+   return std::sqrt(ws->mb_h[kMbScalars]);
 }
 
 // y(c, i, a) = scale(c) x(c, i, opp(a)): P (the swap of each ordinate with
@@ -227,11 +281,11 @@ static int Precondition(ubolt_ctx *ctx, int pc, bool adjoint, const T *x, T *y, 
       if (rc) return rc;
       OppositeScaleKernel<T><<<grid, 256, 0, s>>>(y, tmp, ctx->d_opp, ctx->d_volume, ctx->nb, ctx->A, n, 0);
       CountLaunch();
-      return CudaCheck(cudaMemcpyAsync(y, tmp, n * sizeof(T), cudaMemcpyDeviceToDevice, s), "adjoint pc");
+      return DeviceCopy<T>(y, tmp, n, s, "adjoint pc");
    }
    switch (pc) {
    case UBOLT_PC_NONE:
-      return CudaCheck(cudaMemcpyAsync(y, x, n * sizeof(T), cudaMemcpyDeviceToDevice, s), "pc copy");
+      return DeviceCopy<T>(y, x, n, s, "pc copy");
    case UBOLT_PC_BLOCK: return BlockApply<T>(ctx, x, y, adjoint, stream);
    case UBOLT_PC_SWEEP: return Sweep<T>(ctx, x, y, stream);
    case UBOLT_PC_SWEEP_DSA: {
@@ -266,7 +320,7 @@ static int Gmres(ubolt_ctx *ctx, const ubolt_solver *ws, S *V, S *Zb, S *z, S *t
    out->converged = false;
    while (out->iterations < max_it) {
       if (x_zero) {
-         rc = CudaCheck(cudaMemcpyAsync(V, b, n * sizeof(S), cudaMemcpyDeviceToDevice, s), "gmres");
+         rc = DeviceCopy<S>(V, b, n, s, "gmres");
          x_zero = false;
       } else {
          rc = OperatorApply<S>(ctx, adjoint, x, V, stream);
@@ -299,9 +353,11 @@ static int Gmres(ubolt_ctx *ctx, const ubolt_solver *ws, S *V, S *Zb, S *z, S *t
          MultiAxpyKernel<S><<<grid, 256, 0, s>>>(V, n, j + 1, dh2, -1.0, vn, 1);
          CountLaunch();
          MultiDot<S>(ws, vn, 1, vn, n, dh2 + j + 1, s);
-         cudaMemcpyAsync(h1.data(), dh1, (j + 1) * sizeof(double), cudaMemcpyDeviceToHost, s);
-         cudaMemcpyAsync(h2.data(), dh2, (j + 2) * sizeof(double), cudaMemcpyDeviceToHost, s);
+         ToHost(ws, dh1, kMbH1, j + 1, s);
+         ToHost(ws, dh2, kMbH1 + (m + 2), j + 2, s);
          if ((rc = CudaCheck(cudaStreamSynchronize(s), "gmres"))) return rc;
+         std::copy(ws->mb_h + kMbH1, ws->mb_h + kMbH1 + j + 1, h1.begin());
+         std::copy(ws->mb_h + kMbH1 + (m + 2), ws->mb_h + kMbH1 + (m + 2) + j + 2, h2.begin());
          out->iterations++;
          const double hn = std::sqrt(h2[j + 1]);
          if (!std::isfinite(hn)) return SetError(UBOLT_ERR_NONFINITE, "GMRES Arnoldi vector is not finite");
@@ -335,7 +391,7 @@ static int Gmres(ubolt_ctx *ctx, const ubolt_solver *ws, S *V, S *Zb, S *z, S *t
          for (int k = i + 1; k < j; k++) tt -= H[i * m + k] * y[k];
          y[i] = tt / H[i * m + i];
       }
-      cudaMemcpyAsync(dy, y.data(), j * sizeof(double), cudaMemcpyHostToDevice, s);
+      ToDevice(ws, y.data(), dy, kMbH1, j, s);
       if (Zb) {
          // Flexible: x += Z y, the preconditioned vectors kept
          MultiAxpyKernel<S><<<grid, 256, 0, s>>>(Zb, n, j, dy, 1.0, x, 1);
@@ -538,7 +594,7 @@ static int GmresIso(ubolt_ctx *ctx, const ubolt_solver *ws, S *work, const S *b,
    out->converged = false;
    while (out->iterations < max_it) {
       if (x_zero) {
-         rc = CudaCheck(cudaMemcpyAsync(r0, b, n * sizeof(S), cudaMemcpyDeviceToDevice, s), "gmres");
+         rc = DeviceCopy<S>(r0, b, n, s, "gmres");
          x_zero = false;
       } else {
          rc = OperatorApply<S>(ctx, adjoint, x, r0, stream);
@@ -551,9 +607,9 @@ static int GmresIso(ubolt_ctx *ctx, const ubolt_solver *ws, S *work, const S *b,
       ReducePartialKernel<<<1, 256, 0, s>>>(ws->partial, igrid, 1, scal);
       CountLaunch(2);
       MultiDot<double>(ws, ws->rho, 1, ws->rho, nn, scal + 1, s);
-      double sc[2] = {0.0, 0.0};
-      cudaMemcpyAsync(sc, scal, sizeof sc, cudaMemcpyDeviceToHost, s);
+      ToHost(ws, scal, kMbScalars, 2, s);
       if ((rc = CudaCheck(cudaStreamSynchronize(s), "gmres"))) return rc;
+      const double sc[2] = {ws->mb_h[kMbScalars], ws->mb_h[kMbScalars + 1]};
       // A residual isotropic to rounding (r_perp below 1e-14 of it: the first
       // cycle of an isotropic source) is taken as isotropic: r_perp = 0, and
       // the sweep reads the node vector alone, not r0
@@ -570,7 +626,7 @@ static int GmresIso(ubolt_ctx *ctx, const ubolt_solver *ws, S *work, const S *b,
       }
       // v_0 = r0 / beta: alpha_0 = 1 / beta, phi_0 = rho / beta
       alpha_h[0] = 1.0 / beta;
-      cudaMemcpyAsync(alpha, alpha_h.data(), sizeof(double), cudaMemcpyHostToDevice, s);
+      ToDevice(ws, alpha_h.data(), alpha, kMbScalars, 1, s);
       ScaleKernel<double, double><<<igrid, 256, 0, s>>>(ws->rho, Phi, 1.0 / beta, nn);
       CountLaunch();
       std::fill(gv.begin(), gv.end(), 0.0);
@@ -584,7 +640,8 @@ static int GmresIso(ubolt_ctx *ctx, const ubolt_solver *ws, S *work, const S *b,
             return rc;
          IsoScatterKernel<S><<<igrid, 256, 0, s>>>(z, wgt, sig_s, 1.0 / ctx->sum_weights, ctx->nb, A, nn, pj, pn);
          CountLaunch();
-         cudaMemcpyAsync(alpha + j + 1, alpha + j, sizeof(double), cudaMemcpyDeviceToDevice, s);
+         MailCopyKernel<<<1, 32, 0, s>>>(alpha + j, alpha + j + 1, 1);
+         CountLaunch();
          // Classical Gram-Schmidt, twice, in the compressed inner product
          for (int pass = 0; pass < 2; pass++) {
             double *dh = pass ? dh2 : dh1;
@@ -594,10 +651,13 @@ static int GmresIso(ubolt_ctx *ctx, const ubolt_solver *ws, S *work, const S *b,
             CountLaunch(2);
          }
          MultiDot<double>(ws, pn, 1, pn, nn, dh2 + j + 1, s);
-         cudaMemcpyAsync(h1.data(), dh1, (j + 1) * sizeof(double), cudaMemcpyDeviceToHost, s);
-         cudaMemcpyAsync(h2.data(), dh2, (j + 2) * sizeof(double), cudaMemcpyDeviceToHost, s);
-         cudaMemcpyAsync(&alpha_h[j + 1], alpha + j + 1, sizeof(double), cudaMemcpyDeviceToHost, s);
+         ToHost(ws, dh1, kMbH1, j + 1, s);
+         ToHost(ws, dh2, kMbH1 + (m + 2), j + 2, s);
+         ToHost(ws, alpha + j + 1, kMbScalars, 1, s);
          if ((rc = CudaCheck(cudaStreamSynchronize(s), "gmres"))) return rc;
+         std::copy(ws->mb_h + kMbH1, ws->mb_h + kMbH1 + j + 1, h1.begin());
+         std::copy(ws->mb_h + kMbH1 + (m + 2), ws->mb_h + kMbH1 + (m + 2) + j + 2, h2.begin());
+         alpha_h[j + 1] = ws->mb_h[kMbScalars];
          out->iterations++;
          const double aw = alpha_h[j + 1];
          const double hn = std::sqrt(aw * aw * rp2 + kappa * h2[j + 1]);
@@ -607,7 +667,7 @@ static int GmresIso(ubolt_ctx *ctx, const ubolt_solver *ws, S *work, const S *b,
             ScaleKernel<double, double><<<igrid, 256, 0, s>>>(pn, pn, 1.0 / hn, nn);
             CountLaunch();
             alpha_h[j + 1] = aw / hn;
-            cudaMemcpyAsync(alpha + j + 1, &alpha_h[j + 1], sizeof(double), cudaMemcpyHostToDevice, s);
+            ToDevice(ws, &alpha_h[j + 1], alpha + j + 1, kMbScalars, 1, s);
          }
          for (int i = 0; i < j; i++) {
             const double tt = cs[i] * H[i * m + j] + sn[i] * H[(i + 1) * m + j];
@@ -634,7 +694,7 @@ static int GmresIso(ubolt_ctx *ctx, const ubolt_solver *ws, S *work, const S *b,
          for (int k = i + 1; k < j; k++) tt -= H[i * m + k] * y[k];
          y[i] = tt / H[i * m + i];
       }
-      cudaMemcpyAsync(dy, y.data(), j * sizeof(double), cudaMemcpyHostToDevice, s);
+      ToDevice(ws, y.data(), dy, kMbH1, j, s);
       MultiAxpyKernel<S><<<grid, 256, 0, s>>>(Zb, n, j, dy, 1.0, x, 1);
       CountLaunch();
       if (out->converged) break;
@@ -650,8 +710,15 @@ static void FreeWorkspace(ubolt_ctx *ctx)
    for (void *p : {(void *)ws->r, (void *)ws->z, (void *)ws->t, (void *)ws->V, (void *)ws->V32, (void *)ws->z32,
                    (void *)ws->b32, (void *)ws->t32, (void *)ws->d32, (void *)ws->Z, (void *)ws->Z32,
                    (void *)ws->partial, (void *)ws->h, (void *)ws->Phi, (void *)ws->rho,
-                   (void *)ws->alpha, (void *)ws->scal})
+                   (void *)ws->alpha, (void *)ws->scal, (void *)ws->hb[0], (void *)ws->hb[1], (void *)ws->hx[0],
+                   (void *)ws->hx[1]})
       if (p) cudaFree(p);
+   if (ws->mb_h) cudaFreeHost(ws->mb_h);
+   for (cudaStream_t st : {ws->up, ws->down})
+      if (st) cudaStreamDestroy(st);
+   for (cudaEvent_t ev : {ws->entry, ws->uploaded[0], ws->uploaded[1], ws->solved[0], ws->solved[1],
+                          ws->downloaded[0], ws->downloaded[1]})
+      if (ev) cudaEventDestroy(ev);
    delete ws;
    ctx->solver = nullptr;
 }
@@ -688,6 +755,12 @@ static int EnsureWorkspace(ubolt_ctx *ctx, const ubolt_solve_options *o)
        (rc = alloc((void **)&ws->t, n * 8)) || (rc = alloc((void **)&ws->partial, (size_t)ws->red_blocks * (m + 2) * 8)) ||
        (rc = alloc((void **)&ws->h, 3 * (size_t)(m + 2) * 8)))
       return rc;
+   ws->mb_half = 16 + 3 * (m + 2);
+   if (cudaHostAlloc((void **)&ws->mb_h, 2 * (size_t)ws->mb_half * 8, cudaHostAllocMapped) != cudaSuccess ||
+       cudaHostGetDevicePointer((void **)&ws->mb_d, ws->mb_h, 0) != cudaSuccess) {
+      cudaGetLastError();
+      return SetError(UBOLT_ERR_NOMEM, "solver workspace: mapped host memory");
+   }
    ws->n_nodes = ctx->n_nodes;
    if (!flexible && ((rc = alloc((void **)&ws->Phi, (size_t)(m + 1) * ws->n_nodes * 8)) ||
                      (rc = alloc((void **)&ws->rho, ws->n_nodes * 8)) ||
@@ -790,7 +863,7 @@ static int SolveSystem(ubolt_ctx *ctx, bool adjoint, const double *b, double *x,
       bool x_zero = o.x_zero != 0;
       for (int outer = 0; outer < o.max_outer; outer++) {
          if (x_zero) {
-            cudaMemcpyAsync(ws->r, b, n * sizeof(double), cudaMemcpyDeviceToDevice, s);
+            if ((rc = DeviceCopy<double>(ws->r, b, n, s, "refinement"))) return rc;
          } else {
             if ((rc = OperatorApply<double>(ctx, adjoint, x, ws->r, stream))) return rc;
             ResidualKernel<double><<<grid, 256, 0, s>>>(b, ws->r, n);
@@ -851,6 +924,79 @@ extern "C" int ubolt_solve(ubolt_ctx *ctx, const double *b, double *x, const ubo
                            ubolt_solve_stats *stats, void *stream)
 {
    return SolveSystem(ctx, false, b, x, opts, stats, stream);
+}
+
+// The batch's device buffers, streams and events, made once per workspace
+static int EnsureHostBatch(ubolt_solver *ws)
+{
+   if (ws->up) return UBOLT_OK;
+   const size_t bytes = (size_t)ws->n * sizeof(double);
+   for (double **p : {&ws->hb[0], &ws->hb[1], &ws->hx[0], &ws->hx[1]}) {
+      if (cudaMalloc((void **)p, bytes) != cudaSuccess) {
+         cudaGetLastError();
+         *p = nullptr;
+         return SetError(UBOLT_ERR_NOMEM, "host batch: cudaMalloc of %zu bytes", bytes);
+      }
+   }
+   int rc = 0;
+   if ((rc = CudaCheck(cudaStreamCreateWithFlags(&ws->up, cudaStreamNonBlocking), "host batch stream")) ||
+       (rc = CudaCheck(cudaStreamCreateWithFlags(&ws->down, cudaStreamNonBlocking), "host batch stream")))
+      return rc;
+   for (cudaEvent_t *ev : {&ws->entry, &ws->uploaded[0], &ws->uploaded[1], &ws->solved[0], &ws->solved[1],
+                           &ws->downloaded[0], &ws->downloaded[1]})
+      if ((rc = CudaCheck(cudaEventCreateWithFlags(ev, cudaEventDisableTiming), "host batch event"))) return rc;
+   return UBOLT_OK;
+}
+
+extern "C" int ubolt_solve_host_batch(ubolt_ctx *ctx, int n, const double *const *b_host, double *const *x_host,
+                                      const ubolt_solve_options *opts, ubolt_solve_stats *stats, void *stream)
+{
+   int rc = CheckReady(ctx, true);
+   if (rc) return rc;
+   if (n < 0 || (n > 0 && (!b_host || !x_host))) return SetError(UBOLT_ERR_ARG, "solve_host_batch: bad arguments");
+   if (n == 0) return UBOLT_OK;
+   for (int i = 0; i < n; i++)
+      if (!b_host[i] || !x_host[i]) return SetError(UBOLT_ERR_ARG, "solve_host_batch: NULL buffer %d", i);
+   ubolt_solve_options o;
+   ubolt_solve_defaults(&o);
+   if (opts) o = *opts;
+   o.x_zero = 1;  // the device x buffers hold another solve's x
+   if ((rc = ubolt_solver_setup(ctx, &o))) return rc;
+   ubolt_solver *ws = ctx->solver;
+   if ((rc = EnsureHostBatch(ws))) return rc;
+   cudaStream_t s = (cudaStream_t)stream;
+   const size_t bytes = (size_t)ws->n * sizeof(double);
+   // Upload i + 1 while solve i runs; download i while solve i + 1 runs.
+   // Buffer i % 2 holds b and x of solve i.
+   cudaEventRecord(ws->entry, s);
+   cudaStreamWaitEvent(ws->up, ws->entry, 0);
+   cudaMemcpyAsync(ws->hb[0], b_host[0], bytes, cudaMemcpyHostToDevice, ws->up);
+   cudaEventRecord(ws->uploaded[0], ws->up);
+   for (int i = 0; i < n; i++) {
+      const int k = i & 1;
+      if (i + 1 < n) {
+         const int kn = (i + 1) & 1;
+         if (i >= 1) cudaStreamWaitEvent(ws->up, ws->solved[kn], 0);  // solve i - 1 has read it
+         cudaMemcpyAsync(ws->hb[kn], b_host[i + 1], bytes, cudaMemcpyHostToDevice, ws->up);
+         cudaEventRecord(ws->uploaded[kn], ws->up);
+      }
+      cudaStreamWaitEvent(s, ws->uploaded[k], 0);
+      if (i >= 2) cudaStreamWaitEvent(s, ws->downloaded[k], 0);  // x of solve i - 2 is out
+      rc = SolveSystem(ctx, false, ws->hb[k], ws->hx[k], &o, stats ? &stats[i] : nullptr, stream);
+      if (rc && rc != UBOLT_ERR_NOT_CONVERGED) break;
+      cudaEventRecord(ws->solved[k], s);
+      cudaStreamWaitEvent(ws->down, ws->solved[k], 0);
+      cudaMemcpyAsync(x_host[i], ws->hx[k], bytes, cudaMemcpyDeviceToHost, ws->down);
+      cudaEventRecord(ws->downloaded[k], ws->down);
+      if (rc) break;
+   }
+   // The caller's stream orders after every copy this call issued
+   cudaEventRecord(ws->entry, ws->up);
+   cudaStreamWaitEvent(s, ws->entry, 0);
+   cudaEventRecord(ws->entry, ws->down);
+   cudaStreamWaitEvent(s, ws->entry, 0);
+   const int rc_copy = CudaCheck(cudaGetLastError(), "solve_host_batch");
+   return rc ? rc : rc_copy;
 }
 
 extern "C" int ubolt_solve_adjoint(ubolt_ctx *ctx, const double *g, double *lambda, const ubolt_solve_options *opts,

@@ -224,6 +224,24 @@ class TransportSolver:
         check(lib.ubolt_solve(self.ctx.handle, _p(b), _p(x), C.byref(self.opts), C.byref(st), _stream(stream)))
         return x, {k: getattr(st, k) for k, _ in st._fields_ if k != "pad_"}
 
+    def solve_host_batch(self, bs, xs, stream=None):
+        """x_i = A^{-1} b_i for CPU tensors b_i (pinned memory for the copies
+        to overlap the solves), each solve from zero: the upload of the next
+        b and the download of the previous x run while a solve runs. xs are
+        filled once `stream` (default: the current one) is synchronised.
+        Returns the per-solve stats."""
+        n = len(bs)
+        if n != len(xs):
+            raise ValueError("solve_host_batch: as many x as b")
+        for t in list(bs) + list(xs):
+            if t.device.type != "cpu" or t.dtype != torch.float64 or not t.is_contiguous() or t.numel() != self.ctx.n_rows:
+                raise ValueError("solve_host_batch: contiguous float64 CPU tensors of n_rows entries")
+        bp = (C.c_void_p * n)(*[t.data_ptr() for t in bs])
+        xp = (C.c_void_p * n)(*[t.data_ptr() for t in xs])
+        st = (_lib.SolveStats * n)()
+        check(lib.ubolt_solve_host_batch(self.ctx.handle, n, bp, xp, C.byref(self.opts), st, _stream(stream)))
+        return [{k: getattr(s_, k) for k, _ in s_._fields_ if k != "pad_"} for s_ in st]
+
     def solve_adjoint(self, g, lam=None, stream=None, x_zero=True):
         """(L - S)^T lambda = g with the hand-written transpose operator."""
         lam = torch.zeros_like(g) if lam is None else lam
