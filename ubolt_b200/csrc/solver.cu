@@ -593,8 +593,10 @@ static int GmresIso(ubolt_ctx *ctx, const ubolt_solver *ws, S *work, const S *b,
    out->iterations = 0;
    out->converged = false;
    while (out->iterations < max_it) {
+      // The cycle's residual, read-only from here on: b itself from x = 0
+      const S *res = r0;
       if (x_zero) {
-         rc = DeviceCopy<S>(r0, b, n, s, "gmres");
+         res = b;
          x_zero = false;
       } else {
          rc = OperatorApply<S>(ctx, adjoint, x, r0, stream);
@@ -603,7 +605,7 @@ static int GmresIso(ubolt_ctx *ctx, const ubolt_solver *ws, S *work, const S *b,
       }
       if (rc) return rc;
       // r0 = E_u rho + r_perp; beta^2 = |r_perp|^2 + kappa |rho|^2
-      IsoSplitKernel<S><<<igrid, 256, 0, s>>>(r0, u, A, nn, 1.0 / kappa, ws->rho, ws->partial);
+      IsoSplitKernel<S><<<igrid, 256, 0, s>>>(res, u, A, nn, 1.0 / kappa, ws->rho, ws->partial);
       ReducePartialKernel<<<1, 256, 0, s>>>(ws->partial, igrid, 1, scal);
       CountLaunch(2);
       MultiDot<double>(ws, ws->rho, 1, ws->rho, nn, scal + 1, s);
@@ -616,7 +618,7 @@ static int GmresIso(ubolt_ctx *ctx, const ubolt_solver *ws, S *work, const S *b,
       double rp2 = sc[0];
       const bool iso_r0 = rp2 <= 1e-28 * (rp2 + kappa * sc[1]);
       if (iso_r0) rp2 = 0.0;
-      const S *r0_in = iso_r0 ? nullptr : r0;
+      const S *r0_in = iso_r0 ? nullptr : res;
       const double beta = std::sqrt(rp2 + kappa * sc[1]);
       if (!std::isfinite(beta)) return SetError(UBOLT_ERR_NONFINITE, "GMRES residual is not finite");
       out->estimate = bnorm > 0 ? beta / bnorm : 0.0;
