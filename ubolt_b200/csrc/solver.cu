@@ -175,9 +175,9 @@ template <typename S>
 static void MultiDot(const ubolt_solver *ws, const S *V, int nv, const S *w, int64_t n, double *h, cudaStream_t s)
 {
    const int stride = ws->restart + 2;
-   // At least 16 elements per thread: short (node-space) vectors take few
-   // blocks, and the partials to reduce stay few
-   const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(ws->red_blocks, n / (16 * kRedThreads)));
+   // Four elements per thread: a short (node-space) vector still spreads
+   // over a few hundred blocks, and the partials to reduce stay few
+   const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(ws->red_blocks, n / (4 * kRedThreads)));
    for (int i0 = 0; i0 < nv; i0 += kChunk)
       MultiDotKernel<S><<<blocks, kRedThreads, 0, s>>>(V, n, i0, std::min(kChunk, nv - i0), w, ws->partial, stride);
    ReducePartialKernel<<<nv, 256, 0, s>>>(ws->partial, blocks, stride, h);
