@@ -216,6 +216,25 @@ static void ToHost(const ubolt_solver *ws, const double *dev, int off, int n, cu
    CountLaunch();
 }
 
+// Up to three runs of device values to the mailbox in one launch
+struct MailRuns {
+   const double *src[3];
+   int off[3], n[3];
+};
+
+__global__ void MailGatherKernel(MailRuns r, double *__restrict__ box)
+{
+#pragma unroll
+   for (int k = 0; k < 3; k++)
+      for (int i = threadIdx.x; i < r.n[k]; i += blockDim.x) box[r.off[k] + i] = r.src[k][i];
+}
+
+static void ToHost3(const ubolt_solver *ws, const MailRuns &r, cudaStream_t s)
+{
+   MailGatherKernel<<<1, 64, 0, s>>>(r, ws->mb_d);
+   CountLaunch();
+}
+
 // n host values to the device through the mailbox at off (the previous
 // value at that offset has been consumed: the solver syncs in between)
 static void ToDevice(const ubolt_solver *ws, const double *host, double *dev, int off, int n, cudaStream_t s)
@@ -353,8 +372,7 @@ static int Gmres(ubolt_ctx *ctx, const ubolt_solver *ws, S *V, S *Zb, S *z, S *t
          MultiAxpyKernel<S><<<grid, 256, 0, s>>>(V, n, j + 1, dh2, -1.0, vn, 1);
          CountLaunch();
          MultiDot<S>(ws, vn, 1, vn, n, dh2 + j + 1, s);
-         ToHost(ws, dh1, kMbH1, j + 1, s);
-         ToHost(ws, dh2, kMbH1 + (m + 2), j + 2, s);
+         ToHost3(ws, MailRuns{{dh1, dh2, dh2}, {kMbH1, kMbH1 + (m + 2), 0}, {j + 1, j + 2, 0}}, s);
          if ((rc = CudaCheck(cudaStreamSynchronize(s), "gmres"))) return rc;
          std::copy(ws->mb_h + kMbH1, ws->mb_h + kMbH1 + j + 1, h1.begin());
          std::copy(ws->mb_h + kMbH1 + (m + 2), ws->mb_h + kMbH1 + (m + 2) + j + 2, h2.begin());
@@ -532,12 +550,15 @@ __global__ void __launch_bounds__(256) IsoScatterKernel(const S *__restrict__ z,
    }
 }
 
-// h[i] = alpha[i] alpha[j1] |r_perp|^2 + kappa d[i] for i < j1 (in place over
-// d), then alpha[j1] -= sum_i h[i] alpha[i]: one Gram-Schmidt pass's scalars
-__global__ void IsoCombineKernel(double *__restrict__ d, double *__restrict__ alpha, int j1, double rp2, double kappa)
+// h[i] = alpha[i] alpha_w |r_perp|^2 + kappa d[i] for i < j1 (in place over
+// d), then alpha[j1] = alpha_w - sum_i h[i] alpha[i]: one Gram-Schmidt
+// pass's scalars. alpha_w is alpha[j1], or on the first pass alpha[j1 - 1]
+// (the new vector w = v_j - ... starts with v_j's scalar)
+__global__ void IsoCombineKernel(double *__restrict__ d, double *__restrict__ alpha, int j1, double rp2, double kappa,
+                                 int first)
 {
    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-   const double aw = alpha[j1];
+   const double aw = first ? alpha[j1 - 1] : alpha[j1];
    double upd = 0.0;
    for (int i = 0; i < j1; i++) {
       const double h = alpha[i] * aw * rp2 + kappa * d[i];
@@ -642,20 +663,16 @@ static int GmresIso(ubolt_ctx *ctx, const ubolt_solver *ws, S *work, const S *b,
             return rc;
          IsoScatterKernel<S><<<igrid, 256, 0, s>>>(z, wgt, sig_s, 1.0 / ctx->sum_weights, ctx->nb, A, nn, pj, pn);
          CountLaunch();
-         MailCopyKernel<<<1, 32, 0, s>>>(alpha + j, alpha + j + 1, 1);
-         CountLaunch();
          // Classical Gram-Schmidt, twice, in the compressed inner product
          for (int pass = 0; pass < 2; pass++) {
             double *dh = pass ? dh2 : dh1;
             MultiDot<double>(ws, Phi, j + 1, pn, nn, dh, s);
-            IsoCombineKernel<<<1, 32, 0, s>>>(dh, alpha, j + 1, rp2, kappa);
+            IsoCombineKernel<<<1, 32, 0, s>>>(dh, alpha, j + 1, rp2, kappa, pass == 0);
             MultiAxpyKernel<double><<<igrid, 256, 0, s>>>(Phi, nn, j + 1, dh, -1.0, pn, 1);
             CountLaunch(2);
          }
          MultiDot<double>(ws, pn, 1, pn, nn, dh2 + j + 1, s);
-         ToHost(ws, dh1, kMbH1, j + 1, s);
-         ToHost(ws, dh2, kMbH1 + (m + 2), j + 2, s);
-         ToHost(ws, alpha + j + 1, kMbScalars, 1, s);
+         ToHost3(ws, MailRuns{{dh1, dh2, alpha + j + 1}, {kMbH1, kMbH1 + (m + 2), kMbScalars}, {j + 1, j + 2, 1}}, s);
          if ((rc = CudaCheck(cudaStreamSynchronize(s), "gmres"))) return rc;
          std::copy(ws->mb_h + kMbH1, ws->mb_h + kMbH1 + j + 1, h1.begin());
          std::copy(ws->mb_h + kMbH1 + (m + 2), ws->mb_h + kMbH1 + (m + 2) + j + 2, h2.begin());
