@@ -103,14 +103,22 @@ __device__ __forceinline__ void LoadShared(const T *p, T v[N])
    }
 }
 
+// Upwind runs staged per thread: every face at once where F * NB <= 12,
+// else a ring of two faces fetched ahead of the walk over the faces (DG1
+// tets and hexes, whose F * NB runs would crowd the SM's shared memory)
+template <int NB, int F>
+constexpr int UpSlots() { return F * NB > 12 ? 2 : F; }
+
 // Shared memory of one apply block, in elements of T: the cells' class
-// records [K][L.size], each thread's upwind runs [threads][F][NB][AP], the
+// records [K][L.size], the threads' upwind runs [slots][NB][threads][AP]
+// (thread-fastest, so a warp's 16-byte reads hit distinct banks), the
 // cells' own rows [K][NB][A], then for the scatter the node moments
 // [K][NB], sigma_s / W per cell [K] and the ordinate weights [A]
 template <typename T, int NB, int F, int AP>
 __host__ __device__ constexpr size_t ApplySmemElems(int K, int threads, int A)
 {
-   return (size_t)K * RecordLayout(NB, F, (int)sizeof(T)).size + (size_t)threads * F * NB * AP + (size_t)K * NB * A +
+   return (size_t)K * RecordLayout(NB, F, (int)sizeof(T)).size + (size_t)threads * UpSlots<NB, F>() * NB * AP +
+          (size_t)K * NB * A +
           (size_t)K * NB + (size_t)K + (size_t)A;
 }
 
@@ -125,11 +133,13 @@ __global__ void __launch_bounds__(256, ApplyMinBlocks<T, NB, AP>()) ApplyKernel(
    constexpr RecordLayout L(NB, F, (int)sizeof(T));
    constexpr int CU = AP * (int)sizeof(T);  // bytes of one thread's run of a row
    constexpr int RU = L.size * (int)sizeof(T) / 16;
+   constexpr int XS = UpSlots<NB, F>();
+   constexpr bool kRing = XS < F;
    extern __shared__ __align__(16) unsigned char smem_raw[];
    const int A = g.A, QA = A / AP;
    T *recs = reinterpret_cast<T *>(smem_raw);
    T *xup = recs + K * L.size;
-   T *xs = xup + (size_t)blockDim.x * F * NB * AP;
+   T *xs = xup + (size_t)blockDim.x * XS * NB * AP;
    T *mom = xs + K * NB * A;  // scatter: [K][NB] sigma_s / W sum_b w_b x(node, b)
    T *ssw = mom + K * NB;     // scatter: [K] sigma_s / W
    T *ws = ssw + K;           // scatter: [A] the weights
@@ -143,8 +153,9 @@ __global__ void __launch_bounds__(256, ApplyMinBlocks<T, NB, AP>()) ApplyKernel(
    const bool live = k < kc;
 
    // Stage: the block's own rows (one contiguous range), each cell's class
-   // record and this thread's upwind runs, all in flight at once. Per face
-   // 4 bits of fcode: 8 for an interior face, else the boundary side.
+   // record and this thread's upwind runs, all in flight at once (with the
+   // ring, the first two faces' runs, each in a commit group of its own).
+   // Per face 4 bits of fcode: 8 for an interior face, else the boundary side.
    unsigned fcode = 0;
    {
       const int nu = kc * NB * A * (int)sizeof(T) / CU;
@@ -154,17 +165,21 @@ __global__ void __launch_bounds__(256, ApplyMinBlocks<T, NB, AP>()) ApplyKernel(
    if (live) {
       const T *rec = g.rec + (int64_t)g.cls[c] * L.size;
       for (int u = q; u < RU; u += QA) CpAsync<16>(recs + k * L.size + u * (16 / (int)sizeof(T)), rec + u * (16 / (int)sizeof(T)));
+      if constexpr (kRing) CpAsyncCommit();
 #pragma unroll
       for (int f = 0; f < F; f++) {
          const int32_t cf = g.code[c * F + f];
          if (FaceInterior(cf)) {
             fcode |= 8u << (4 * f);
+            if (!kRing || f < XS) {
 #pragma unroll
-            for (int j = 0; j < NB; j++)
-               CpAsync<CU>(xup + ((t * F + f) * NB + j) * AP, x + ((int64_t)cf * NB + j) * A + a0);
+               for (int j = 0; j < NB; j++)
+                  CpAsync<CU>(xup + ((f * NB + j) * (int)blockDim.x + t) * AP, x + ((int64_t)cf * NB + j) * A + a0);
+            }
          } else {
             fcode |= (unsigned)FaceSide(cf) << (4 * f);
          }
+         if (kRing && f < XS) CpAsyncCommit();
       }
    }
    T om[3 * AP];
@@ -176,7 +191,11 @@ __global__ void __launch_bounds__(256, ApplyMinBlocks<T, NB, AP>()) ApplyKernel(
    }
    if constexpr (SCATTER)
       for (int b = t; b < A; b += blockDim.x) ws[b] = g.w[b];
-   CpAsyncWaitAll();
+   // The shared rows and records are in; with the ring, a live thread's two
+   // face groups may still be in flight (a thread without a cell committed
+   // no group, so it waits for all of its copies)
+   if (kRing && live) CpAsyncWaitGroup<XS>();
+   else CpAsyncWaitAll();
    __syncthreads();
 
    if constexpr (SCATTER) {
@@ -236,11 +255,17 @@ __global__ void __launch_bounds__(256, ApplyMinBlocks<T, NB, AP>()) ApplyKernel(
          T na[4];
          LoadShared<T, 4>(r + L.nA(f), na);
          T xn[AP][NB];
+         const int slot = kRing ? (f & 1) : f;
+         if constexpr (kRing) {
+            // This face's group is in once at most the next face's is pending
+            if (f + 1 < F) CpAsyncWaitGroup<1>();
+            else CpAsyncWaitGroup<0>();
+         }
          if (fc & 8u) {
 #pragma unroll
             for (int j = 0; j < NB; j++) {
                T v[AP];
-               LoadShared<T, AP>(xup + ((t * F + f) * NB + j) * AP, v);
+               LoadShared<T, AP>(xup + ((slot * NB + j) * (int)blockDim.x + t) * AP, v);
 #pragma unroll
                for (int p = 0; p < AP; p++) xn[p][j] = v[p];
             }
@@ -291,6 +316,18 @@ __global__ void __launch_bounds__(256, ApplyMinBlocks<T, NB, AP>()) ApplyKernel(
                      acc[p][i] += sm[p] * v;
                   }
             }
+         }
+         if constexpr (kRing) {
+            // This face's runs are used: fetch face f + 2's into the slot
+            if (f + XS < F) {
+               const int32_t cf = g.code[c * F + f + XS];
+               if (FaceInterior(cf)) {
+#pragma unroll
+                  for (int j = 0; j < NB; j++)
+                     CpAsync<CU>(xup + ((slot * NB + j) * (int)blockDim.x + t) * AP, x + ((int64_t)cf * NB + j) * A + a0);
+               }
+            }
+            CpAsyncCommit();
          }
       }
    }
