@@ -154,14 +154,26 @@ struct SweepDev {
 // walk reads it with 16-byte loads
 __host__ __device__ constexpr int GStride(int NB, int elem) { return (NB * NB * elem + 15) / 16 * 16 / elem; }
 
+// A position's S couplings in shared memory. A run of a multiple of four
+// 16-byte units (the 4 x 4 blocks of 3D DG1) is padded by one unit: a
+// quarter-warp's 16-byte reads of one slot at consecutive positions would
+// otherwise fall on the same banks, 8-way. Shorter conflicts are left alone:
+// the padding's shared memory costs L1 (the shapes on triangles and quads
+// run slower with it).
+__host__ __device__ constexpr int PosStride(int S, int NB, int elem)
+{
+   return (S * GStride(NB, elem) * elem / 16 % 4 == 0 ? S * GStride(NB, elem) * elem + 16
+                                                       : S * GStride(NB, elem) * elem) / elem;
+}
+
 struct SweepSlice {
    size_t loc, G, bytes;
    __host__ __device__ SweepSlice(int P, int S, int NB, int elem)
    {
       auto up = [](size_t v) { return (v + 15) & ~(size_t)15; };
       loc = 0;                                           // T [P][NB], by local cell
-      G = up(loc + (size_t)P * NB * elem);               // T [P][S][GStride], by position
-      bytes = up(G + (size_t)P * S * GStride(NB, elem) * elem);
+      G = up(loc + (size_t)P * NB * elem);               // T [P][PosStride], by position
+      bytes = up(G + (size_t)P * PosStride(S, NB, elem) * elem);
    }
 };
 
@@ -337,6 +349,7 @@ __global__ void __launch_bounds__(128, SweepMinBlocks<T, NB, PL>()) SweepKernel(
    const T *never = reinterpret_cast<const T *>(s.ctrl + kCtrlNever);
    const size_t R = (size_t)NB * NB * (1 + S);
    constexpr int GS = GStride(NB, (int)sizeof(T));
+   const int PS = PosStride(S, NB, (int)sizeof(T));
    // The task's five scalars, one lane each, in one round trip
    auto scalars = [&](int64_t tt) -> int64_t {
       if (tt >= s.n_tasks) return 0;
@@ -402,7 +415,7 @@ __global__ void __launch_bounds__(128, SweepMinBlocks<T, NB, PL>()) SweepKernel(
 #pragma unroll
                for (int e = 0; e < SM * NB * NB; e++)
                   if (e < S * NB * NB)
-                     CpAsync<sizeof(T)>(G + ((size_t)i * S + e / (NB * NB)) * GS + e % (NB * NB),
+                     CpAsync<sizeof(T)>(G + (size_t)i * PS + (e / (NB * NB)) * GS + e % (NB * NB),
                                         ft + (size_t)(NB * NB + e) * ncell);
             }
          }
@@ -449,7 +462,7 @@ __global__ void __launch_bounds__(128, SweepMinBlocks<T, NB, PL>()) SweepKernel(
                for (int j = 0; j < NB; j++) Wk[ii][j] = ft[(size_t)(ii * NB + j) * ncell];
          } else {
             const T om[3] = {g.omega[3 * a], g.omega[3 * a + 1], g.omega[3 * a + 2]};
-            CellFactors<T, NB, F>(g, c, om, s.tmask[off + i], Wk, G + (size_t)i * S * GS, (size_t)GS, 1);
+            CellFactors<T, NB, F>(g, c, om, s.tmask[off + i], Wk, G + (size_t)i * PS, (size_t)GS, 1);
          }
          T y[NB];
 #pragma unroll
@@ -477,7 +490,7 @@ __global__ void __launch_bounds__(128, SweepMinBlocks<T, NB, PL>()) SweepKernel(
 #pragma unroll
                for (int sl = 0; sl < SM; sl++) {
                   if (my_up[k][sl] < 0) continue;
-                  SubCoupling<T, NB>(G + ((size_t)i * S + sl) * GS, xp[k][sl], y);
+                  SubCoupling<T, NB>(G + (size_t)i * PS + sl * GS, xp[k][sl], y);
                   my_up[k][sl] = -1;
                }
             }
@@ -512,7 +525,7 @@ __global__ void __launch_bounds__(128, SweepMinBlocks<T, NB, PL>()) SweepKernel(
                }
                T xn[NB];
                PollUpwind<T, NB>(src, stride, s, xn);
-               SubCoupling<T, NB>(G + ((size_t)i * S + sl) * GS, xn, y);
+               SubCoupling<T, NB>(G + (size_t)i * PS + sl * GS, xn, y);
             }
 #pragma unroll
             for (int sl = 0; sl < SM; sl++) {
@@ -520,7 +533,7 @@ __global__ void __launch_bounds__(128, SweepMinBlocks<T, NB, PL>()) SweepKernel(
                T xn[NB];
 #pragma unroll
                for (int j = 0; j < NB; j++) xn[j] = loc[my_ul[k][sl] * NB + j];
-               SubCoupling<T, NB>(G + ((size_t)i * S + sl) * GS, xn, y);
+               SubCoupling<T, NB>(G + (size_t)i * PS + sl * GS, xn, y);
             }
             const int64_t c = base + local;
 #pragma unroll
