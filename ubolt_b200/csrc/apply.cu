@@ -475,7 +475,8 @@ __global__ void DiagonalKernel(const DevGeom<T> g, T *__restrict__ d)
 
 // Cells per block for QA threads per cell: the most live threads resident
 // per SM for this kernel (registers and shared memory), then the fewest idle
-// lanes, then the block nearest 256 threads. Cached per kernel and QA.
+// lanes, then the most blocks per SM (more blocks stage their copies
+// independently). Cached per kernel and QA.
 template <typename Kern, typename Smem>
 static int ApplyCells(Kern kern, int QA, Smem smem_of)
 {
@@ -490,9 +491,9 @@ static int ApplyCells(Kern kern, int QA, Smem smem_of)
    int dev = 0, smem_max = 48 * 1024;
    cudaGetDevice(&dev);
    cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-   int best = 1;
+   int best = 1, best_blocks = 0;
    long best_live = -1;
-   double best_idle = 2.0, best_dist = 1e9;
+   double best_idle = 2.0;
    for (int K = 1; K * QA <= 256; K++) {
       const int thr = (K * QA + 31) / 32 * 32;
       const size_t smem = smem_of(K, thr);
@@ -509,13 +510,12 @@ static int ApplyCells(Kern kern, int QA, Smem smem_of)
       }
       const long live = (long)per_sm * K * QA;
       const double idle = (double)(thr - K * QA) / thr;
-      const double dist = std::abs(thr - 256);
       if (live > best_live || (live == best_live && (idle < best_idle - 1e-9 ||
-                                                     (idle < best_idle + 1e-9 && dist < best_dist)))) {
+                                                     (idle < best_idle + 1e-9 && per_sm > best_blocks)))) {
          best = K;
          best_live = live;
          best_idle = idle;
-         best_dist = dist;
+         best_blocks = per_sm;
       }
    }
    std::lock_guard<std::mutex> lk(mu);
