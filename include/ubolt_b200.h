@@ -415,8 +415,9 @@ int ubolt_solve(ubolt_ctx *ctx, const double *b, double *x, const ubolt_solve_op
  * already on `stream`; on return `stream` waits for the last download, so
  * x_host is complete once `stream` is synchronised. stats (n entries, may be
  * NULL) per solve; every solve starts from zero. Stops at the first solve
- * that fails, returning its status.
- * The batched form of TransportSolver::solve over a PETSc host Vec. */
+ * that fails, returning its status. The batched form of
+ * TransportSolver::solve (src/transport_solverk.kokkos.cxx:334-343) for
+ * right-hand sides in host Vecs. */
 int ubolt_solve_host_batch(ubolt_ctx *ctx, int n, const double *const *b_host, double *const *x_host,
                            const ubolt_solve_options *opts, ubolt_solve_stats *stats, void *stream);
 
