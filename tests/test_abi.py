@@ -52,3 +52,19 @@ def test_geometry_view_roundtrip(order):
     g = P.build_geometry(m, order)
     assert g.n_cells == 6 and g.faces_per_cell == 4
     assert ("face_own" in g.arrays) == (order == 1)
+
+
+def test_option_defaults_and_struct_sizes():
+    """The ctypes mirrors of the option structs match the header's defaults,
+    and the new entry points reject a NULL context."""
+    o = _lib.DsaOptions()
+    lib.ubolt_dsa_defaults(C.byref(o))
+    assert (o.penalty, o.consistent_power, o.consistent_d, o.inner_iterations) == (4.0, 1.5, 1, 30)
+    assert (o.void_sigma_t, o.void_d, o.void_bridge) == (0.0, 0.0, 1)
+    assert C.sizeof(_lib.DsaOptions) == 48
+    s = _lib.SolveOptions()
+    lib.ubolt_solve_defaults(C.byref(s))
+    assert (s.rtol, s.max_it, s.restart, s.x_zero) == (1e-8, 500, 30, 1)
+    n, br, ch = C.c_int64(0), C.c_int32(0), C.c_double(0.0)
+    assert lib.ubolt_dsa_void_info(None, C.byref(n), C.byref(br), C.byref(ch)) == 1
+    assert lib.ubolt_solve_host_batch(None, 0, None, None, None, None, None) == 1

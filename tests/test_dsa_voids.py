@@ -265,3 +265,14 @@ def test_gpu_solve_through_a_void_with_dsa():
         assert s1["converged"]
         assert (x1 - x0).abs().max().item() <= 1e-7 * x0.abs().max().item()
     ctx.close()
+
+
+def test_all_void_is_masked_not_bridged():
+    """Every cell void: nothing to bridge to, so the voids are masked and the
+    operator is V times the identity."""
+    g, q = _box(2, 1, [4, 3], 0.25)
+    z = np.zeros(g.n_cells)
+    pol = O.VoidPolicy(g, z, z)
+    assert pol.n_void == g.n_cells and not pol.bridged and pol.masked.all() and not pol.singular
+    D = O.dsa_matrix(g, q, z, z, policy=pol).toarray()
+    assert np.array_equal(D, np.diag(np.repeat(g.volume, g.n_basis)))
