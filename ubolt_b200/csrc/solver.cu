@@ -49,6 +49,7 @@ struct ubolt_solver {
    // Reductions: partial[red_blocks][restart + 2], h[3 * (restart + 2)]
    double *partial = nullptr, *h = nullptr;
    int red_blocks = 0;
+   unsigned *md_count = nullptr;  // the multi-dot's finished-block counter, zero between launches
    // The compressed form (sweep preconditioner, exact sweep): node-space
    // basis (restart + 1) x n_nodes, the residual's isotropic part, the basis
    // scalars alpha[restart + 2] and four reduction slots
@@ -74,11 +75,15 @@ namespace ubolt {
 constexpr int kRedThreads = 256;
 constexpr int kChunk = 8;
 
-// partial[blk][i0 + i] = this block's share of V_{i0+i} . w
+// h[i0 + i] = V_{i0+i} . w for i < nc: each block's share to
+// partial[blk][i0 + i], then the last block to finish (an integer counter,
+// reset by that block) adds the shares in block order, one warp per value.
+// No block waits on another.
 template <typename S>
 __global__ void __launch_bounds__(kRedThreads) MultiDotKernel(const S *__restrict__ V, int64_t n, int i0, int nc,
                                                               const S *__restrict__ w, double *__restrict__ partial,
-                                                              int stride)
+                                                              int stride, double *__restrict__ h,
+                                                              unsigned *__restrict__ count)
 {
    double acc[kChunk];
 #pragma unroll
@@ -103,7 +108,22 @@ __global__ void __launch_bounds__(kRedThreads) MultiDotKernel(const S *__restric
       double s = 0.0;
       for (int k = 0; k < kRedThreads / 32; k++) s += red[threadIdx.x][k];
       partial[(int64_t)blockIdx.x * stride + i0 + threadIdx.x] = s;
+      __threadfence();
    }
+   __shared__ bool last;
+   __syncthreads();
+   if (threadIdx.x == 0) last = atomicAdd(count, 1u) == gridDim.x - 1;
+   __syncthreads();
+   if (!last) return;
+   __threadfence();
+   if (warp < nc) {
+      double s = 0.0;
+      for (int b = lane; b < (int)gridDim.x; b += 32) s += __ldcg(&partial[(int64_t)b * stride + i0 + warp]);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      if (lane == 0) h[i0 + warp] = s;
+   }
+   if (threadIdx.x == 0) *count = 0;
 }
 
 // out[i] = sum over blocks of partial[blk][i]
@@ -179,9 +199,9 @@ static void MultiDot(const ubolt_solver *ws, const S *V, int nv, const S *w, int
    // over a few hundred blocks, and the partials to reduce stay few
    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(ws->red_blocks, n / (4 * kRedThreads)));
    for (int i0 = 0; i0 < nv; i0 += kChunk)
-      MultiDotKernel<S><<<blocks, kRedThreads, 0, s>>>(V, n, i0, std::min(kChunk, nv - i0), w, ws->partial, stride);
-   ReducePartialKernel<<<nv, 256, 0, s>>>(ws->partial, blocks, stride, h);
-   CountLaunch((nv + kChunk - 1) / kChunk + 1);
+      MultiDotKernel<S><<<blocks, kRedThreads, 0, s>>>(V, n, i0, std::min(kChunk, nv - i0), w, ws->partial, stride,
+                                                       h, ws->md_count);
+   CountLaunch((nv + kChunk - 1) / kChunk);
 }
 
 // y = x on the SMs: a device-to-device cudaMemcpy may go to a copy engine,
@@ -730,7 +750,7 @@ static void FreeWorkspace(ubolt_ctx *ctx)
                    (void *)ws->b32, (void *)ws->t32, (void *)ws->d32, (void *)ws->Z, (void *)ws->Z32,
                    (void *)ws->partial, (void *)ws->h, (void *)ws->Phi, (void *)ws->rho,
                    (void *)ws->alpha, (void *)ws->scal, (void *)ws->hb[0], (void *)ws->hb[1], (void *)ws->hx[0],
-                   (void *)ws->hx[1]})
+                   (void *)ws->hx[1], (void *)ws->md_count})
       if (p) cudaFree(p);
    if (ws->mb_h) cudaFreeHost(ws->mb_h);
    for (cudaStream_t st : {ws->up, ws->down})
@@ -774,6 +794,8 @@ static int EnsureWorkspace(ubolt_ctx *ctx, const ubolt_solve_options *o)
        (rc = alloc((void **)&ws->t, n * 8)) || (rc = alloc((void **)&ws->partial, (size_t)ws->red_blocks * (m + 2) * 8)) ||
        (rc = alloc((void **)&ws->h, 3 * (size_t)(m + 2) * 8)))
       return rc;
+   if ((rc = alloc((void **)&ws->md_count, 16))) return rc;
+   if ((rc = CudaCheck(cudaMemset(ws->md_count, 0, 16), "solver workspace"))) return rc;
    ws->mb_half = 16 + 3 * (m + 2);
    if (cudaHostAlloc((void **)&ws->mb_h, 2 * (size_t)ws->mb_half * 8, cudaHostAllocMapped) != cudaSuccess ||
        cudaHostGetDevicePointer((void **)&ws->mb_d, ws->mb_h, 0) != cudaSuccess) {
