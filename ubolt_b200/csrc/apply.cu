@@ -122,8 +122,9 @@ __host__ __device__ constexpr size_t ApplySmemElems(int K, int threads, int A)
           (size_t)K * NB + (size_t)K + (size_t)A;
 }
 
-// Three 256-thread blocks per SM (at most 80 registers); two where the four
-// basis functions' rows of AP > 1 ordinates need more
+// The register cap, as 256-thread blocks per SM: three (at most 80
+// registers, so 768 threads fit whatever block size the launch picks), two
+// where the four basis functions' rows of AP > 1 ordinates need more
 template <typename T, int NB, int AP>
 constexpr int ApplyMinBlocks() { return (NB == 4 && AP > 1) ? 2 : 3; }
 
