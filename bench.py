@@ -27,6 +27,10 @@ import sys
 import threading
 import time
 
+# The CPU legs run OpenMP on every host core, threads kept close to their
+# parent; set before any OpenMP runtime starts in this process
+os.environ.setdefault("OMP_PROC_BIND", "close")
+
 import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -145,15 +149,29 @@ def _dist():
     return world, rank, local
 
 
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def run_reference(args):
-    """The CPU restatement of the reference path on every host core."""
+    """The CPU restatement of the reference path on every host core. The
+    workload's mesh and seeded data come from the library's pure-NumPy
+    builders, its geometry and ordinates from the oracle: the library itself
+    is never loaded here."""
     world, rank, _ = _dist()
     if rank != 0:
         return
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     from ubolt_b200 import problem as P
-    prob = P.config_tri256(scale=args.scale)
+    prob = P.config_tri256(scale=args.scale, geometry=O.geometry_from_mesh, quadrature=O.lqn)
     g, q = prob.geometry, prob.quad
     op = O.Operator(g, q, prob.sigma_t[0], prob.sigma_s[0, 0])
     b = O.rhs(g, q, prob.source[0])
@@ -173,6 +191,7 @@ def run_reference(args):
             "config": {"workload": WORKLOAD, "rtol": 1e-8, "rows": int(op.n), "iterations": int(np.median(its)),
                        "parallelism": f"replicas{args.gpus}"},
             "cpu_baseline": {"value": v, "unit": "s/solve", "cores": cores, "kind": "port",
+                             "cpu_model": cpu_model(), "omp_proc_bind": os.environ.get("OMP_PROC_BIND"),
                              "sample": "the full workload: one FP64 GMRES solve to 1e-8 with an upwind-sweep "
                                        "preconditioner per step, OpenMP on every host core"},
             "e2e": {"value": v, "unit": "s/solve", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -193,9 +212,10 @@ def cpu_baseline(args):
     for _ in range(n):
         x, it, res = op.solve(b, rtol=1e-8)
     v = (time.perf_counter() - t0) / n
-    return {"value": v, "unit": "s/solve", "cores": O.threads(), "kind": "port",
+    return {"value": v, "unit": "s/solve", "cores": O.threads(), "kind": "port", "cpu_model": cpu_model(),
+            "omp_proc_bind": os.environ.get("OMP_PROC_BIND"),
             "sample": f"the full workload, {n} FP64 solves to 1e-8 ({it} iterations each), GMRES + CPU upwind "
-                      "sweep, OpenMP"}, x
+                      "sweep, OpenMP, on the oracle's own geometry and ordinates"}, x
 
 
 def profile_kernel(args, ctx, T, stream):

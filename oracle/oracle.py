@@ -2,18 +2,26 @@
 
 Loads oracle/_build/liboracle.so (built by `make -C oracle`), the plain-C
 restatement of UBOLT's assembled operator in oracle/ubolt_oracle.c, and
-returns SciPy CSR matrices and NumPy vectors. Only tests/, the smoke check
-and bench.py's CPU baseline use this module; the library never does.
+returns SciPy CSR matrices and NumPy vectors. It computes with its own
+geometry (oracle/geometry.py) and the reference's own ordinate tables
+(oracle/quadrature.py), never with the library's: handed a geometry or an
+ordinate set the library built, it builds its own from the same mesh and
+order. Only tests/, the smoke check and bench.py's CPU baseline use this
+module; the library never does.
 """
 import ctypes as C
 import os
 import subprocess
+import sys
 
 import numpy as np
 import scipy.sparse as sp
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "_build", "liboracle.so")
+sys.path.insert(0, HERE)
+import geometry as _geometry  # noqa: E402  (the oracle's own geometry)
+import quadrature as _quadrature  # noqa: E402  (the reference's ordinate sets)
 
 
 def build():
@@ -59,6 +67,41 @@ _sig("oracle_threads", C.c_int)
 PC_NONE, PC_BLOCK, PC_SWEEP = 0, 1, 2
 
 
+def geometry_from_mesh(mesh, order, side_bc=None):
+    """The oracle's own geometry of a mesh (oracle/geometry.py)."""
+    return _geometry.build(mesh.dim, mesh.cell_type, mesh.vertices, mesh.cells, order, side_bc)
+
+
+def lqn(dim, sn):
+    """The reference's level-symmetric set, from its own generator's tables."""
+    return _quadrature.lqn(dim, sn)
+
+
+def own_geometry(g):
+    """The oracle never computes with the library's geometry: a geometry the
+    library built carries the mesh it came from, and the oracle builds its
+    own from that (once per object). An oracle geometry passes through."""
+    if not hasattr(g, "arrays"):
+        return g
+    cached = g.__dict__.get("_oracle_geometry")
+    if cached is None:
+        mesh, order, side_bc = g.__dict__["source"]
+        cached = geometry_from_mesh(mesh, order, side_bc)
+        g.__dict__["_oracle_geometry"] = cached
+    return cached
+
+
+def own_quadrature(q):
+    """Likewise the ordinates: the reference's set of the same order."""
+    if not hasattr(q, "struct"):
+        return q
+    cached = q.__dict__.get("_oracle_quadrature")
+    if cached is None:
+        cached = lqn(q.dim, q.sn)
+        q.__dict__["_oracle_quadrature"] = cached
+    return cached
+
+
 def _ptr(a):
     return None if a is None else a.ctypes.data_as(C.c_void_p)
 
@@ -68,7 +111,8 @@ class Operator:
     scatter: the reference's TransportOperator shell, on the CPU."""
 
     def __init__(self, geometry, quad, sigma_t, sigma_s):
-        g = geometry
+        g = own_geometry(geometry)
+        quad = own_quadrature(quad)
         self.nb, self.F, self.nc, self.A = g.n_basis, g.faces_per_cell, g.n_cells, quad.n_angles
         self.n = self.nc * self.nb * self.A
         self.quad = quad
@@ -138,6 +182,7 @@ class Operator:
 
 
 def angular_integral(psi, n_nodes, quad):
+    quad = own_quadrature(quad)
     phi = np.empty(n_nodes)
     _lib.oracle_angular_integral(n_nodes, quad.n_angles, quad.w, np.ascontiguousarray(psi, dtype=np.float64), phi)
     return phi
@@ -145,7 +190,8 @@ def angular_integral(psi, n_nodes, quad):
 
 def rhs(geometry, quad, source_cell, side_inflow=None):
     """b = ghost inflow + isotropic source, added onto zero as the driver does."""
-    g = geometry
+    g = own_geometry(geometry)
+    quad = own_quadrature(quad)
     n = g.n_cells * g.n_basis * quad.n_angles
     b = np.zeros(n)
     if side_inflow is not None and np.any(np.asarray(side_inflow) != 0.0):
@@ -161,6 +207,7 @@ def rhs(geometry, quad, source_cell, side_inflow=None):
 
 
 def add_transfer(b, phi, sigma_s, n_cells, nb, quad):
+    quad = own_quadrature(quad)
     _lib.oracle_add_transfer(n_cells, nb, quad.n_angles, quad.sum_weights, np.ascontiguousarray(phi),
                              np.ascontiguousarray(sigma_s, dtype=np.float64), b)
     return b
@@ -168,6 +215,7 @@ def add_transfer(b, phi, sigma_s, n_cells, nb, quad):
 
 def fd2d(nx, ny, quad, sigma_t, side_bc=(0, 0, 0, 0), lx=1.0, ly=1.0):
     """Streaming + removal of the structured 2D FD backend (ghost-flux rows)."""
+    quad = own_quadrature(quad)
     A = quad.n_angles
     n = nx * ny * A
     row_ptr = np.zeros(n + 1, dtype=np.int64)
@@ -202,7 +250,7 @@ class VoidPolicy:
     the diffusion operator would be singular."""
 
     def __init__(self, geometry, sigma_t, sigma_s, void_sigma_t=0.0, bridge=True, void_d=0.0):
-        g = geometry
+        g = own_geometry(geometry)
         nc = g.n_cells
         self.is_void = np.zeros(nc, dtype=np.uint8)
         self.masked = np.zeros(nc, dtype=np.uint8)
@@ -221,7 +269,8 @@ class VoidPolicy:
 def dsa_matrix(geometry, quad, sigma_t, sigma_s, penalty=4.0, consistent=True, power=1.5, policy=None):
     """The DSA diffusion matrix (MIP at DG1, two-point flux at DG0) as SciPy
     CSR, with D and the masks of `policy` (default: the void policy's defaults)."""
-    g = geometry
+    g = own_geometry(geometry)
+    quad = own_quadrature(quad)
     nc, F, nb = g.n_cells, g.faces_per_cell, g.n_basis
     cap = nc * (F + 1) * nb * nb
     ri, ci, v = np.zeros(cap, dtype=np.int64), np.zeros(cap, dtype=np.int64), np.zeros(cap)
@@ -240,7 +289,8 @@ def dsa_matrix(geometry, quad, sigma_t, sigma_s, penalty=4.0, consistent=True, p
 
 
 def dsa_restrict(x, geometry, quad, masked=None):
-    g = geometry
+    g = own_geometry(geometry)
+    quad = own_quadrature(quad)
     rhs = np.empty(g.n_cells * g.n_basis)
     m = None if masked is None else np.ascontiguousarray(masked, dtype=np.uint8)
     _lib.oracle_dsa_restrict(g.n_cells, g.n_basis, quad.n_angles, quad.w, g.volume,
@@ -249,7 +299,8 @@ def dsa_restrict(x, geometry, quad, masked=None):
 
 
 def dsa_prolong(u, geometry, quad, masked=None):
-    g = geometry
+    g = own_geometry(geometry)
+    quad = own_quadrature(quad)
     y = np.empty(g.n_cells * g.n_basis * quad.n_angles)
     m = None if masked is None else np.ascontiguousarray(masked, dtype=np.uint8)
     _lib.oracle_dsa_prolong(g.n_cells, g.n_basis, quad.n_angles, quad.sum_weights,

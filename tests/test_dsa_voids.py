@@ -75,7 +75,7 @@ def test_masked_void_is_the_box_cut_off_at_the_void(dim, order):
     rest = np.setdiff1d(np.arange(Df.shape[0]), nodes_f)
     assert np.abs(Df[np.ix_(nodes_f, rest)]).max() == 0.0
     void_nodes = (np.flatnonzero(void)[:, None] * nb + np.arange(nb)).ravel()
-    want = np.diag(np.repeat(gf.volume[void], nb))
+    want = np.diag(np.repeat(O.own_geometry(gf).volume[void], nb))
     assert np.array_equal(Df[np.ix_(void_nodes, void_nodes)], want)
     # P D^-1 R: x a smooth function of (position, ordinate), the same on both boxes
     A = q.n_angles

@@ -14,10 +14,17 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import _lib
-from ._lib import lib, check
-
 SEED_BASE = 20261203
+# Cell shapes (UBOLT_TRI, ... of the C ABI)
+TRI, QUAD, TET, HEX = 3, 4, 10, 12
+
+
+def _native():
+    """The library's binding, loaded on first use: the mesh builders and the
+    named workloads' seeded data need no native code, so a CPU-only caller
+    (the oracle's baseline) can build them without loading the library."""
+    from . import _lib
+    return _lib, _lib.lib, _lib.check
 
 
 # ~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~
@@ -38,6 +45,7 @@ class Ordinates:
         return len(self.w)
 
     def struct(self):
+        _lib, _, _ = _native()
         q = _lib.Quadrature()
         q.dim, q.n_angles, q.sum_weights = self.dim, self.n_angles, self.sum_weights
         q.omega = self.omega.ctypes.data_as(_lib.dp)
@@ -56,6 +64,7 @@ class Ordinates:
 
 def lqn(dim, sn):
     """The level-symmetric S_N set in 2D (XY) or 3D."""
+    _lib, lib, check = _native()
     na, sw = C.c_int32(), C.c_double()
     check(lib.ubolt_quadrature_lqn(dim, sn, None, None, None, C.byref(na), C.byref(sw)))
     A = na.value
@@ -70,6 +79,7 @@ def lqn(dim, sn):
 
 def lqn_octant(sn):
     """(mu levels, 1-based level triples, whole-sphere weight fractions) of one octant."""
+    _lib, lib, check = _native()
     nl, npnt = C.c_int32(), C.c_int32()
     check(lib.ubolt_lqn_octant(sn, None, None, None, C.byref(nl), C.byref(npnt)))
     mu = np.zeros(nl.value)
@@ -130,7 +140,7 @@ def box_quads(nx, ny, lx=1.0, ly=1.0, jitter=0.0, rng=None, tile=8):
     i, j = ij[:, 0], ij[:, 1]
     vid = lambda a, b: b * (nx + 1) + a
     cells = np.stack([vid(i, j), vid(i + 1, j), vid(i + 1, j + 1), vid(i, j + 1)], axis=1)
-    return Mesh(2, _lib.QUAD, v, cells.astype(np.int64), (nx, ny))
+    return Mesh(2, QUAD, v, cells.astype(np.int64), (nx, ny))
 
 
 def box_tris(nx, ny, lx=1.0, ly=1.0, jitter=0.0, rng=None, tile=8, diagonals="random"):
@@ -149,7 +159,7 @@ def box_tris(nx, ny, lx=1.0, ly=1.0, jitter=0.0, rng=None, tile=8, diagonals="ra
     t0 = np.where(flip[:, None], c[:, [0, 1, 3]], c[:, [0, 1, 2]])
     t1 = np.where(flip[:, None], c[:, [1, 2, 3]], c[:, [0, 2, 3]])
     cells = np.stack([t0, t1], axis=1).reshape(-1, 3)
-    return Mesh(2, _lib.TRI, q.vertices, cells, (nx, ny))
+    return Mesh(2, TRI, q.vertices, cells, (nx, ny))
 
 
 def box_hexes(nx, ny, nz, lx=1.0, ly=1.0, lz=1.0, jitter=0.0, rng=None, tile=4):
@@ -165,7 +175,7 @@ def box_hexes(nx, ny, nz, lx=1.0, ly=1.0, lz=1.0, jitter=0.0, rng=None, tile=4):
     cells = np.stack([vid(i, j, k), vid(i + 1, j, k), vid(i + 1, j + 1, k), vid(i, j + 1, k),
                       vid(i, j, k + 1), vid(i + 1, j, k + 1), vid(i + 1, j + 1, k + 1), vid(i, j + 1, k + 1)],
                      axis=1)
-    return Mesh(3, _lib.HEX, v, cells.astype(np.int64), (nx, ny, nz))
+    return Mesh(3, HEX, v, cells.astype(np.int64), (nx, ny, nz))
 
 
 # Kuhn's six tetrahedra of a cube, all sharing the diagonal from vertex 0 to
@@ -176,7 +186,7 @@ _KUHN = [(0, 1, 2, 6), (0, 1, 5, 6), (0, 3, 2, 6), (0, 3, 7, 6), (0, 4, 5, 6), (
 def box_tets(nx, ny, nz, jitter=0.0, rng=None, tile=4):
     hx = box_hexes(nx, ny, nz, jitter=jitter, rng=rng, tile=tile)
     cells = np.concatenate([hx.cells[:, list(t)][:, None, :] for t in _KUHN], axis=1).reshape(-1, 4)
-    return Mesh(3, _lib.TET, hx.vertices, cells, (nx, ny, nz))
+    return Mesh(3, TET, hx.vertices, cells, (nx, ny, nz))
 
 
 # ~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~
@@ -207,6 +217,7 @@ class Geometry:
         raise AttributeError(name)
 
     def struct(self):
+        _lib, _, _ = _native()
         g = _lib.DGGeometry()
         g.dim, g.n_basis, g.faces_per_cell, g.n_cells = self.dim, self.n_basis, self.faces_per_cell, self.n_cells
         for name, dt, _ in _GEOM_ARRAYS + _DG1_ARRAYS:
@@ -217,7 +228,10 @@ class Geometry:
 
 
 def build_geometry(mesh, order, side_bc=None):
-    """ubolt_geometry_build on a Mesh; side_bc[2 * dim] are UBOLT_BC_* (default vacuum)."""
+    """ubolt_geometry_build on a Mesh; side_bc[2 * dim] are UBOLT_BC_* (default vacuum).
+    The result remembers what it was built from (`source`), so a checker can
+    build its own geometry from the same mesh."""
+    _lib, lib, check = _native()
     dim = mesh.dim
     sbc = np.zeros(2 * dim, dtype=np.int32) if side_bc is None else np.asarray(side_bc, dtype=np.int32)
     v = np.ascontiguousarray(mesh.vertices, dtype=np.float64)
@@ -237,7 +251,9 @@ def build_geometry(mesh, order, side_bc=None):
             ptr = getattr(view, name)
             n = sizes[sz]
             arrays[name] = np.ctypeslib.as_array(ptr, shape=(n,)).astype(dt, copy=True)
-        return Geometry(view.dim, nb, F, nc, arrays)
+        geo = Geometry(view.dim, nb, F, nc, arrays)
+        geo.source = (mesh, order, sbc.copy())
+        return geo
     finally:
         lib.ubolt_geometry_free(h)
 
@@ -279,14 +295,14 @@ def _streams(i, n=4):
     return [np.random.Generator(np.random.PCG64(s)) for s in np.random.SeedSequence(SEED_BASE + i).spawn(n)]
 
 
-def config_fd64(scale=1.0):
+def config_fd64(scale=1.0, geometry=None, quadrature=None):
     """64 x 64 unit-square cells, S4, one group, sigma_t 1, sigma_s 0.5, unit
     source in the central 16 x 16 cells, vacuum - the reference's plain CPU
     case. As DG0 on a uniform quad box, the structured upwind FD stencil's twin."""
     n = max(4, int(round(64 * scale)))
     mesh = box_quads(n, n, tile=8)
-    geom = build_geometry(mesh, 0)
-    quad = lqn(2, 4)
+    geom = (geometry or build_geometry)(mesh, 0)
+    quad = (quadrature or lqn)(2, 4)
     c = geom.centroid.reshape(-1, 3)
     lo, hi = 0.5 - 8.0 / 64.0, 0.5 + 8.0 / 64.0
     inside = (c[:, 0] > lo) & (c[:, 0] < hi) & (c[:, 1] > lo) & (c[:, 1] < hi)
@@ -296,15 +312,15 @@ def config_fd64(scale=1.0):
                    meta={"n": n})
 
 
-def config_tri256(scale=1.0, order=1, sn=8):
+def config_tri256(scale=1.0, order=1, sn=8, geometry=None, quadrature=None):
     """DG1 on a jittered 256 x 256 quad grid split into triangles, S8, one group:
     sigma_t lognormal(0, 0.5), c ~ U(0.3, 0.99), source 1.0 in a disk of 20%
     area with a seeded centre, cold vacuum."""
     n = max(4, int(round(256 * scale)))
     s_mesh, s_xs, s_src, _ = _streams(1)
     mesh = box_tris(n, n, jitter=0.2, rng=s_mesh, tile=8, diagonals="random")
-    geom = build_geometry(mesh, order)
-    quad = lqn(2, sn)
+    geom = (geometry or build_geometry)(mesh, order)
+    quad = (quadrature or lqn)(2, sn)
     nc = geom.n_cells
     sigma_t = s_xs.lognormal(0.0, 0.5, size=nc)
     ratio = s_xs.uniform(0.3, 0.99, size=nc)
@@ -317,7 +333,7 @@ def config_tri256(scale=1.0, order=1, sn=8):
                    meta={"n": n, "disk_centre": centre.tolist(), "disk_radius": r})
 
 
-def config_hex128(scale=1.0, order=1, sn=8, n_groups=4):
+def config_hex128(scale=1.0, order=1, sn=8, n_groups=4, geometry=None, quadrature=None):
     """128^3 hex box, S8 (80 angles), 4 groups, downscatter only: sigma_t per
     (8^3 block, group) = 10^U(-1, 1); per (block, group) a total scattering
     fraction f = U(0.5, 0.9) of sigma_t, of which U(0.5, 0.9) stays in group
@@ -326,8 +342,8 @@ def config_hex128(scale=1.0, order=1, sn=8, n_groups=4):
     n = max(8, int(round(128 * scale)))
     _, s_xs, _, _ = _streams(2)
     mesh = box_hexes(n, n, n, tile=4)
-    geom = build_geometry(mesh, order)
-    quad = lqn(3, sn)
+    geom = (geometry or build_geometry)(mesh, order)
+    quad = (quadrature or lqn)(3, sn)
     nc = geom.n_cells
     nb_blocks = max(1, n // 8)
     c = geom.centroid.reshape(-1, 3)
@@ -356,14 +372,14 @@ def config_hex128(scale=1.0, order=1, sn=8, n_groups=4):
                    np.zeros(6, dtype=np.int32), rtol=1e-8, meta={"n": n})
 
 
-def config_tet44(scale=1.0, order=1, sn=8):
+def config_tet44(scale=1.0, order=1, sn=8, geometry=None, quadrature=None):
     """Jittered Kuhn tets of a 44^3 cube grid (511,104 tets), S8 3D, one group:
     sigma_t lognormal(0, 1), c ~ U(0.5, 0.999), source 1.0 in [0.25, 0.75]^3."""
     n = max(2, int(round(44 * scale)))
     s_mesh, s_xs, _, _ = _streams(4)
     mesh = box_tets(n, n, n, jitter=0.2, rng=s_mesh, tile=4)
-    geom = build_geometry(mesh, order)
-    quad = lqn(3, sn)
+    geom = (geometry or build_geometry)(mesh, order)
+    quad = (quadrature or lqn)(3, sn)
     nc = geom.n_cells
     sigma_t = s_xs.lognormal(0.0, 1.0, size=nc)
     ratio = s_xs.uniform(0.5, 0.999, size=nc)
