@@ -306,3 +306,52 @@ def dsa_prolong(u, geometry, quad, masked=None):
     _lib.oracle_dsa_prolong(g.n_cells, g.n_basis, quad.n_angles, quad.sum_weights,
                             np.ascontiguousarray(u, dtype=np.float64), None if m is None else m.ctypes.data, y)
     return y
+
+
+def dsa_structured(nx, ny, hx, hy, quad, sigma_t, sigma_s, vacuum=(True, True, True, True), consistent=True,
+                   power=1.5):
+    """The structured backend's DSA matrix, cell-centred 5-point star per unit
+    volume (DSAStructured::assemble, src/dsa_structuredk.kokkos.cxx:183-288):
+    diagonal sigma_a + sum of the face terms; an interior face the harmonic
+    mean of the two D = 1/(3 sigma_t), blended with the axis's half-range
+    current times h when `consistent` (BlendD, dsa_operatork.hpp:122-126);
+    a vacuum side the Marshak term 1 / (h (2 + h / (2 D_b))), D_b the cell's
+    D blended the same way. Cells x-fastest; vacuum = (x lo, x hi, y lo, y hi)."""
+    quad = own_quadrature(quad)
+    st = np.asarray(sigma_t, dtype=np.float64)
+    ss = np.asarray(sigma_s, dtype=np.float64)
+    d = 1.0 / (3.0 * st)
+    h = (hx, hy)
+    half = [float(np.sum(np.where(quad.omega[:, ax] > 0.0, quad.w * quad.omega[:, ax], 0.0)) / quad.sum_weights)
+            for ax in range(2)]
+
+    def blend(v, m):
+        if not consistent:
+            return v
+        return v + m if power == 1.0 else (v ** power + m ** power) ** (1.0 / power)
+
+    n = nx * ny
+    rows, cols, vals = [], [], []
+    for j in range(ny):
+        for i in range(nx):
+            c = j * nx + i
+            diag = st[c] - ss[c]
+            for ax in range(2):
+                hd = h[ax]
+                for side in (-1, 1):
+                    ni, nj = (i + side, j) if ax == 0 else (i, j + side)
+                    inside = 0 <= ni < nx and 0 <= nj < ny
+                    if inside:
+                        cn = nj * nx + ni
+                        df = blend(2.0 * d[c] * d[cn] / (d[c] + d[cn]), half[ax] * hd)
+                        rows.append(c)
+                        cols.append(cn)
+                        vals.append(-df / (hd * hd))
+                        diag += df / (hd * hd)
+                    elif vacuum[2 * ax + (0 if side < 0 else 1)]:
+                        db = blend(d[c], half[ax] * hd)
+                        diag += 1.0 / (hd * (2.0 + hd / (2.0 * db)))
+            rows.append(c)
+            cols.append(c)
+            vals.append(diag)
+    return sp.csr_matrix((vals, (rows, cols)), shape=(n, n))

@@ -56,6 +56,33 @@ def test_dg0_two_point_flux_of_a_constant_is_absorption():
     assert np.abs(Du[inner] - (g.volume * (st - ss))[inner]).max() <= 1e-12 * np.abs(Du).max()
 
 
+@pytest.mark.parametrize("consistent", [True, False])
+def test_structured_dsa_is_the_dg0_two_point_dsa_on_a_uniform_box(consistent):
+    """The structured backend's DSA star (the reference's config-0 DSA,
+    dsa_structuredk.kokkos.cxx:183-288: harmonic face D, Marshak vacuum sides,
+    the consistent-D blend) restated in the oracle, against the DG0
+    two-point-flux DSA on the same uniform quad box: the same operator, the
+    plex rows carrying the cell volume. This is what links config 0's DSA to
+    the DG0 kernels the GPU path runs."""
+    nx, ny = 9, 7
+    mesh = P.box_quads(nx, ny)
+    g = P.build_geometry(mesh, 0)
+    q = P.lqn(2, 4)
+    rng = np.random.default_rng(12)
+    st = rng.uniform(0.5, 3.0, g.n_cells)
+    ss = st * rng.uniform(0.2, 0.95, g.n_cells)
+    Dp = O.dsa_matrix(g, q, st, ss, consistent=consistent).toarray()
+    og = O.own_geometry(g)
+    c = og.centroid.reshape(-1, 3)
+    ij = np.floor(c[:, 0] * nx).astype(int) + nx * np.floor(c[:, 1] * ny).astype(int)
+    order = np.empty(g.n_cells, dtype=int)
+    order[ij] = np.arange(g.n_cells)      # structured index -> plex cell
+    Ds = O.dsa_structured(nx, ny, 1.0 / nx, 1.0 / ny, q, st[order], ss[order], consistent=consistent).toarray()
+    V = og.volume[order]
+    got = Dp[np.ix_(order, order)]
+    assert np.abs(got - V[:, None] * Ds).max() <= 1e-12 * np.abs(got).max()
+
+
 def test_restrict_prolong_round_trip():
     """P D^{-1} R hands back u / W from the x that restricts to D u
     (verify_plexk check 11, the apply round trip)."""
