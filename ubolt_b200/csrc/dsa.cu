@@ -69,8 +69,9 @@ constexpr int kDsaScalars = 4;
 
 // Deterministic sum of d over the grid into *out: each block's total goes to
 // part[blockIdx.x]; the last block to finish (an integer counter) adds the
-// totals in block order, writes *out and resets the counter. No block waits
-// on another. Every thread of the block must call it.
+// totals in a fixed order - per-lane strided sums, then a shuffle tree, the
+// same every run - writes *out and resets the counter. No block waits on
+// another. Every thread of the block must call it.
 __device__ __forceinline__ void GridSum(double d, double *part, unsigned *count, double *out)
 {
    __shared__ double red[kDsaThreads / 32];
@@ -488,7 +489,7 @@ int DsaCorrect(ubolt_ctx *ctx, const T *r, T *y, T *tmp, void *stream)
    ubolt_dsa *ds = ctx->dsa;
    if ((rc = OperatorApply<T>(ctx, false, y, tmp, stream))) return rc;
    const int64_t threads = ds->n_nodes * 32;
-   DsaRestrictKernel<T><<<(threads + 255) / 256, 256, 0, s>>>(ds->n_nodes, ds->nb, ctx->A, ctx->g64.w, ctx->d_volume,
+   DsaRestrictKernel<T><<<(threads + 255) / 256, 256, 0, s>>>(ds->n_nodes, ds->nb, ctx->A, ctx->geom<double>().w, ctx->d_volume,
                                                               r, tmp, ds->mask, ds->rhs);
    CountLaunch();
    if ((rc = DsaSolveOnDevice(ctx, s))) return rc;
@@ -667,7 +668,7 @@ extern "C" int ubolt_dsa_restrict(ubolt_ctx *ctx, const double *x, double *rhs, 
    if (!x || !rhs) return SetError(UBOLT_ERR_ARG, "dsa_restrict: NULL array");
    const int64_t threads = ctx->n_nodes * 32;
    DsaRestrictKernel<double><<<(threads + 255) / 256, 256, 0, (cudaStream_t)stream>>>(
-      ctx->n_nodes, ctx->nb, ctx->A, ctx->g64.w, ctx->d_volume, x, nullptr, DsaMask(ctx), rhs);
+      ctx->n_nodes, ctx->nb, ctx->A, ctx->geom<double>().w, ctx->d_volume, x, nullptr, DsaMask(ctx), rhs);
    return CheckLaunch("dsa_restrict");
 }
 
@@ -689,7 +690,7 @@ extern "C" int ubolt_dsa_apply(ubolt_ctx *ctx, const double *x, double *y, void 
    cudaStream_t s = (cudaStream_t)stream;
    ubolt_dsa *ds = ctx->dsa;
    const int64_t threads = ds->n_nodes * 32;
-   DsaRestrictKernel<double><<<(threads + 255) / 256, 256, 0, s>>>(ds->n_nodes, ds->nb, ctx->A, ctx->g64.w,
+   DsaRestrictKernel<double><<<(threads + 255) / 256, 256, 0, s>>>(ds->n_nodes, ds->nb, ctx->A, ctx->geom<double>().w,
                                                                    ctx->d_volume, x, nullptr, ds->mask, ds->rhs);
    CountLaunch();
    if ((rc = DsaSolveOnDevice(ctx, s))) return rc;
@@ -766,14 +767,14 @@ extern "C" int ubolt_dsa_apply_static(ubolt_ctx *ctx, const double *x, double *y
    double *scal = base + 6 * nn;
    cudaStream_t s = (cudaStream_t)stream;
    const int64_t threads = ds->n_nodes * 32;
-   DsaRestrictKernel<double><<<(threads + 255) / 256, 256, 0, s>>>(ds->n_nodes, ds->nb, ctx->A, ctx->g64.w,
+   DsaRestrictKernel<double><<<(threads + 255) / 256, 256, 0, s>>>(ds->n_nodes, ds->nb, ctx->A, ctx->geom<double>().w,
                                                                    ctx->d_volume, x, nullptr, ds->mask, rhs);
    CountLaunch();
    // The same fixed-count block-Jacobi PCG as the workspace path; the
    // scalars are cleared here, every vector is written before it is read
    const int64_t nodes = ds->n_nodes;
    const int64_t grid = (nodes + 255) / 256;
-   cudaMemsetAsync(scal, 0, kDsaScalars * sizeof(double), s);
+   if ((rc = CudaCheck(cudaMemsetAsync(scal, 0, kDsaScalars * sizeof(double), s), "dsa_apply_static"))) return rc;
    CgStartKernel<<<grid, 256, 0, s>>>(nodes, ds->nb, ds->jinv, rhs, u, r, z, p, scal);
    CountLaunch();
    for (int it = 0; it < ds->inner_its; it++) {

@@ -77,8 +77,9 @@ constexpr int kChunk = 8;
 
 // h[i0 + i] = V_{i0+i} . w for i < nc: each block's share to
 // partial[blk][i0 + i], then the last block to finish (an integer counter,
-// reset by that block) adds the shares in block order, one warp per value.
-// No block waits on another.
+// reset by that block) adds the shares in a fixed order, one warp per value:
+// per-lane strided sums, then a shuffle tree, the same every run. No block
+// waits on another.
 template <typename S>
 __global__ void __launch_bounds__(kRedThreads) MultiDotKernel(const S *__restrict__ V, int64_t n, int i0, int nc,
                                                               const S *__restrict__ w, double *__restrict__ partial,
@@ -873,6 +874,9 @@ static int SolveSystem(ubolt_ctx *ctx, bool adjoint, const double *b, double *x,
    const int64_t n = ws->n;
    const int grid = GridFor(n);
    const auto t0 = std::chrono::steady_clock::now();
+   // The multi-dot's finished-block counter starts every solve at zero,
+   // whatever an earlier launch that failed part-way left in it
+   if ((rc = CudaCheck(cudaMemsetAsync(ws->md_count, 0, sizeof(unsigned), s), "solve"))) return rc;
    // The compressed form wherever its identity holds: the exact sweep alone
    // as preconditioner, and room for its four full-length vectors
    const bool iso = o.pc == UBOLT_PC_SWEEP && ws->Phi && SweepIsExact(ctx) &&
