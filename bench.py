@@ -49,6 +49,9 @@ def _args():
     p.add_argument("--scale", type=float, default=1.0, help="mesh scale (1.0 = the named workload)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--quick", action="store_true", help="skip the secondary measurements")
+    p.add_argument("--no-workloads", action="store_true",
+                   help="skip the hex128 and tet44 solve configurations that follow the headline")
+    p.add_argument("--reps", type=int, default=2, help="timed repetitions of each hex128 / tet44 measurement")
     p.add_argument("--workload", default="tri256", choices=["tri256", "hex128", "tet44"],
                    help="tri256 is the headline line; hex128 (4 groups) and tet44 time the other solve configs")
     p.add_argument("--restart", type=int, default=0, help="GMRES restart (0: 30, or 10 for hex128)")
@@ -245,6 +248,185 @@ def profile_kernel(args, ctx, T, stream):
                       "us_per_launch": e0.elapsed_time(e1) / args.steps * 1e3}), flush=True)
 
 
+def _events_ms(fn, stream, reps=1, warm=1):
+    """Median milliseconds of fn() over reps runs, CUDA events on `stream`."""
+    import torch
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    out = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        out.append(e0.elapsed_time(e1))
+    return float(np.median(out))
+
+
+def kernel_map(ctx, T, prob, stream, peak, peak_kind):
+    """Every kernel of the path on the workload, alone, with CUDA events: its
+    time, the algorithmic bytes of one launch (ψ in and out, cross sections;
+    geometry and indices excluded, so the figure never exceeds what must
+    move) over that time, and the fraction of the measured copy bandwidth."""
+    import torch
+    n, nc, nn, nb = ctx.n_rows, ctx.n_cells, ctx.n_nodes, prob.geometry.n_basis
+    F = prob.geometry.faces_per_cell
+    g = torch.Generator(device="cuda").manual_seed(11)
+    x64 = torch.rand(n, dtype=torch.float64, device="cuda", generator=g)
+    y64 = torch.empty_like(x64)
+    x32, y32 = x64.float(), torch.empty(n, dtype=torch.float32, device="cuda")
+    phi = torch.rand(nn, dtype=torch.float64, device="cuda", generator=g)
+    src = torch.rand(nc, dtype=torch.float64, device="cuda", generator=g)
+    A = T.TransportOperator(ctx)
+    B = T.ElementBlockInverse(ctx)
+    B.setup()
+    sw = T.Sweep.__new__(T.Sweep)
+    sw.ctx = ctx
+    ss = torch.tensor(prob.sigma_s[0, 0], device="cuda")
+    tr = T.GroupTransfer(ctx, [[ss, ss], [ss, ss]], [src, src])
+    tr.phi = [phi, phi]
+    dsa = T.DSAPrecon(ctx)
+    dsa.set_group()
+    u = torch.rand(nn, dtype=torch.float64, device="cuda", generator=g)
+    lam = torch.rand(n, dtype=torch.float64, device="cuda", generator=g)
+    nnz = nc * (F + 1) * nb * nb
+    cases = {
+        "apply_fp64": (lambda: A.mult(x64, y64), 2 * n * 8 + 2 * nc * 8),
+        "apply_fp32": (lambda: A.mult(x32, y32), 2 * n * 4 + 2 * nc * 4),
+        "apply_unscattered_fp64": (lambda: A.mult_unscattered(x64, y64), 2 * n * 8 + nc * 8),
+        "apply_adjoint_fp64": (lambda: A.mult_transpose(x64, y64), 2 * n * 8 + 2 * nc * 8),
+        "block_apply_fp64": (lambda: B.apply(x64, y64), 2 * n * 8 + nc * 8),
+        "sweep_fp64": (lambda: sw.apply(x64, y64), 2 * n * 8 + nc * 8),
+        "sweep_fp32": (lambda: sw.apply(x32, y32), 2 * n * 4 + nc * 4),
+        "scalar_flux_fp64": (lambda: T.angular_integral(ctx, x64, phi), n * 8 + nn * 8),
+        "add_transfer_fp64": (lambda: tr.add_transfer(0, 1, y64), 2 * n * 8 + nn * 8 + nc * 8),
+        "dsa_restrict_fp64": (lambda: dsa.restrict(x64), n * 8 + nn * 8),
+        "dsa_prolong_fp64": (lambda: dsa.prolong(u), n * 8 + nn * 8),
+        "dsa_spmv_fp64": (lambda: dsa.spmv(u), nnz * 8 + 2 * nn * 8),
+        "gradient_fp64": (lambda: T.gradient(ctx, x64, lam), 2 * n * 8 + 2 * nc * 8),
+    }
+    out = {}
+    for name, (fn, nbytes) in cases.items():
+        ms = _events_ms(lambda: [fn() for _ in range(10)], stream, reps=3, warm=1) / 10
+        gbs = nbytes / (ms * 1e-3) / 1e9
+        out[name] = {"us": ms * 1e3, "bytes": int(nbytes), "gbs": gbs, "frac": gbs / peak}
+    out["_peak"] = {"gbs": peak, "source": peak_kind}
+    return out
+
+
+def workload_hex128(args, stream):
+    """The mixed-precision configuration: 128^3 hexes, DG1, S8, 4 downscatter
+    groups; FP64 and FP32+refinement group solves to 1e-8, medians of
+    args.reps after a warm-up."""
+    import torch
+    from ubolt_b200 import problem as P
+    from ubolt_b200 import transport as T
+    t0 = time.perf_counter()
+    prob = P.config_hex128(scale=args.scale)
+    ctx = T.Context(prob.geometry, prob.quad)
+    out = {"workload": prob.name + ": 128^3 hex box, DG1 (4 modes), S8 (80 ordinates), 4 groups, downscatter",
+           "rows_per_group": ctx.n_rows, "restart": 10, "setup_s": time.perf_counter() - t0}
+    phis = {}
+    for precision in ("fp64", "mixed"):
+        opts = dict(rtol=prob.rtol, precision=precision, pc="sweep", restart=10, max_it=500)
+        res = {}
+
+        def run():
+            res["phi"], res["stats"] = T.solve_groups(ctx, prob.sigma_t, prob.sigma_s, prob.source, **opts)
+
+        ms = _events_ms(run, stream, reps=args.reps, warm=1)
+        st = res["stats"]
+        phis[precision] = [p_.clone() for p_ in res["phi"]]
+        out[precision] = {"s_per_solve": ms / 1e3, "iterations": [s_["iterations"] for s_ in st],
+                          "outer": [s_["outer"] for s_ in st], "residual": max(s_["residual"] for s_ in st)}
+    out["mixed"]["phi_rel_err_vs_fp64"] = max(float((m - f).norm() / f.norm())
+                                              for m, f in zip(phis["mixed"], phis["fp64"]))
+    out["mixed"]["speedup_vs_fp64"] = out["fp64"]["s_per_solve"] / out["mixed"]["s_per_solve"]
+    sw = T.Sweep.__new__(T.Sweep)
+    sw.ctx = ctx
+    xr = torch.rand(ctx.n_rows, dtype=torch.float64, device="cuda")
+    yr = torch.empty_like(xr)
+    out["sweep_ms"] = {"fp64": _events_ms(lambda: sw.apply(xr, yr), stream, reps=3)}
+    del xr, yr
+    xf = torch.rand(ctx.n_rows, dtype=torch.float32, device="cuda")
+    yf = torch.empty_like(xf)
+    out["sweep_ms"]["fp32"] = _events_ms(lambda: sw.apply(xf, yf), stream, reps=3)
+    del xf, yf
+    info = sw.status()
+    out["sweep"] = {k: info[k] for k in ("n_tasks", "n_split", "n_lagged", "factor_bytes", "patch_size", "kernel")}
+    ctx.close()
+    return out
+
+
+def workload_tet44(args, stream):
+    """The combined configuration: 511,104 jittered Kuhn tets, DG1, S8 3D, one
+    group, diffusive: FP64 and mixed forward solves, sweep + DSA against the
+    sweep alone, and the adjoint gradient of a detector response with respect
+    to the per-cell cross sections through the mixed form."""
+    import torch
+    from ubolt_b200 import problem as P
+    from ubolt_b200 import transport as T
+    t0 = time.perf_counter()
+    prob = P.config_tet44(scale=args.scale)
+    ctx = T.Context(prob.geometry, prob.quad)
+    st = torch.tensor(prob.sigma_t[0], device="cuda")
+    ss = torch.tensor(prob.sigma_s[0, 0], device="cuda")
+    ctx.set_group(st, ss)
+    src = torch.tensor(prob.source[0], device="cuda")
+    b = ctx.vector(fill=0.0)
+    T.GroupTransfer(ctx, [[ss]], [src]).add_external(0, b)
+    out = {"workload": prob.name + ": 44^3 cubes in Kuhn tets (jittered), DG1 (4 modes), S8 (80 ordinates), 1 group",
+           "rows": ctx.n_rows, "setup_s": time.perf_counter() - t0}
+    xs = {}
+    for key, opts in (("fp64", dict(precision="fp64", pc="sweep")), ("mixed", dict(precision="mixed", pc="sweep")),
+                      ("fp64_dsa", dict(precision="fp64", pc="sweep+dsa"))):
+        solver = T.TransportSolver(ctx, rtol=prob.rtol, restart=30, max_it=500, **opts)
+        if key == "fp64_dsa":
+            dsa = T.DSAPrecon(ctx)
+            dsa.set_group()
+        x = ctx.vector(fill=0.0)
+        res = {}
+
+        def run():
+            res["x"], res["stats"] = solver.solve(b, x)
+
+        ms = _events_ms(run, stream, reps=args.reps, warm=1)
+        xs[key] = res["x"].clone()
+        out[key] = {"s_per_solve": ms / 1e3, "iterations": res["stats"]["iterations"],
+                    "residual": res["stats"]["residual"]}
+    phi64 = T.angular_integral(ctx, xs["fp64"])
+    out["mixed"]["phi_rel_err_vs_fp64"] = float((T.angular_integral(ctx, xs["mixed"]) - phi64).norm() / phi64.norm())
+    out["mixed"]["speedup_vs_fp64"] = out["fp64"]["s_per_solve"] / out["mixed"]["s_per_solve"]
+    out["fp64_dsa"]["phi_rel_err_vs_fp64"] = float((T.angular_integral(ctx, xs["fp64_dsa"]) - phi64).norm()
+                                                   / phi64.norm())
+    out["fp64_dsa"]["speedup_vs_sweep_only"] = out["fp64"]["s_per_solve"] / out["fp64_dsa"]["s_per_solve"]
+    # Adjoint gradient through the mixed form
+    det = P.detector_patch(prob, cells_per_side=11, seed_index=4).astype(np.float64)
+    model = T.DetectorResponse(ctx, prob.source[0], det, rtol=prob.rtol, max_it=500, precision="mixed")
+    sig_t = st.clone().requires_grad_(True)
+    sig_s = ss.clone().requires_grad_(True)
+    J = model(sig_t, sig_s)
+    torch.autograd.grad(J, (sig_t, sig_s))
+    torch.cuda.synchronize()
+    g0, g1, g2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    g0.record(stream)
+    J = model(sig_t, sig_s)
+    g1.record(stream)
+    gt, gs = torch.autograd.grad(J, (sig_t, sig_s))
+    g2.record(stream)
+    torch.cuda.synchronize()
+    fwd, tot = g0.elapsed_time(g1), g0.elapsed_time(g2)
+    out["adjoint"] = {"grad_s": tot / 1e3, "forward_s": fwd / 1e3, "adjoint_over_forward": (tot - fwd) / fwd,
+                      "precision": "mixed", "parameters": 2 * ctx.n_cells, "J": float(J.item()),
+                      "adjoint_iterations": model.last_adjoint["iterations"],
+                      "detector_cells": int(det.sum())}
+    ctx.set_group(st, ss)
+    ctx.close()
+    return out
+
+
 def run_workload(args):
     """--workload hex128 | tet44: the other solve configs, FP64 and mixed, as one
     JSON line each (no CPU baseline: the restatement would take hours here)."""
@@ -387,6 +569,9 @@ def main():
         sweep_bytes64 = 2 * n * 8 + ctx.n_cells * 8
         extra["apply_gbs"] = {"fp64": apply_bytes64 / t_apply64 / 1e6, "fp32": apply_bytes32 / t_apply32 / 1e6,
                               "fp64_us": t_apply64 * 1e3, "fp32_us": t_apply32 * 1e3}
+        peak, peak_kind = _peaks()
+        extra["kernels"] = kernel_map(ctx, T, prob, stream, peak, peak_kind)
+        ctx.set_group(st, ss)
         extra["sweep_us"] = {"fp64": t_sweep64 * 1e3, "fp32": t_sweep32 * 1e3}
         # Dominant kernel of the solve: one sweep per iteration; the full basis
         # adds one apply per iteration and a sweep per cycle
@@ -401,15 +586,20 @@ def main():
         else:
             ach = apply_bytes64 / t_apply64 / 1e6
             kernel, traffic_key = "ApplyKernel<double,3,3,0>", "apply_fp64"
-        traffic = None
+        # DRAM bytes of one launch of that kernel, from a committed ncu capture
+        # (not measured by this run)
+        traffic, traffic_source = None, None
         tpath = os.path.join(ROOT, "profiles", "traffic.json")
         if os.path.exists(tpath):
             try:
-                traffic = json.load(open(tpath)).get(traffic_key)
+                tj = json.load(open(tpath))
+                traffic = tj.get(traffic_key)
+                traffic_source = f"ncu capture, profiles/traffic.json [{traffic_key}]: {tj.get('_source', '')}"
             except Exception:
-                traffic = None
+                traffic, traffic_source = None, None
         extra["roofline"] = {"bound": "hbm", "kernel": kernel, "achieved": ach, "peak": peak, "unit": "GB/s",
                              "frac": ach / peak, "peak_source": peak_kind, "traffic": traffic,
+                             "traffic_unit": "bytes per launch", "traffic_source": traffic_source,
                              "share_of_solve": (t_sweep64 * sweeps if dom_sweep else t_apply64 * applies) / ms}
 
         # ~~~ Mixed precision: FP32 operator / sweep / Krylov storage + FP64 refinement
@@ -494,6 +684,15 @@ def main():
         phi_o = O.angular_integral(xcpu, ctx.n_nodes, q)
         cpu["phi_rel_diff_gpu_vs_cpu"] = float(np.linalg.norm(phi_c - phi_o) / np.linalg.norm(phi_o))
 
+    ctx.close()
+    # ~~~ The other solve configurations (one GPU each; under torchrun every
+    # rank runs its own copy, so all ranks take the same steps)
+    if not args.quick and not args.no_workloads:
+        torch.cuda.empty_cache()
+        extra["hex128"] = workload_hex128(args, stream)
+        torch.cuda.empty_cache()
+        extra["tet44"] = workload_tet44(args, stream)
+
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "s/solve", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
@@ -513,7 +712,6 @@ def main():
         if cpu:
             line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)
-    ctx.close()
     if world > 1:
         dist.destroy_process_group()
 
