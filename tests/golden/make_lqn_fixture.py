@@ -12,7 +12,9 @@ import json
 import os
 import sys
 
-ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: python tests/golden/make_lqn_fixture.py /path/to/UBOLT")
+ref = sys.argv[1]
 sys.path.insert(0, os.path.join(ref, "src"))
 import sn_lqn_table as gen  # noqa: E402
 
