@@ -227,16 +227,34 @@ typedef struct {
    int32_t grid;          /* blocks of the last launch */
    int64_t total_levels;
    uint32_t timeouts;     /* bounded waits that gave up since the last status */
-   uint32_t pad_;
+   int32_t kernel;        /* UBOLT_SWEEP_TASKS or UBOLT_SWEEP_WAVE: what ubolt_sweep (FP64) runs now */
    int64_t factor_bytes;  /* device bytes held by the factor stores (FP64 + FP32) */
 } ubolt_sweep_info;
 
+/* The two sweep kernels. TASKS: persistent warps over (patch, ordinate)
+ * tasks that wait on each other's values through L2 - any mesh, cycles
+ * included. WAVE: one block per ordinate walks that ordinate's levels with a
+ * barrier between them, its upwind front in shared memory and its factors
+ * streamed in by bulk copies - meshes whose every ordinate's upwind graph is
+ * acyclic (2D, hexahedra), with a reserved factor store, no wait on another
+ * block. One block per ordinate leaves most SMs idle and pays for every
+ * scattered psi word on one SM, so AUTO picks WAVE only where it applies
+ * and the problem is small (n_cells A <= 2^17, where it measured faster),
+ * TASKS otherwise. */
+enum { UBOLT_SWEEP_AUTO = 0, UBOLT_SWEEP_TASKS = 1, UBOLT_SWEEP_WAVE = 2 };
+
 /* Build the sweep plan: patches of patch_size consecutive cells (0 picks 64;
- * at most 256), per-ordinate upwind orders, task list. Host
- * work plus one upload; independent of the group. Called by the first sweep
- * if not before. The streaming stage of the preconditioner, in place of
+ * at most 256), per-ordinate upwind orders, task list; then reserve the
+ * factor stores (see ubolt_sweep_set_factor_limit). Host work, one upload
+ * and the sweep's only device allocations; independent of the group.
+ * Called by the first sweep if not before. The streaming stage of the preconditioner, in place of
  * PCAIR (src/transport_solverk.kokkos.cxx:238-260, composite index 1). */
 int ubolt_sweep_setup(ubolt_ctx *ctx, int patch_size);
+/* Choose the sweep kernel (UBOLT_SWEEP_*; AUTO by default). WAVE where it
+ * does not apply gives UBOLT_ERR_STATE. Both give L^{-1} q to rounding. A
+ * set-up call: the factor stores are reserved again in the chosen kernel's
+ * order (and rebuilt by the next sweep). */
+int ubolt_sweep_set_kernel(ubolt_ctx *ctx, int kernel);
 /* psi = L^{-1} q for every ordinate: exact where the per-ordinate upwind
  * graph is acyclic; reflective inflow and cycle-breaking couplings are lagged
  * to zero. psi is first filled with all-ones bytes on `stream` (the kernel's
@@ -244,14 +262,15 @@ int ubolt_sweep_setup(ubolt_ctx *ctx, int patch_size);
  * bounded; check ubolt_sweep_status. */
 int ubolt_sweep(ubolt_ctx *ctx, const double *q, double *psi, void *stream);
 int ubolt_sweep_f32(ubolt_ctx *ctx, const float *q, float *psi, void *stream);
-/* The factor store: each cell-ordinate's B^{-1} and upwind couplings
+/* The factor stores: each cell-ordinate's B^{-1} and upwind couplings
  * G_f = B^{-1} s_f face_up_f, which depend on geometry and sigma_t but not on
- * q, built once per group (ubolt_set_group starts a new group) and read by
- * every sweep instead of being recomputed: n_cells A nb^2 (1 + slots)
- * values per precision, in task order. bytes < 0 (the default): build it
- * when it fits half the free device memory, at most 96 GiB; 0: never;
- * otherwise the limit in bytes. Either way the result is the same, bit for
- * bit. Frees a store the new limit does not admit. */
+ * q, rebuilt by one kernel launch on the first sweep after ubolt_set_group
+ * and read by every sweep instead of being recomputed: n_cells A nb^2 (1 +
+ * slots) values per precision, in task order. Reserved when the plan is
+ * built, or now by this call - never inside a sweep. bytes < 0 (the
+ * default): each store that fits half the free device memory at that
+ * moment (at most 96 GiB), FP32 first; 0: none; otherwise the byte limit
+ * for both together. Either way the result is the same, bit for bit. */
 int ubolt_sweep_set_factor_limit(ubolt_ctx *ctx, int64_t bytes);
 /* Plan statistics and the sticky timeout flag (synchronises `stream`):
  * returns UBOLT_ERR_TIMEOUT, and clears the flag, if a wait gave up. */
@@ -286,6 +305,45 @@ typedef struct {
 int ubolt_sweep_plan_build(const ubolt_dg_geometry *geom, const ubolt_quadrature *quad, int patch_size,
                            ubolt_sweep_plan_host **out, ubolt_sweep_plan_view *view);
 void ubolt_sweep_plan_free(ubolt_sweep_plan_host *plan);
+
+/* The wave plan on the host alone, for inspection: per ordinate, the cells
+ * in level order (positions) and the front slot of shared memory each
+ * solved value lives in while later levels read it. */
+typedef struct ubolt_wave_plan_host ubolt_wave_plan_host;
+typedef struct {
+   int32_t acyclic;          /* 0: some ordinate's upwind graph has a cycle; the arrays below are NULL */
+   int32_t slots;            /* most gathered upwind faces of one position */
+   int32_t n_front;          /* front slots the busiest ordinate needs */
+   int32_t max_width;        /* most positions in one level */
+   int32_t max_levels;       /* most levels of one ordinate */
+   int32_t pad_;
+   int64_t total_levels;     /* summed over the ordinates */
+   const int32_t *lvl_base;  /* [A + 1]: ordinate a's levels are lvl_base[a] .. lvl_base[a + 1] - 1 */
+   const int32_t *lvl_pos;   /* [total_levels + A]: level l of ordinate a starts at position
+                                lvl_pos[lvl_base[a] + a + l]; one end entry per ordinate */
+   const int32_t *meta;      /* [A][n_cells][4] per position: cell; front slot | gathered-face mask << 16
+                                (slot 0xffff: no later level reads it); the upwind cells' slots in face
+                                order, two 16-bit slots per word */
+} ubolt_wave_plan_view;
+int ubolt_wave_plan_build(const ubolt_dg_geometry *geom, const ubolt_quadrature *quad, ubolt_wave_plan_host **out,
+                          ubolt_wave_plan_view *view);
+/* One precision's layout of the wave sweep, for a block with at most
+ * max_shared_bytes of shared memory: the block's shared memory (mbarriers,
+ * level tables, the front at front_off, the ring of `cap` bytes at
+ * ring_base) and the factor store (ordinate a's region at byte region[a];
+ * level chunks at region-relative chunk_rel[.], indexed as lvl_pos, landing
+ * in the ring at ring_off[.]). Arrays are owned by the plan handle and
+ * replaced by the next call. UBOLT_ERR_STATE where a level does not fit. */
+typedef struct {
+   int32_t front_off, ring_base, cap, smem;
+   int64_t store_bytes;
+   const int64_t *region;
+   const int32_t *chunk_rel;
+   const int32_t *ring_off;
+} ubolt_wave_layout_view;
+int ubolt_wave_plan_layout(ubolt_wave_plan_host *plan, int n_basis, int elem_bytes, int max_shared_bytes,
+                           ubolt_wave_layout_view *view);
+void ubolt_wave_plan_free(ubolt_wave_plan_host *plan);
 
 /* ~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~
  * DSA: the diffusion correction y = P D^{-1} R x (DSAPrecon, include/ubolt/dsa.hpp)
@@ -345,6 +403,8 @@ int ubolt_dsa_prolong(ubolt_ctx *ctx, const double *u, double *y, void *stream);
  * by every GPU that loads the library until the process exits. The first
  * call on a device looks up the array's device address (cudaGetSymbolAddress)
  * with that device current; make that first call before any stream capture.
+ * The address is kept for the life of the process: after a cudaDeviceReset
+ * on that device the library must be reloaded before this call is used again.
  * Every call, from any context on the device, shares the one array and
  * leaves the last call's values in it: calls that overlap on the GPU race.
  * ubolt_dsa_setup and ubolt_dsa_set_group must have run; the call itself

@@ -36,11 +36,15 @@ ACYCLIC = [c for c in CASES if c[1] == 2 or c[0].startswith("hex")]
 @pytest.mark.parametrize("case", ACYCLIC, ids=[c[0] for c in ACYCLIC])
 @pytest.mark.parametrize("patch", [0, 16, 100])
 def test_sweep_matches_oracle(case, patch):
-    """Both ways to the factors - the per-group store and the in-sweep
-    computation - give the oracle's sweep, and each other's bit for bit."""
+    """Task kernel: both ways to the factors - the per-group store and the
+    in-sweep computation - give the oracle's sweep, and each other's bit for
+    bit. Wave kernel (one block per ordinate): the oracle's sweep too, the
+    same bits on every run, and the task kernel's result to rounding."""
+    from ubolt_b200 import _lib
     mesh, g, q, st, ss = build(case)
     ctx, keep = ctx_for(g, q, st, ss)
     sw = T.Sweep(ctx, patch)
+    sw.set_kernel("tasks")
     op = O.Operator(g, q, st, ss)
     qv = np.random.default_rng(1).standard_normal(op.n)
     ref = op.sweep(qv)
@@ -49,6 +53,7 @@ def test_sweep_matches_oracle(case, patch):
     assert all(torch.equal(r, psi) for r in runs)  # and the result does not depend on timing
     info = sw.status()
     assert info["timeouts"] == 0 and info["n_lagged"] == 0 and info["factor_bytes"] > 0
+    assert info["kernel"] == _lib.SWEEP_TASKS
     assert np.abs(psi.cpu().numpy() - ref).max() <= 1e-12 * np.abs(ref).max()
     psi32 = sw.apply(dev(qv, torch.float32))
     assert np.abs(psi32.double().cpu().numpy() - ref).max() <= 1e-4 * np.abs(ref).max()
@@ -56,6 +61,44 @@ def test_sweep_matches_oracle(case, patch):
     assert sw.status()["factor_bytes"] == 0
     assert torch.equal(sw.apply(dev(qv)), psi)
     assert torch.equal(sw.apply(dev(qv, torch.float32)), psi32)
+
+    sw.set_factor_limit(-1)
+    sw.set_kernel("wave")
+    waves = [sw.apply(dev(qv)) for _ in range(3)]
+    info = sw.status()
+    assert info["kernel"] == _lib.SWEEP_WAVE and info["timeouts"] == 0 and info["factor_bytes"] > 0
+    assert all(torch.equal(r, waves[0]) for r in waves)
+    assert np.abs(waves[0].cpu().numpy() - ref).max() <= 1e-12 * np.abs(ref).max()
+    assert float((waves[0] - psi).abs().max()) <= 1e-13 * float(psi.abs().max())
+    wave32 = sw.apply(dev(qv, torch.float32))
+    assert np.abs(wave32.double().cpu().numpy() - ref).max() <= 1e-4 * np.abs(ref).max()
+    ctx.close()
+
+
+def test_named_triangle_mesh_sweep_kernels_agree():
+    """256 x 256 jittered quads split into triangles, DG1, S8 (the plain FP64
+    workload): the wave kernel and the task kernel give the same sweep to
+    rounding, in FP64 and in FP32. Its 40 ordinates do not fill the device,
+    so the automatic choice is the task kernel."""
+    from ubolt_b200 import _lib
+    prob = P.config_tri256()
+    g, q = prob.geometry, prob.quad
+    ctx, keep = ctx_for(g, q, prob.sigma_t[0], prob.sigma_s[0, 0])
+    sw = T.Sweep(ctx)
+    assert sw.status()["kernel"] == _lib.SWEEP_TASKS
+    sw.set_kernel("wave")
+    assert sw.status()["kernel"] == _lib.SWEEP_WAVE
+    qv = dev(np.random.default_rng(12).uniform(0.0, 1.0, ctx.n_rows))
+    wave64 = sw.apply(qv)
+    wave32 = sw.apply(qv.float())
+    assert sw.status()["timeouts"] == 0
+    sw.set_kernel("tasks")
+    task64 = sw.apply(qv)
+    task32 = sw.apply(qv.float())
+    scale = float(task64.abs().max())
+    assert float((wave64 - task64).abs().max()) <= 1e-13 * scale
+    assert float((wave32 - task32).abs().max()) <= 1e-5 * scale
+    assert float((wave32.double() - wave64).abs().max()) <= 1e-5 * scale
     ctx.close()
 
 
@@ -72,6 +115,34 @@ def test_sweep_factor_store_follows_the_group():
     psi = sw.apply(dev(qv)).cpu().numpy()
     ref = O.Operator(g, q, st2, ss).sweep(qv)
     assert np.abs(psi - ref).max() <= 1e-12 * np.abs(ref).max()
+    ctx.close()
+
+
+def test_sweep_and_solve_allocate_nothing_once_set_up():
+    """Once the solver and the sweep plan are set up (the factor stores are
+    reserved then), a new group, its sweeps and its solves allocate no device
+    memory: the stores are rebuilt by a kernel, the workspace is reused
+    (the reference's rule for the group sweep, AGENTS.md:46-47)."""
+    mesh, g, q, st, ss = build(CASES[0])
+    ctx, keep = ctx_for(g, q, st, ss)
+    solver = T.TransportSolver(ctx, rtol=1e-10, pc="sweep")
+    sw = T.Sweep.__new__(T.Sweep)
+    sw.ctx = ctx
+    assert sw.status()["factor_bytes"] > 0
+    rng = np.random.default_rng(9)
+    b = dev(rng.uniform(0.1, 1.0, ctx.n_rows))
+    x = ctx.vector(fill=0.0)
+    qv, psi = dev(rng.standard_normal(ctx.n_rows)), ctx.vector()
+    keep2 = (dev(st * 1.3), dev(ss * 0.7))
+    solver.solve(b, x)
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    ctx.set_group(*keep2)
+    sw.apply(qv, psi)
+    x, stats = solver.solve(b, x)
+    torch.cuda.synchronize()
+    assert stats["converged"]
+    assert torch.cuda.mem_get_info()[0] == free0
     ctx.close()
 
 
@@ -218,14 +289,53 @@ def test_multigroup_downscatter_sweep_matches_oracle():
     ctx.close()
 
 
-def test_sweep_wait_that_runs_out_is_reported_and_recovers():
-    """A sweep whose one wait can never be met (a value nothing stores) with a
-    short limit: the sweep still completes, the host reads UBOLT_ERR_TIMEOUT,
-    and the next sweep on the same context is exact again."""
+def test_plain_cpu_workload_sweep_dsa_solve_matches_the_fd_oracle():
+    """The reference's plain CPU case at its full size: 64 x 64 unit-square
+    cells, S4, sigma_t 1, sigma_s 0.5, unit source in the central 16 x 16
+    cells, vacuum, rtol 1e-10 - on the GPU as DG0 on the uniform quad box
+    (the structured FD stencil's twin) with the sweep + DSA preconditioner,
+    against the oracle's structured FD operator solved directly."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spla
+    prob = P.config_fd64()
+    g, q = prob.geometry, prob.quad
+    n = prob.meta["n"]
+    A = q.n_angles
+    st, ss, src = prob.sigma_t[0], prob.sigma_s[0, 0], prob.source[0]
+    og = O.own_geometry(g)
+    cen = og.centroid.reshape(-1, 3)
+    natural = (np.floor(cen[:, 1] * n).astype(int) * n + np.floor(cen[:, 0] * n).astype(int))
+    inv = np.empty_like(natural)
+    inv[natural] = np.arange(g.n_cells)
+    L = O.fd2d(n, n, q, st[inv])
+    oq = O.own_quadrature(q)
+    S = sp.kron(sp.diags(ss[inv]), np.outer(np.ones(A), oq.w / oq.sum_weights), format="csr")
+    b_nat = np.repeat(src[inv] / oq.sum_weights, A)
+    x_nat = spla.spsolve((L - S).tocsc(), b_nat)
+    phi_ref = (x_nat.reshape(-1, A) @ oq.w)[natural]
+    ctx, keep = ctx_for(g, q, st, ss)
+    dsa = T.DSAPrecon(ctx)
+    dsa.set_group()
+    b = ctx.vector(fill=0.0)
+    T.GroupTransfer(ctx, [[keep[1]]], [dev(src)]).add_external(0, b)
+    x, stats = T.TransportSolver(ctx, rtol=prob.rtol, pc="sweep+dsa", max_it=500).solve(b)
+    assert stats["converged"] and stats["residual"] <= prob.rtol * 1.01
+    phi = T.angular_integral(ctx, x).cpu().numpy()
+    assert np.linalg.norm(phi - phi_ref) <= 1e-9 * np.linalg.norm(phi_ref)
+    ctx.close()
+
+
+@pytest.mark.parametrize("kernel", ["tasks", "wave"])
+def test_sweep_wait_that_runs_out_is_reported_and_recovers(kernel):
+    """A sweep whose one wait can never be met, with a short limit - the task
+    kernel polls a value nothing stores, the wave kernel waits for a level's
+    copy that is never issued: the sweep still completes, the host reads
+    UBOLT_ERR_TIMEOUT, and the next sweep on the same context is exact again."""
     from ubolt_b200 import _lib
     mesh, g, q, st, ss = build(CASES[0])
     ctx, keep = ctx_for(g, q, st, ss)
     sw = T.Sweep(ctx, 16)
+    sw.set_kernel(kernel)
     op = O.Operator(g, q, st, ss)
     qv = np.random.default_rng(1).standard_normal(op.n)
     _lib.check(_lib.lib.ubolt_sweep_test_wait(ctx.handle, 2000, 1))

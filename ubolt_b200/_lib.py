@@ -94,7 +94,7 @@ def declared_symbols(header=None):
 class SweepInfo(C.Structure):
     _fields_ = [("patch_size", C.c_int32), ("n_patches", C.c_int32), ("n_tasks", C.c_int64),
                 ("n_lagged", C.c_int64), ("n_split", C.c_int64), ("max_levels", C.c_int32), ("grid", C.c_int32),
-                ("total_levels", C.c_int64), ("timeouts", C.c_uint32), ("pad_", C.c_uint32),
+                ("total_levels", C.c_int64), ("timeouts", C.c_uint32), ("kernel", C.c_int32),
                 ("factor_bytes", C.c_int64)]
 
 
@@ -157,6 +157,64 @@ def sweep_plan(geometry, quad, patch_size=0):
         return out
     finally:
         lib.ubolt_sweep_plan_free(h)
+
+SWEEP_AUTO, SWEEP_TASKS, SWEEP_WAVE = 0, 1, 2
+_sig("ubolt_sweep_set_kernel", C.c_int, vp, C.c_int)
+
+
+class WavePlanView(C.Structure):
+    _fields_ = [("acyclic", C.c_int32), ("slots", C.c_int32), ("n_front", C.c_int32), ("max_width", C.c_int32),
+                ("max_levels", C.c_int32), ("pad_", C.c_int32), ("total_levels", C.c_int64), ("lvl_base", i32p),
+                ("lvl_pos", i32p), ("meta", i32p)]
+
+
+_sig("ubolt_wave_plan_build", C.c_int, C.POINTER(DGGeometry), C.POINTER(Quadrature), C.POINTER(vp),
+     C.POINTER(WavePlanView))
+_sig("ubolt_wave_plan_free", None, vp)
+
+
+class WaveLayoutView(C.Structure):
+    _fields_ = [("front_off", C.c_int32), ("ring_base", C.c_int32), ("cap", C.c_int32), ("smem", C.c_int32),
+                ("store_bytes", C.c_int64), ("region", i64p), ("chunk_rel", i32p), ("ring_off", i32p)]
+
+
+_sig("ubolt_wave_plan_layout", C.c_int, vp, C.c_int, C.c_int, C.c_int, C.POINTER(WaveLayoutView))
+
+B200_MAX_SHARED_PER_BLOCK = 232448  # cudaDevAttrMaxSharedMemoryPerBlockOptin on sm_100
+
+
+def wave_plan(geometry, quad, layouts=()):
+    """The wave plan built on the host, as NumPy arrays (for inspection and
+    tests); layouts: (n_basis, elem_bytes, max_shared_bytes) triples whose
+    store and shared-memory layouts to add under "layout"."""
+    import numpy as np
+    h = vp()
+    view = WavePlanView()
+    gs, qs = geometry.struct(), quad.struct()
+    check(lib.ubolt_wave_plan_build(C.byref(gs), C.byref(qs), C.byref(h), C.byref(view)))
+    try:
+        A = quad.n_angles
+        out = {"acyclic": bool(view.acyclic), "slots": view.slots, "n_front": view.n_front,
+               "max_width": view.max_width, "max_levels": view.max_levels, "total_levels": view.total_levels,
+               "lvl_base": np.ctypeslib.as_array(view.lvl_base, shape=(A + 1,)).copy()}
+        if view.acyclic:
+            out["lvl_pos"] = np.ctypeslib.as_array(view.lvl_pos, shape=(view.total_levels + A,)).copy()
+            out["meta"] = np.ctypeslib.as_array(view.meta, shape=(A * geometry.n_cells * 4,)).copy().reshape(
+                A, geometry.n_cells, 4)
+        out["layout"] = {}
+        for key in layouts:
+            lv = WaveLayoutView()
+            check(lib.ubolt_wave_plan_layout(h, *key, C.byref(lv)))
+            n = view.total_levels + A
+            out["layout"][tuple(key)] = {
+                "front_off": lv.front_off, "ring_base": lv.ring_base, "cap": lv.cap, "smem": lv.smem,
+                "store_bytes": lv.store_bytes, "region": np.ctypeslib.as_array(lv.region, shape=(A,)).copy(),
+                "chunk_rel": np.ctypeslib.as_array(lv.chunk_rel, shape=(n,)).copy(),
+                "ring_off": np.ctypeslib.as_array(lv.ring_off, shape=(n,)).copy()}
+        return out
+    finally:
+        lib.ubolt_wave_plan_free(h)
+
 
 _sig("ubolt_launch_count", C.c_uint64)
 _sig("ubolt_solve_adjoint", C.c_int, vp, vp, vp, C.POINTER(SolveOptions), C.POINTER(SolveStats), vp)

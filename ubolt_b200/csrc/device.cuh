@@ -316,4 +316,51 @@ __host__ inline int CellsPerBlock(int A)
    return k < 1 ? 1 : k;
 }
 
+// The factors of one (cell, ordinate) for the sweep: W = B^{-1} of its
+// streaming + removal block, and G_s = W (s_f face_up_f) for each gathered
+// face f in face order (slot s); element (s, ii, j) goes to Gout[s * gs + (ii * NB + j) * ge].
+// A singular block gives zero factors. Returns false then.
+template <typename T, int NB, int F>
+__device__ __forceinline__ bool CellFactors(const DevGeom<T> &g, int64_t c, const T om[3], uint32_t mask, T W[NB][NB],
+                                            T *Gout, size_t gs, size_t ge)
+{
+   const int32_t cl = g.cls[c];
+   T B[NB][NB];
+   BuildBlock<T, NB, F>(g, cl, om, g.sigma_t[c], B);
+   const bool ok = InvertBlock<T, NB>(B, W);
+   if (!ok)
+#pragma unroll
+      for (int ii = 0; ii < NB; ii++)
+#pragma unroll
+         for (int j = 0; j < NB; j++) W[ii][j] = T(0);
+   int slot = 0;
+#pragma unroll
+   for (int f = 0; f < F; f++) {
+      if (!(((mask >> f) | (mask >> (8 + f))) & 1u)) continue;
+      const T sf = Dot3(om, g.nA + ((int64_t)cl * F + f) * 3);
+      T *Gf = Gout + (size_t)slot * gs;
+      if constexpr (NB == 1) {
+         Gf[0] = W[0][0] * (sf * g.inv_vol[cl]);
+      } else {
+         const T *M = g.fup + ((int64_t)cl * F + f) * NB * NB;
+         T Ms[NB][NB];
+#pragma unroll
+         for (int kk = 0; kk < NB; kk++)
+#pragma unroll
+            for (int j = 0; j < NB; j++) Ms[kk][j] = sf * M[kk * NB + j];
+#pragma unroll
+         for (int ii = 0; ii < NB; ii++)
+#pragma unroll
+            for (int j = 0; j < NB; j++) {
+               T u = T(0);
+#pragma unroll
+               for (int kk = 0; kk < NB; kk++) u += W[ii][kk] * Ms[kk][j];
+               Gf[(size_t)(ii * NB + j) * ge] = u;
+            }
+      }
+      slot++;
+   }
+   return ok;
+}
+
 }  // namespace ubolt

@@ -30,6 +30,7 @@
 // records a timeout, reads the value as zero and the sweep completes.
 #include "ctx.h"
 #include "sweep_plan.h"
+#include "wave.h"
 
 #include <algorithm>
 #include <vector>
@@ -38,7 +39,7 @@
 // warp increments the counter, and a spinning lane must not contend with it.
 // Words [kCtrlNever, kCtrlNever + 2) hold a sentinel nothing overwrites (the
 // target of the bounded-wait test hook).
-constexpr int kCtrlCounter = 0, kCtrlError = 32, kCtrlNever = 48, kCtrlWords = 64;
+constexpr int kCtrlCounter = 0, kCtrlError = ubolt::kSweepCtrlError, kCtrlNever = 48, kCtrlWords = 64;
 constexpr int kSweepBlocksPerSm = 8;  // of 4 warps
 constexpr int kDefaultPatch = 64;
 
@@ -67,6 +68,18 @@ struct ubolt_sweep_plan {
    void *fac[2] = {nullptr, nullptr};
    uint64_t fac_epoch[2] = {0, 0};
    int64_t fac_limit = -1;
+   // The wave plan (one block per ordinate), where every ordinate's upwind
+   // graph is acyclic and a level fits a block: wave[which].smem > 0 where
+   // precision `which` (0 FP64, 1 FP32) can run it. fac_wave[which]: the
+   // store reserved for that precision is in wave order (the wave kernel runs)
+   bool wave_ok = false;
+   int wave_threads = 256;
+   int64_t wave_levels = 0;
+   ubolt::WaveDev wave[2];
+   int64_t wave_bytes[2] = {0, 0};
+   bool fac_wave[2] = {false, false};
+   int kernel_mode = UBOLT_SWEEP_AUTO;
+   int64_t unmet_level = -1;  // ubolt_sweep_test_wait: one level's copy is never issued
    ~ubolt_sweep_plan()
    {
       for (void *f : fac)
@@ -241,53 +254,6 @@ __device__ __forceinline__ void SubCoupling(const T *__restrict__ Gf, const T xn
       for (int j = 0; j < NB; j++) u += gv[ii * NB + j] * xn[j];
       y[ii] -= u;
    }
-}
-
-// The factors of one (cell, ordinate) for the sweep: W = B^{-1} of its
-// streaming + removal block, and G_s = W (s_f face_up_f) for each gathered
-// face f in face order (slot s); element (s, ii, j) goes to Gout[s * gs + (ii * NB + j) * ge].
-// A singular block gives zero factors. Returns false then.
-template <typename T, int NB, int F>
-__device__ __forceinline__ bool CellFactors(const DevGeom<T> &g, int64_t c, const T om[3], uint32_t mask, T W[NB][NB],
-                                            T *Gout, size_t gs, size_t ge)
-{
-   const int32_t cl = g.cls[c];
-   T B[NB][NB];
-   BuildBlock<T, NB, F>(g, cl, om, g.sigma_t[c], B);
-   const bool ok = InvertBlock<T, NB>(B, W);
-   if (!ok)
-#pragma unroll
-      for (int ii = 0; ii < NB; ii++)
-#pragma unroll
-         for (int j = 0; j < NB; j++) W[ii][j] = T(0);
-   int slot = 0;
-#pragma unroll
-   for (int f = 0; f < F; f++) {
-      if (!(((mask >> f) | (mask >> (8 + f))) & 1u)) continue;
-      const T sf = Dot3(om, g.nA + ((int64_t)cl * F + f) * 3);
-      T *Gf = Gout + (size_t)slot * gs;
-      if constexpr (NB == 1) {
-         Gf[0] = W[0][0] * (sf * g.inv_vol[cl]);
-      } else {
-         const T *M = g.fup + ((int64_t)cl * F + f) * NB * NB;
-         T Ms[NB][NB];
-#pragma unroll
-         for (int kk = 0; kk < NB; kk++)
-#pragma unroll
-            for (int j = 0; j < NB; j++) Ms[kk][j] = sf * M[kk * NB + j];
-#pragma unroll
-         for (int ii = 0; ii < NB; ii++)
-#pragma unroll
-            for (int j = 0; j < NB; j++) {
-               T u = T(0);
-#pragma unroll
-               for (int kk = 0; kk < NB; kk++) u += W[ii][kk] * Ms[kk][j];
-               Gf[(size_t)(ii * NB + j) * ge] = u;
-            }
-      }
-      slot++;
-   }
-   return ok;
 }
 
 // The factor store: per task, element-major over its positions, so a warp's
@@ -549,6 +515,62 @@ __global__ void __launch_bounds__(128, SweepMinBlocks<T, NB, PL>()) SweepKernel(
 
 // ~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~
 
+static int ReserveFactors(ubolt_ctx *ctx, int64_t limit);
+
+// The wave plan and both precisions' store layouts (host work and uploads;
+// no store is reserved here). Leaves wave_ok false where the mesh has an
+// upwind cycle or a level or front too large for one block.
+static int BuildWavePlan(ubolt_ctx *ctx, ubolt_sweep_plan *plan)
+{
+   HostWavePlan h;
+   BuildHostWavePlan(ctx->n_cells, ctx->F, ctx->A, ctx->h_omega.data(), ctx->h_nA.data(), ctx->h_code.data(), h);
+   if (!h.acyclic || h.S > std::min(4, ctx->F - 1) || h.n_slots >= 0xffff || h.max_width > 512) return UBOLT_OK;
+   const int S = std::max(1, h.S);
+   int dev = 0, max_smem = 0;
+   cudaGetDevice(&dev);
+   if (cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) {
+      cudaGetLastError();
+      return UBOLT_OK;
+   }
+   const int A = ctx->A;
+   const int64_t total = h.lvl_base[A];
+   std::vector<int32_t> lvl_ord(total);
+   for (int a = 0; a < A; a++)
+      for (int32_t L = h.lvl_base[a]; L < h.lvl_base[a + 1]; L++) lvl_ord[L] = a;
+   int rc = 0;
+   ubolt::WaveDev base;
+   base.A = A;
+   base.S = S;
+   base.n_slots = h.n_slots;
+   base.max_levels = h.max_levels;
+   base.n_cells = ctx->n_cells;
+   const int32_t *meta = nullptr;
+   if ((rc = UploadVec(ctx, h.lvl_base, &base.lvl_base)) || (rc = UploadVec(ctx, h.lvl_pos, &base.lvl_pos)) ||
+       (rc = UploadVec(ctx, lvl_ord, &base.lvl_ord)) || (rc = UploadVec(ctx, h.meta, &meta)))
+      return rc;
+   base.meta = reinterpret_cast<const int4 *>(meta);
+   bool any = false;
+   for (int which = 0; which < 2; which++) {
+      WaveLayout L;
+      if (!BuildWaveLayout(h, ctx->nb, which ? 4 : 8, max_smem, L)) continue;
+      ubolt::WaveDev w = base;
+      if ((rc = UploadVec(ctx, L.region, &w.region)) || (rc = UploadVec(ctx, L.chunk_rel, &w.chunk_rel)) ||
+          (rc = UploadVec(ctx, L.ring_off, &w.ring_off)))
+         return rc;
+      w.front_off = L.front_off;
+      w.ring_base = L.ring_base;
+      w.cap = L.cap;
+      w.smem = L.smem;
+      plan->wave[which] = w;
+      plan->wave_bytes[which] = L.store_bytes;
+      any = true;
+   }
+   plan->wave_ok = any;
+   plan->wave_threads = h.max_width <= 256 ? 256 : 512;
+   plan->wave_levels = total;
+   return UBOLT_OK;
+}
+
 int BuildSweepPlan(ubolt_ctx *ctx, int patch_size)
 {
    const int64_t nc = ctx->n_cells;
@@ -612,10 +634,16 @@ int BuildSweepPlan(ubolt_ctx *ctx, int patch_size)
    plan->ctrl = static_cast<uint32_t *>(p);
    cudaMemset(plan->ctrl, 0, kCtrlWords * sizeof(uint32_t));
    cudaMemset(plan->ctrl + kCtrlNever, 0xff, 2 * sizeof(uint32_t));
-   if (ctx->sweep) plan->fac_limit = ctx->sweep->fac_limit;
+   if ((rc = BuildWavePlan(ctx, plan))) { delete plan; return rc; }
+   if (ctx->sweep) {
+      plan->fac_limit = ctx->sweep->fac_limit;
+      plan->kernel_mode = ctx->sweep->kernel_mode;
+   }
+   if (plan->kernel_mode == UBOLT_SWEEP_WAVE && !plan->wave_ok) plan->kernel_mode = UBOLT_SWEEP_AUTO;
    delete ctx->sweep;
    ctx->sweep = plan;
-   return CudaCheck(cudaDeviceSynchronize(), "sweep plan");
+   if ((rc = CudaCheck(cudaDeviceSynchronize(), "sweep plan"))) return rc;
+   return ReserveFactors(ctx, plan->fac_limit);
 }
 
 static SweepDev DevPlan(const ubolt_sweep_plan *pl)
@@ -648,31 +676,71 @@ static int64_t FactorBytes(const ubolt_ctx *ctx, const ubolt_sweep_plan *pl, siz
    return (int64_t)ctx->n_cells * ctx->A * ctx->nb * ctx->nb * (1 + pl->slots) * (int64_t)elem;
 }
 
-// The factor store for precision T, (re)built for the current group if it
-// fits the limit: by default half the free device memory (the solver's
-// workspace is allocated before its first sweep), at most 96 GiB. Returns
-// the store, or nullptr to compute factors in the sweep.
+// Reserve the factor stores - at set-up (plan build, or an explicit limit),
+// never inside a sweep. limit < 0: each store that fits, FP32 first, within
+// half the free device memory at that moment (at most 96 GiB); 0: none;
+// otherwise the byte limit for both together. A store not reserved means
+// the sweep computes its factors as it goes: the result is the same.
+// The automatic choice. The wave kernel runs one block per ordinate, and a
+// block's level costs about one L1 wavefront per scattered q and psi word:
+// on one B200 it beat the task kernel only on small problems (64^2 quads
+// DG0 S4: 0.078 against 0.110 ms) and lost from 128^2 triangles DG1 S8
+// (0.77 against 0.39 ms) up to 256^2 at S16 (3.78 against 3.71 ms). So it is
+// taken up to 2^17 cell-ordinates.
+static bool WavePreferred(const ubolt_ctx *ctx) { return ctx->n_cells * (int64_t)ctx->A <= ((int64_t)1 << 17); }
+
+static int ReserveFactors(ubolt_ctx *ctx, int64_t limit)
+{
+   ubolt_sweep_plan *pl = ctx->sweep;
+   if (pl->fac[0] || pl->fac[1]) cudaDeviceSynchronize();
+   for (int which = 0; which < 2; which++) {
+      if (pl->fac[which]) cudaFree(pl->fac[which]);
+      pl->fac[which] = nullptr;
+      pl->fac_epoch[which] = 0;
+   }
+   if (limit < 0) {
+      size_t free_b = 0, total_b = 0;
+      if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+         cudaGetLastError();
+         return UBOLT_OK;
+      }
+      limit = std::min<int64_t>((int64_t)(free_b / 2), (int64_t)96 << 30);
+   }
+   int64_t left = limit;
+   for (int which : {1, 0}) {
+      // The wave kernel where it applies and is chosen (its store is in wave
+      // order), else the task kernel's
+      const bool wave = pl->wave[which].smem > 0 &&
+                        (pl->kernel_mode == UBOLT_SWEEP_WAVE || (pl->kernel_mode == UBOLT_SWEEP_AUTO && WavePreferred(ctx)));
+      pl->fac_wave[which] = false;
+      const int64_t bytes = wave ? pl->wave_bytes[which] : FactorBytes(ctx, pl, which ? 4 : 8);
+      if (bytes > left) continue;
+      void *p = nullptr;
+      if (cudaMalloc(&p, (size_t)bytes) != cudaSuccess) {
+         cudaGetLastError();
+         continue;
+      }
+      pl->fac[which] = p;
+      pl->fac_wave[which] = wave;
+      left -= bytes;
+   }
+   return UBOLT_OK;
+}
+
+// The factor store for precision T, rebuilt by a kernel (no allocation) for
+// the current group: ubolt_set_group starts a new one. nullptr where none
+// is reserved: the sweep then computes its factors as it goes.
 template <typename T, int NB, int F>
 static T *EnsureFactors(ubolt_ctx *ctx, cudaStream_t st)
 {
    ubolt_sweep_plan *pl = ctx->sweep;
    const int which = sizeof(T) == 8 ? 0 : 1;
-   if (pl->fac[which] && pl->fac_epoch[which] == ctx->group_epoch) return static_cast<T *>(pl->fac[which]);
-   const int64_t bytes = FactorBytes(ctx, pl, sizeof(T));
-   if (!pl->fac[which]) {
-      int64_t limit = pl->fac_limit;
-      if (limit < 0) {
-         size_t free_b = 0, total_b = 0;
-         if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return nullptr;
-         limit = std::min<int64_t>((int64_t)(free_b / 2), (int64_t)96 << 30);
-      }
-      if (bytes > limit) return nullptr;
-      void *p = nullptr;
-      if (cudaMalloc(&p, (size_t)bytes) != cudaSuccess) {
-         cudaGetLastError();
-         return nullptr;
-      }
-      pl->fac[which] = p;
+   if (!pl->fac[which]) return nullptr;
+   if (pl->fac_epoch[which] == ctx->group_epoch) return static_cast<T *>(pl->fac[which]);
+   if (pl->fac_wave[which]) {
+      if (WaveFactors(ctx, pl->wave[which], pl->fac[which], (int)sizeof(T), st, pl->wave_levels)) return nullptr;
+      pl->fac_epoch[which] = ctx->group_epoch;
+      return static_cast<T *>(pl->fac[which]);
    }
    int n_sm = 0, dev = 0;
    cudaGetDevice(&dev);
@@ -688,7 +756,28 @@ template <typename T, int NB, int F>
 static int LaunchSweep(ubolt_ctx *ctx, const T *q, T *psi, cudaStream_t st, const SweepDev *affine = nullptr)
 {
    ubolt_sweep_plan *pl = ctx->sweep;
+   const int which = sizeof(T) == 8 ? 0 : 1;
    const T *fac = EnsureFactors<T, NB, F>(ctx, st);
+   if (pl->fac_wave[which]) {
+      // One block per ordinate over the store in wave order (no sentinel fill)
+      if (!fac) return UBOLT_ERR_CUDA;  // the failed launch set the message
+      WaveDev w = pl->wave[which];
+      w.ctrl = pl->ctrl;
+      w.spin_limit = pl->spin_limit;
+      w.unmet_level = pl->unmet_level;
+      pl->unmet_level = -1;
+      pl->unmet_task = -1;
+      pl->grid = ctx->A;
+      WaveInput in;
+      if (affine) {
+         in.alpha = affine->aff_alpha;
+         in.phi = affine->aff_phi;
+         in.rho = affine->aff_rho;
+         in.u = affine->aff_u;
+         in.iso = affine->aff_iso;
+      }
+      return WaveSweep(ctx, w, q, psi, fac, (int)sizeof(T), affine ? &in : nullptr, pl->wave_threads, st);
+   }
    const int threads = 32 * pl->warps_per_block;
    const size_t smem = (size_t)pl->warps_per_block * SweepSlice(pl->P, pl->slots, NB, (int)sizeof(T)).bytes;
    auto kern = fac ? (pl->P <= 32 ? SweepKernel<T, NB, F, 1, true>
@@ -788,6 +877,22 @@ extern "C" int ubolt_sweep_setup(ubolt_ctx *ctx, int patch_size)
    return BuildSweepPlan(ctx, patch_size);
 }
 
+extern "C" int ubolt_sweep_set_kernel(ubolt_ctx *ctx, int kernel)
+{
+   int rc = CheckReady(ctx, false);
+   if (rc) return rc;
+   if (kernel < UBOLT_SWEEP_AUTO || kernel > UBOLT_SWEEP_WAVE) return SetError(UBOLT_ERR_ARG, "sweep kernel %d", kernel);
+   if (!ctx->sweep && (rc = BuildSweepPlan(ctx, 0))) return rc;
+   ubolt_sweep_plan *pl = ctx->sweep;
+   if (kernel == UBOLT_SWEEP_WAVE && !pl->wave_ok)
+      return SetError(UBOLT_ERR_STATE, "the wave sweep does not apply here (an upwind cycle, or a level or front too "
+                                       "large for one block)");
+   if (kernel == pl->kernel_mode) return UBOLT_OK;
+   pl->kernel_mode = kernel;
+   // The stores' layout follows the kernel: reserved again, rebuilt by the next sweep
+   return ReserveFactors(ctx, pl->fac_limit);
+}
+
 extern "C" int ubolt_sweep(ubolt_ctx *ctx, const double *q, double *psi, void *stream)
 {
    return Sweep<double>(ctx, q, psi, stream);
@@ -802,16 +907,11 @@ extern "C" int ubolt_sweep_set_factor_limit(ubolt_ctx *ctx, int64_t bytes)
 {
    int rc = CheckReady(ctx, false);
    if (rc) return rc;
-   if (!ctx->sweep && (rc = BuildSweepPlan(ctx, 0))) return rc;
-   ubolt_sweep_plan *pl = ctx->sweep;
-   pl->fac_limit = bytes;
-   for (int which = 0; which < 2; which++)
-      if (pl->fac[which] && bytes >= 0 && FactorBytes(ctx, pl, which ? 4 : 8) > bytes) {
-         cudaDeviceSynchronize();
-         cudaFree(pl->fac[which]);
-         pl->fac[which] = nullptr;
-      }
-   return UBOLT_OK;
+   if (!ctx->sweep) {
+      if ((rc = BuildSweepPlan(ctx, 0))) return rc;
+   }
+   ctx->sweep->fac_limit = bytes;
+   return ReserveFactors(ctx, bytes);
 }
 
 extern "C" int ubolt_sweep_status(ubolt_ctx *ctx, ubolt_sweep_info *info, void *stream)
@@ -834,7 +934,11 @@ extern "C" int ubolt_sweep_status(ubolt_ctx *ctx, ubolt_sweep_info *info, void *
       info->total_levels = pl->total_levels;
       info->grid = pl->grid;
       info->timeouts = h[1];
-      info->factor_bytes = (pl->fac[0] ? FactorBytes(ctx, pl, 8) : 0) + (pl->fac[1] ? FactorBytes(ctx, pl, 4) : 0);
+      info->kernel = (pl->fac[0] && pl->fac_wave[0]) ? UBOLT_SWEEP_WAVE : UBOLT_SWEEP_TASKS;
+      info->factor_bytes = 0;
+      for (int which = 0; which < 2; which++)
+         if (pl->fac[which])
+            info->factor_bytes += pl->fac_wave[which] ? pl->wave_bytes[which] : FactorBytes(ctx, pl, which ? 4 : 8);
    }
    if (h[0]) {
       cudaMemsetAsync(pl->ctrl + kCtrlError, 0, 2 * sizeof(uint32_t), s);
@@ -853,12 +957,20 @@ extern "C" int ubolt_sweep_test_wait(ubolt_ctx *ctx, uint32_t spin_limit, int ma
    if (spin_limit < 16) return SetError(UBOLT_ERR_ARG, "spin limit %u too small", spin_limit);
    pl->spin_limit = spin_limit;
    pl->unmet_task = -1;
+   pl->unmet_level = -1;
+   if (make_one_wait_unmet && pl->fac[0] && pl->fac_wave[0]) {
+      // The wave kernel runs the next FP64 sweep: ordinate 0's first level
+      // waits for a copy never issued
+      pl->unmet_level = 0;
+      return UBOLT_OK;
+   }
    if (make_one_wait_unmet) {
       // The first task that has an upstream task polls, for its first
-      // upwind value, a word nothing writes
-      // task of this sweep publishes
+      // upwind value, a word that no task of the sweep stores
       std::vector<int32_t> dp(pl->n_tasks + 1);
-      cudaMemcpy(dp.data(), pl->dep_ptr, dp.size() * sizeof(int32_t), cudaMemcpyDeviceToHost);
+      if ((rc = CudaCheck(cudaMemcpy(dp.data(), pl->dep_ptr, dp.size() * sizeof(int32_t), cudaMemcpyDeviceToHost),
+                          "sweep_test_wait")))
+         return rc;
       for (int64_t t = 0; t < pl->n_tasks; t++)
          if (dp[t + 1] > dp[t]) { pl->unmet_task = t; break; }
       if (pl->unmet_task < 0) return SetError(UBOLT_ERR_STATE, "no task of this plan waits on another");

@@ -189,6 +189,12 @@ class Sweep:
         """Cache each cell-ordinate's B^{-1} and couplings (-1 automatic, 0 never, else a byte limit)."""
         check(lib.ubolt_sweep_set_factor_limit(self.ctx.handle, int(nbytes)))
 
+    KERNELS = {"auto": _lib.SWEEP_AUTO, "tasks": _lib.SWEEP_TASKS, "wave": _lib.SWEEP_WAVE}
+
+    def set_kernel(self, kind):
+        """"tasks" (any mesh), "wave" (one block per ordinate; acyclic meshes) or "auto"."""
+        check(lib.ubolt_sweep_set_kernel(self.ctx.handle, self.KERNELS[kind]))
+
     def apply(self, q, psi=None, stream=None):
         psi = torch.empty_like(q) if psi is None else psi
         fn = lib.ubolt_sweep if q.dtype == torch.float64 else lib.ubolt_sweep_f32
