@@ -55,7 +55,8 @@ def _args():
     p.add_argument("--workload", default="tri256", choices=["tri256", "hex128", "tet44"],
                    help="tri256 is the headline line; hex128 (4 groups) and tet44 time the other solve configs")
     p.add_argument("--restart", type=int, default=0, help="GMRES restart (0: 30, or 10 for hex128)")
-    p.add_argument("--profile", default="", choices=["", "apply", "apply32", "sweep", "sweep32", "adjoint"],
+    p.add_argument("--profile", default="",
+                   choices=["", "apply", "apply32", "sweep", "sweep32", "wave", "wave32", "adjoint", "dsa_spmv"],
                    help="run only this kernel, --warmup + --steps launches on the workload, for a profiler")
     return p.parse_args()
 
@@ -229,9 +230,16 @@ def profile_kernel(args, ctx, T, stream):
     xr = torch.rand(ctx.n_rows, dtype=torch.float64, device="cuda", generator=g).to(dt)
     yr = torch.empty_like(xr)
     kind = args.profile.rstrip("32")
-    if kind == "sweep":
+    if kind in ("sweep", "wave"):
         sw = T.Sweep(ctx, 0)
+        sw.set_kernel("tasks" if kind == "sweep" else "wave")
         fn = lambda: sw.apply(xr, yr)
+    elif kind == "dsa_spmv":
+        dsa = T.DSAPrecon(ctx)
+        dsa.set_group()
+        u = dsa.restrict(xr)
+        v = torch.empty_like(u)
+        fn = lambda: dsa.spmv(u, v)
     else:
         A = T.TransportOperator(ctx)
         fn = (lambda: A.mult(xr, yr)) if kind == "apply" else (lambda: A.mult_transpose(xr, yr))

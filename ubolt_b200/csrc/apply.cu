@@ -103,6 +103,20 @@ __device__ __forceinline__ void LoadShared(const T *p, T v[N])
    }
 }
 
+// One run of CU bytes (4, 8, 16 or a multiple of 16), both addresses aligned
+// to min(CU, 16)
+template <int CU>
+__device__ __forceinline__ void CpAsyncRun(void *dst, const void *src)
+{
+   if constexpr (CU <= 16) {
+      CpAsync<CU>(dst, src);
+   } else {
+#pragma unroll
+      for (int u = 0; u < CU / 16; u++)
+         CpAsync<16>(static_cast<unsigned char *>(dst) + 16 * u, static_cast<const unsigned char *>(src) + 16 * u);
+   }
+}
+
 // Upwind runs staged per thread: every face at once where F * NB <= 12,
 // else a ring of two faces fetched ahead of the walk over the faces (DG1
 // tets and hexes, whose F * NB runs would crowd the SM's shared memory)
@@ -161,7 +175,7 @@ __global__ void __launch_bounds__(256, ApplyMinBlocks<T, NB, AP>()) ApplyKernel(
    {
       const int nu = kc * NB * A * (int)sizeof(T) / CU;
       const unsigned char *src = reinterpret_cast<const unsigned char *>(x + c0 * NB * A);
-      for (int u = t; u < nu; u += blockDim.x) CpAsync<CU>(reinterpret_cast<unsigned char *>(xs) + u * CU, src + u * CU);
+      for (int u = t; u < nu; u += blockDim.x) CpAsyncRun<CU>(reinterpret_cast<unsigned char *>(xs) + u * CU, src + u * CU);
    }
    if (live) {
       const T *rec = g.rec + (int64_t)g.cls[c] * L.size;
@@ -175,7 +189,7 @@ __global__ void __launch_bounds__(256, ApplyMinBlocks<T, NB, AP>()) ApplyKernel(
             if (!kRing || f < XS) {
 #pragma unroll
                for (int j = 0; j < NB; j++)
-                  CpAsync<CU>(xup + ((f * NB + j) * (int)blockDim.x + t) * AP, x + ((int64_t)cf * NB + j) * A + a0);
+                  CpAsyncRun<CU>(xup + ((f * NB + j) * (int)blockDim.x + t) * AP, x + ((int64_t)cf * NB + j) * A + a0);
             }
          } else {
             fcode |= (unsigned)FaceSide(cf) << (4 * f);
@@ -325,7 +339,7 @@ __global__ void __launch_bounds__(256, ApplyMinBlocks<T, NB, AP>()) ApplyKernel(
                if (FaceInterior(cf)) {
 #pragma unroll
                   for (int j = 0; j < NB; j++)
-                     CpAsync<CU>(xup + ((slot * NB + j) * (int)blockDim.x + t) * AP, x + ((int64_t)cf * NB + j) * A + a0);
+                     CpAsyncRun<CU>(xup + ((slot * NB + j) * (int)blockDim.x + t) * AP, x + ((int64_t)cf * NB + j) * A + a0);
                }
             }
             CpAsyncCommit();
