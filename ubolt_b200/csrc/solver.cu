@@ -889,6 +889,7 @@ static int SolveSystem(ubolt_ctx *ctx, bool adjoint, const double *b, double *x,
    ubolt_solve_stats st{};
    st.krylov = iso ? UBOLT_KRYLOV_COMPRESSED : UBOLT_KRYLOV_FULL;
    bool converged = false;
+   bool r_of_x = false;  // ws->r holds b - A x of the x to be returned, st.residual its norm
    if (bnorm == 0.0) {
       cudaMemsetAsync(x, 0, n * sizeof(double), s);
       converged = true;
@@ -904,27 +905,32 @@ static int SolveSystem(ubolt_ctx *ctx, bool adjoint, const double *b, double *x,
       st.outer = 1;
       converged = res.converged;
    } else {
-      // Iterative refinement: r = b - A x in FP64, A d = r in FP32, x += d
+      // Iterative refinement: r = b - A x in FP64, A d = r in FP32, x += d.
+      // From x = 0 the first residual is b itself, its norm already known
       bool x_zero = o.x_zero != 0;
       for (int outer = 0; outer < o.max_outer; outer++) {
+         const double *resid = ws->r;
+         double rnorm = bnorm;
          if (x_zero) {
-            if ((rc = DeviceCopy<double>(ws->r, b, n, s, "refinement"))) return rc;
+            resid = b;
          } else {
             if ((rc = OperatorApply<double>(ctx, adjoint, x, ws->r, stream))) return rc;
             ResidualKernel<double><<<grid, 256, 0, s>>>(b, ws->r, n);
             CountLaunch();
+            rnorm = Norm<double>(ws, ws->r, n, s, &rc);
+            if (rc) return rc;
+            r_of_x = true;
          }
-         const double rnorm = Norm<double>(ws, ws->r, n, s, &rc);
-         if (rc) return rc;
          if (!std::isfinite(rnorm)) return SetError(UBOLT_ERR_NONFINITE, "refinement residual is not finite");
          st.residual = rnorm / bnorm;
          if (rnorm <= o.rtol * bnorm) {
             converged = true;
             break;
          }
+         r_of_x = false;
          st.outer = outer + 1;
          // The correction equation, scaled to unit norm so FP32 has the range
-         ScaleKernel<double, float><<<grid, 256, 0, s>>>(ws->r, ws->b32, 1.0 / rnorm, n);
+         ScaleKernel<double, float><<<grid, 256, 0, s>>>(resid, ws->b32, 1.0 / rnorm, n);
          CountLaunch();
          cudaMemsetAsync(ws->d32, 0, n * sizeof(float), s);
          GmresResult res;
@@ -943,13 +949,16 @@ static int SolveSystem(ubolt_ctx *ctx, bool adjoint, const double *b, double *x,
          if (st.iterations >= o.max_it) break;
       }
    }
-   // The true residual of what is returned
-   if ((rc = OperatorApply<double>(ctx, adjoint, x, ws->r, stream))) return rc;
-   ResidualKernel<double><<<grid, 256, 0, s>>>(b, ws->r, n);
-   CountLaunch();
-   const double rn = Norm<double>(ws, ws->r, n, s, &rc);
-   if (rc) return rc;
-   st.residual = bnorm > 0 ? rn / bnorm : 0.0;
+   // The true residual of what is returned (the refinement's last residual
+   // where that was taken of the x returned)
+   if (!r_of_x) {
+      if ((rc = OperatorApply<double>(ctx, adjoint, x, ws->r, stream))) return rc;
+      ResidualKernel<double><<<grid, 256, 0, s>>>(b, ws->r, n);
+      CountLaunch();
+      const double rn = Norm<double>(ws, ws->r, n, s, &rc);
+      if (rc) return rc;
+      st.residual = bnorm > 0 ? rn / bnorm : 0.0;
+   }
    st.rnorm0 = bnorm;
    st.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
    if (ctx->sweep && (o.pc == UBOLT_PC_SWEEP || o.pc == UBOLT_PC_SWEEP_DSA)) {
