@@ -319,33 +319,71 @@ class DetectorResponse:
         return _Response.apply(sigma_t, sigma_s, self)
 
 
-def solve_groups(ctx, sigma_t, sigma_s, source, side_inflow=None, dsa=None, keep_psi=False, **solver_opts):
-    """The downscatter group sweep of the reference driver
-    (tests/transportk.kokkos.cxx:1036-1157, one forward pass - exact for
-    downscatter only, docs/architecture.md:362-364): per group g, point the
-    operator (and the DSA) at g's cross sections, build b = inflow + source
-    + sum_{g' < g} transfer(g' -> g) from the cached scalar fluxes, solve,
-    and cache phi_g.
-
-    sigma_t: (G, n_cells), sigma_s: (G, G, n_cells) [from, to], source:
-    (G, n_cells) - NumPy or device tensors. Returns (phi per group, stats per
-    group[, psi per group])."""
+def group_tables(ctx, sigma_t, sigma_s, source):
+    """The cross-section and source tables on the device, float64, contiguous:
+    (st[g], ss[g][h], src[g]). NumPy arrays are uploaded; device tensors are
+    used as they are (converted only if their dtype or layout differs)."""
     dev = ctx.device
-    as_dev = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float64, device=dev)
+
+    def as_dev(a):
+        if isinstance(a, torch.Tensor):
+            return a.to(device=dev, dtype=torch.float64).contiguous()
+        return torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float64, device=dev)
+
     G = len(sigma_t)
     st = [as_dev(sigma_t[g]) for g in range(G)]
     ss = [[as_dev(sigma_s[g][h]) for h in range(G)] for g in range(G)]
     src = [as_dev(source[g]) for g in range(G)]
-    for g in range(G):
-        for h in range(g):
-            if torch.count_nonzero(ss[g][h]).item():
-                raise _lib.UboltError(1, f"upscatter {g} -> {h}: the group sweep is downscatter only")
+    return st, ss, src
+
+
+def solve_groups(ctx, sigma_t, sigma_s, source, side_inflow=None, dsa=None, keep_psi=False, solver=None,
+                 outer_rtol=1e-8, outer_max_it=1000, outer_inner_gamma=0.01, outer_info=None, **solver_opts):
+    """The group loop of the reference driver (tests/transportk.kokkos.cxx:
+    1036-1208): per group g, point the operator (and the DSA) at g's cross
+    sections, build b = inflow + source + the transfer out of the other
+    groups' cached scalar fluxes, solve, and cache phi_g.
+
+    Downscatter only: one pass over the groups in order, exact
+    (docs/architecture.md:362-364).
+
+    With upscatter (some group scatters into a lower one), the reference's
+    outer iteration, angular store (one psi per group, -outer_store angular):
+    the first pass solves every group in order, a thermal group (from g_up,
+    the lowest group anything scatters up into) reading zero for the groups
+    not solved yet; each later pass re-solves the thermal block, every group
+    warm-started from its own last psi and taking every other group's
+    transfer. After a pass, change = ||phi_new - phi_old|| / ||phi_new||
+    over the thermal block, rho the ratio of successive changes, and the
+    error estimate change rho / (1 - rho); the iteration stops when that
+    estimate is below outer_rtol (or the change is exactly zero), on a pass
+    whose thermal solves ran at the solver's own rtol: the inner rtol of a
+    thermal pass is max(rtol, outer_inner_gamma min(change, 1)) until the
+    test first passes, then one more pass at rtol. outer_rtol below the
+    solver's rtol is refused (a warm start that moves by less than its rtol
+    takes no iterations, and the outer test would pass falsely).
+
+    sigma_t: (G, n_cells), sigma_s: (G, G, n_cells) [from, to], source:
+    (G, n_cells) - NumPy arrays, or device tensors (used in place, as from
+    group_tables). solver: a TransportSolver set up on ctx (else one is made
+    from solver_opts; its workspace allocation is then part of the call).
+    outer_info: a dict, filled with the outer iteration's record. Returns
+    (phi per group, stats of each group's last solve[, psi per group])."""
+    st, ss, src = group_tables(ctx, sigma_t, sigma_s, source)
+    G = len(st)
+    # Which transfers are nonzero, in one read-back for every pair
+    nonzero = [[False] * G for _ in range(G)]
+    if G > 1:
+        pairs = [(g, h) for g in range(G) for h in range(G) if g != h]
+        flags = torch.stack([torch.count_nonzero(ss[g][h]) for g, h in pairs]).tolist()
+        for (g, h), n in zip(pairs, flags):
+            nonzero[g][h] = n > 0
+    g_up = min([h for g in range(G) for h in range(g) if nonzero[g][h]], default=G)
     transfer = GroupTransfer(ctx, ss, src)
-    solver = TransportSolver(ctx, **solver_opts)
+    solver = TransportSolver(ctx, **solver_opts) if solver is None else solver
     b = ctx.vector()
-    psi = ctx.vector(fill=0.0)
-    phis, stats, psis = [], [], []
-    for g in range(G):
+
+    def rhs(g, from_all):
         ctx.set_group(st[g], ss[g][g])
         if dsa is not None:
             dsa.set_group()
@@ -353,16 +391,80 @@ def solve_groups(ctx, sigma_t, sigma_s, source, side_inflow=None, dsa=None, keep
         if side_inflow is not None:
             fill_inflow(ctx, side_inflow, b)
         transfer.add_external(g, b)
-        for h in range(g):
-            if torch.count_nonzero(ss[h][g]).item():
+        for h in range(G if from_all else g):
+            if h != g and nonzero[h][g]:
                 transfer.add_transfer(h, g, b)
-        psi, s = solver.solve(b, psi)
-        transfer.set_scalar_flux(g, psi)
-        transfer.phi[g] = transfer.phi[g].clone()
-        phis.append(transfer.phi[g])
-        stats.append(s)
-        if keep_psi:
-            psis.append(psi.clone())
+
+    if g_up == G:
+        psi = ctx.vector(fill=0.0)
+        phis, stats, psis = [], [], []
+        for g in range(G):
+            rhs(g, False)
+            psi, s = solver.solve(b, psi)
+            transfer.set_scalar_flux(g, psi)
+            transfer.phi[g] = transfer.phi[g].clone()
+            phis.append(transfer.phi[g])
+            stats.append(s)
+            if keep_psi:
+                psis.append(psi.clone())
+        if outer_info is not None:
+            outer_info.update(upscatter=False, outer_iterations=1, converged=True)
+        return (phis, stats, psis) if keep_psi else (phis, stats)
+
+    inner_rtol = solver.opts.rtol
+    if outer_rtol < inner_rtol:
+        raise _lib.UboltError(1, f"outer_rtol {outer_rtol:g} is below the solver's rtol {inner_rtol:g}: a warm start "
+                                 "that moves by less than its rtol takes no iterations and the outer test would pass "
+                                 "falsely")
+    psis = [ctx.vector(fill=0.0) for _ in range(G)]
+    for g in range(g_up, G):
+        transfer.phi[g] = torch.zeros(ctx.n_nodes, dtype=torch.float64, device=ctx.device)
+    new_phi = torch.empty(ctx.n_nodes, dtype=torch.float64, device=ctx.device)
+    stats = [None] * G
+    outer_change, final_sweep, converged = 0.0, False, False
+    changes, inner_its = [], 0
+    err = float("inf")
+    try:
+        for outer in range(outer_max_it):
+            sweep_rtol = inner_rtol
+            if outer_inner_gamma > 0.0 and not final_sweep:
+                sweep_rtol = max(inner_rtol, outer_inner_gamma * (1.0 if outer == 0 else min(outer_change, 1.0)))
+            sums = torch.zeros(2, dtype=torch.float64, device=ctx.device)
+            for g in range(0 if outer == 0 else g_up, G):
+                thermal = g >= g_up
+                rhs(g, thermal)
+                solver.opts.rtol = sweep_rtol if thermal else inner_rtol
+                psis[g], s = solver.solve(b, psis[g], x_zero=(outer == 0))
+                stats[g] = s
+                inner_its += s["iterations"]
+                if thermal:
+                    angular_integral(ctx, psis[g], new_phi)
+                    sums[0] += torch.sum((new_phi - transfer.phi[g]) ** 2)
+                    sums[1] += torch.sum(new_phi * new_phi)
+                    transfer.phi[g].copy_(new_phi)
+                else:
+                    transfer.set_scalar_flux(g, psis[g])
+            change_sq, norm_sq = sums.tolist()
+            change = (change_sq / norm_sq) ** 0.5 if norm_sq > 0.0 else change_sq ** 0.5
+            have_rho = outer >= 2 and outer_change > 0.0
+            rho = change / outer_change if have_rho else 0.0
+            outer_change = change
+            err = change * rho / (1.0 - rho) if have_rho and rho < 1.0 else float("inf")
+            changes.append(change)
+            if change == 0.0 or err < outer_rtol:
+                if sweep_rtol == inner_rtol:
+                    converged = True
+                    break
+                final_sweep = True
+    finally:
+        solver.opts.rtol = inner_rtol
+    if outer_info is not None:
+        outer_info.update(upscatter=True, g_up=g_up, outer_iterations=len(changes), changes=changes,
+                          error_estimate=err, inner_iterations=inner_its, converged=converged)
+    if not converged:
+        raise _lib.UboltError(5, f"outer iteration not converged after {len(changes)} passes: error estimate "
+                                 f"{err:.3e}, outer_rtol {outer_rtol:g}")
+    phis = [transfer.phi[g].clone() for g in range(G)]
     return (phis, stats, psis) if keep_psi else (phis, stats)
 
 
