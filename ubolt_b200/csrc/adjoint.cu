@@ -12,46 +12,53 @@ namespace ubolt {
 
 // g(c, 0, a) += d(c) V_c w_a: the source whose inner product with psi is
 // J = sum_c d(c) V_c phi(c, basis 0) - the detector's volume-integrated flux
-__global__ void ResponseSourceKernel(const DevGeom<double> g, const double *__restrict__ volume,
-                                     const double *__restrict__ d, double *__restrict__ out)
+__global__ void __launch_bounds__(256) ResponseSourceKernel(const DevGeom<double> g, const double *__restrict__ volume,
+                                                            const double *__restrict__ d, double *__restrict__ out)
 {
-   const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-   if (tid >= g.n_cells * g.A) return;
-   const int64_t c = tid / g.A;
-   const int a = (int)(tid - c * g.A);
-   if (d[c] != 0.0) out[c * g.nb * g.A + a] += d[c] * volume[c] * g.w[a];
+   const int lane = threadIdx.x & 31, sub = lane & (kLpn - 1);
+   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+   const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+   for (int64_t c0 = warp * 4; c0 < g.n_cells; c0 += n_warps * 4) {
+      const int64_t c = c0 + (lane >> 3);
+      if (c >= g.n_cells || d[c] == 0.0) continue;
+      const double v = d[c] * volume[c];
+      double *run = out + c * g.nb * g.A;
+      for (int a = sub; a < g.A; a += kLpn) run[a] += v * g.w[a];
+   }
 }
 
-// One warp per cell
-__global__ void GradientKernel(const DevGeom<double> g, const double *__restrict__ psi,
-                               const double *__restrict__ lam, double *__restrict__ gt, double *__restrict__ gs)
+// A cell-run kernel: 8 lanes per cell (its nb node runs one after another),
+// four cells per warp, as the node-run kernels
+__global__ void __launch_bounds__(256) GradientKernel(const DevGeom<double> g, const double *__restrict__ psi,
+                                                      const double *__restrict__ lam, double *__restrict__ gt,
+                                                      double *__restrict__ gs)
 {
-   const int64_t c = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-   const int lane = threadIdx.x & 31;
-   if (c >= g.n_cells) return;
+   const int lane = threadIdx.x & 31, sub = lane & (kLpn - 1);
+   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+   const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
    const int A = g.A;
-   double rt = 0.0, rs = 0.0;
-   for (int i = 0; i < g.nb; i++) {
-      const int64_t base = (c * g.nb + i) * A;
-      double l_sum = 0.0, phi = 0.0;
-      for (int a = lane; a < A; a += 32) {
-         const double l = lam[base + a], p = psi[base + a];
-         rt += l * p;
-         l_sum += l;
-         phi += g.w[a] * p;
+   for (int64_t c0 = warp * 4; c0 < g.n_cells; c0 += n_warps * 4) {
+      const int64_t c = c0 + (lane >> 3);
+      const bool live = c < g.n_cells;
+      double rt = 0.0, rs = 0.0;
+      for (int i = 0; i < g.nb; i++) {
+         double l_sum = 0.0, phi = 0.0;
+         if (live) {
+            const int64_t base = (c * g.nb + i) * A;
+            for (int a = sub; a < A; a += kLpn) {
+               const double l = lam[base + a], p = psi[base + a];
+               rt += l * p;
+               l_sum += l;
+               phi += g.w[a] * p;
+            }
+         }
+         rs += GroupSum(l_sum) * GroupSum(phi);
       }
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-         l_sum += __shfl_xor_sync(0xffffffffu, l_sum, o);
-         phi += __shfl_xor_sync(0xffffffffu, phi, o);
+      rt = GroupSum(rt);
+      if (live && sub == 0) {
+         if (gt) gt[c] = -rt;
+         if (gs) gs[c] = rs * g.inv_sum_weights;
       }
-      rs += l_sum * phi;
-   }
-#pragma unroll
-   for (int o = 16; o > 0; o >>= 1) rt += __shfl_xor_sync(0xffffffffu, rt, o);
-   if (lane == 0) {
-      if (gt) gt[c] = -rt;
-      if (gs) gs[c] = rs * g.inv_sum_weights;
    }
 }
 
@@ -64,8 +71,8 @@ extern "C" int ubolt_add_response_source(ubolt_ctx *ctx, const double *detector,
    int rc = CheckReady(ctx, false);
    if (rc) return rc;
    if (!detector || !g) return SetError(UBOLT_ERR_ARG, "add_response_source: NULL array");
-   const int64_t n = ctx->n_cells * ctx->A;
-   ResponseSourceKernel<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(ctx->g64, ctx->d_volume, detector, g);
+   ResponseSourceKernel<<<RunGrid(ctx->n_cells), 256, 0, (cudaStream_t)stream>>>(ctx->g64, ctx->d_volume, detector,
+                                                                                 g);
    return CheckLaunch("add_response_source");
 }
 
@@ -75,8 +82,7 @@ extern "C" int ubolt_gradient(ubolt_ctx *ctx, const double *psi, const double *l
    int rc = CheckReady(ctx, false);
    if (rc) return rc;
    if (!psi || !lambda || (!grad_sigma_t && !grad_sigma_s)) return SetError(UBOLT_ERR_ARG, "gradient: NULL array");
-   const int64_t threads = ctx->n_cells * 32;
-   GradientKernel<<<(threads + 255) / 256, 256, 0, (cudaStream_t)stream>>>(ctx->g64, psi, lambda, grad_sigma_t,
+   GradientKernel<<<RunGrid(ctx->n_cells), 256, 0, (cudaStream_t)stream>>>(ctx->g64, psi, lambda, grad_sigma_t,
                                                                             grad_sigma_s);
    return CheckLaunch("gradient");
 }

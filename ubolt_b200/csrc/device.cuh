@@ -363,4 +363,26 @@ __device__ __forceinline__ bool CellFactors(const DevGeom<T> &g, int64_t c, cons
    return ok;
 }
 
+// Node-run kernels. A node's A ordinates are one contiguous run of psi. A
+// warp takes kLpn = 8 lanes per node, four nodes at a time; lane `sub` of a
+// node strides its run by 8, so every load or store of the warp covers four
+// runs of 8 consecutive values (whole sectors), and a node's eight partial
+// sums meet in 3 shuffle steps. All lanes of a warp run the same iterations.
+constexpr int kLpn = 8;
+
+__device__ __forceinline__ double GroupSum(double v)
+{
+   v += __shfl_xor_sync(0xffffffffu, v, 4);
+   v += __shfl_xor_sync(0xffffffffu, v, 2);
+   v += __shfl_xor_sync(0xffffffffu, v, 1);
+   return v;
+}
+
+// Blocks of 256 threads for a grid-stride loop over groups of four runs
+__host__ inline int RunGrid(int64_t n_runs)
+{
+   const int64_t want = (n_runs + 31) / 32;
+   return (int)(want < 1 ? 1 : (want > 148 * 16 ? 148 * 16 : want));
+}
+
 }  // namespace ubolt

@@ -133,37 +133,48 @@ __global__ void DsaSpmvKernel(int64_t n_nodes, int nb, int F, const int32_t *__r
    if (scal) GridSum(d, scal + kDsaScalars, GridCount(scal), &scal[2]);
 }
 
-// rhs(node) = V_c sum_a w_a (x(node, a) - ax(node, a)); ax may be NULL. Warp per node.
-// A masked void's nodes restrict to zero (mask may be NULL: none).
+// rhs(node) = V_c sum_a w_a (x(node, a) - ax(node, a)); ax may be NULL. A
+// node-run kernel. A masked void's nodes restrict to zero (mask may be NULL: none).
 template <typename T>
-__global__ void DsaRestrictKernel(int64_t n_nodes, int nb, int A, const double *__restrict__ w,
-                                  const double *__restrict__ volume, const T *__restrict__ x,
-                                  const T *__restrict__ ax, const uint8_t *__restrict__ mask,
-                                  double *__restrict__ rhs)
+__global__ void __launch_bounds__(256) DsaRestrictKernel(int64_t n_nodes, int nb, int A, const double *__restrict__ w,
+                                                         const double *__restrict__ volume, const T *__restrict__ x,
+                                                         const T *__restrict__ ax, const uint8_t *__restrict__ mask,
+                                                         double *__restrict__ rhs)
 {
-   const int64_t node = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-   const int lane = threadIdx.x & 31;
-   if (node >= n_nodes) return;
-   double s = 0.0;
-   for (int a = lane; a < A; a += 32) {
-      double v = (double)x[node * A + a];
-      if (ax) v -= (double)ax[node * A + a];
-      s += w[a] * v;
+   const int lane = threadIdx.x & 31, sub = lane & (kLpn - 1);
+   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+   const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+   for (int64_t n0 = warp * 4; n0 < n_nodes; n0 += n_warps * 4) {
+      const int64_t node = n0 + (lane >> 3);
+      const bool live = node < n_nodes;
+      double s = 0.0;
+      if (live)
+         for (int a = sub; a < A; a += kLpn) {
+            double v = (double)x[node * A + a];
+            if (ax) v -= (double)ax[node * A + a];
+            s += w[a] * v;
+         }
+      s = GroupSum(s);
+      if (live && sub == 0) rhs[node] = (mask && mask[node / nb]) ? 0.0 : s * volume[node / nb];
    }
-#pragma unroll
-   for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-   if (lane == 0) rhs[node] = (mask && mask[node / nb]) ? 0.0 : s * volume[node / nb];
 }
 
 // y(node, a) (+)= u(node) / W; a masked void's rows get zero (mask may be NULL)
 template <typename T>
-__global__ void DsaProlongKernel(int64_t n_rows, int nb, int A, double inv_w, const double *__restrict__ u,
-                                 const uint8_t *__restrict__ mask, T *__restrict__ y, int add)
+__global__ void __launch_bounds__(256) DsaProlongKernel(int64_t n_nodes, int nb, int A, double inv_w,
+                                                        const double *__restrict__ u, const uint8_t *__restrict__ mask,
+                                                        T *__restrict__ y, int add)
 {
-   const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-   if (r >= n_rows) return;
-   const double v = (mask && mask[r / ((int64_t)nb * A)]) ? 0.0 : u[r / A] * inv_w;
-   y[r] = add ? (T)((double)y[r] + v) : (T)v;
+   const int lane = threadIdx.x & 31, sub = lane & (kLpn - 1);
+   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+   const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+   for (int64_t n0 = warp * 4; n0 < n_nodes; n0 += n_warps * 4) {
+      const int64_t node = n0 + (lane >> 3);
+      if (node >= n_nodes) continue;
+      const double v = (mask && mask[node / nb]) ? 0.0 : u[node] * inv_w;
+      T *run = y + node * A;
+      for (int a = sub; a < A; a += kLpn) run[a] = add ? (T)((double)run[a] + v) : (T)v;
+   }
 }
 
 // ~~~ Block-Jacobi PCG on the device, a fixed number of iterations from u = 0
@@ -488,12 +499,11 @@ int DsaCorrect(ubolt_ctx *ctx, const T *r, T *y, T *tmp, void *stream)
    cudaStream_t s = (cudaStream_t)stream;
    ubolt_dsa *ds = ctx->dsa;
    if ((rc = OperatorApply<T>(ctx, false, y, tmp, stream))) return rc;
-   const int64_t threads = ds->n_nodes * 32;
-   DsaRestrictKernel<T><<<(threads + 255) / 256, 256, 0, s>>>(ds->n_nodes, ds->nb, ctx->A, ctx->geom<double>().w, ctx->d_volume,
+   DsaRestrictKernel<T><<<RunGrid(ds->n_nodes), 256, 0, s>>>(ds->n_nodes, ds->nb, ctx->A, ctx->geom<double>().w, ctx->d_volume,
                                                               r, tmp, ds->mask, ds->rhs);
    CountLaunch();
    if ((rc = DsaSolveOnDevice(ctx, s))) return rc;
-   DsaProlongKernel<T><<<(ctx->n_rows + 255) / 256, 256, 0, s>>>(ctx->n_rows, ds->nb, ctx->A, 1.0 / ctx->sum_weights,
+   DsaProlongKernel<T><<<RunGrid(ctx->n_nodes), 256, 0, s>>>(ctx->n_nodes, ds->nb, ctx->A, 1.0 / ctx->sum_weights,
                                                                   ds->u, ds->mask, y, 1);
    return CheckLaunch("dsa correct");
 }
@@ -666,8 +676,7 @@ extern "C" int ubolt_dsa_restrict(ubolt_ctx *ctx, const double *x, double *rhs, 
    int rc = CheckReady(ctx, false);
    if (rc) return rc;
    if (!x || !rhs) return SetError(UBOLT_ERR_ARG, "dsa_restrict: NULL array");
-   const int64_t threads = ctx->n_nodes * 32;
-   DsaRestrictKernel<double><<<(threads + 255) / 256, 256, 0, (cudaStream_t)stream>>>(
+   DsaRestrictKernel<double><<<RunGrid(ctx->n_nodes), 256, 0, (cudaStream_t)stream>>>(
       ctx->n_nodes, ctx->nb, ctx->A, ctx->geom<double>().w, ctx->d_volume, x, nullptr, DsaMask(ctx), rhs);
    return CheckLaunch("dsa_restrict");
 }
@@ -677,8 +686,8 @@ extern "C" int ubolt_dsa_prolong(ubolt_ctx *ctx, const double *u, double *y, voi
    int rc = CheckReady(ctx, false);
    if (rc) return rc;
    if (!u || !y) return SetError(UBOLT_ERR_ARG, "dsa_prolong: NULL array");
-   DsaProlongKernel<double><<<(ctx->n_rows + 255) / 256, 256, 0, (cudaStream_t)stream>>>(
-      ctx->n_rows, ctx->nb, ctx->A, 1.0 / ctx->sum_weights, u, DsaMask(ctx), y, 0);
+   DsaProlongKernel<double><<<RunGrid(ctx->n_nodes), 256, 0, (cudaStream_t)stream>>>(
+      ctx->n_nodes, ctx->nb, ctx->A, 1.0 / ctx->sum_weights, u, DsaMask(ctx), y, 0);
    return CheckLaunch("dsa_prolong");
 }
 
@@ -689,12 +698,11 @@ extern "C" int ubolt_dsa_apply(ubolt_ctx *ctx, const double *x, double *y, void 
    if (!x || !y || x == y) return SetError(UBOLT_ERR_ARG, "dsa_apply: x and y must be distinct device arrays");
    cudaStream_t s = (cudaStream_t)stream;
    ubolt_dsa *ds = ctx->dsa;
-   const int64_t threads = ds->n_nodes * 32;
-   DsaRestrictKernel<double><<<(threads + 255) / 256, 256, 0, s>>>(ds->n_nodes, ds->nb, ctx->A, ctx->geom<double>().w,
+   DsaRestrictKernel<double><<<RunGrid(ds->n_nodes), 256, 0, s>>>(ds->n_nodes, ds->nb, ctx->A, ctx->geom<double>().w,
                                                                    ctx->d_volume, x, nullptr, ds->mask, ds->rhs);
    CountLaunch();
    if ((rc = DsaSolveOnDevice(ctx, s))) return rc;
-   DsaProlongKernel<double><<<(ctx->n_rows + 255) / 256, 256, 0, s>>>(ctx->n_rows, ds->nb, ctx->A,
+   DsaProlongKernel<double><<<RunGrid(ctx->n_nodes), 256, 0, s>>>(ctx->n_nodes, ds->nb, ctx->A,
                                                                       1.0 / ctx->sum_weights, ds->u, ds->mask, y, 0);
    return CheckLaunch("dsa_apply");
 }
@@ -766,8 +774,7 @@ extern "C" int ubolt_dsa_apply_static(ubolt_ctx *ctx, const double *x, double *y
    double *rhs = base, *u = base + nn, *r = base + 2 * nn, *z = base + 3 * nn, *p = base + 4 * nn, *q = base + 5 * nn;
    double *scal = base + 6 * nn;
    cudaStream_t s = (cudaStream_t)stream;
-   const int64_t threads = ds->n_nodes * 32;
-   DsaRestrictKernel<double><<<(threads + 255) / 256, 256, 0, s>>>(ds->n_nodes, ds->nb, ctx->A, ctx->geom<double>().w,
+   DsaRestrictKernel<double><<<RunGrid(ds->n_nodes), 256, 0, s>>>(ds->n_nodes, ds->nb, ctx->A, ctx->geom<double>().w,
                                                                    ctx->d_volume, x, nullptr, ds->mask, rhs);
    CountLaunch();
    // The same fixed-count block-Jacobi PCG as the workspace path; the
@@ -785,7 +792,7 @@ extern "C" int ubolt_dsa_apply_static(ubolt_ctx *ctx, const double *x, double *y
       CgRotateScalars<<<1, 1, 0, s>>>(scal);
       CountLaunch(5);
    }
-   DsaProlongKernel<double><<<(ctx->n_rows + 255) / 256, 256, 0, s>>>(ctx->n_rows, ds->nb, ctx->A,
+   DsaProlongKernel<double><<<RunGrid(ctx->n_nodes), 256, 0, s>>>(ctx->n_nodes, ds->nb, ctx->A,
                                                                       1.0 / ctx->sum_weights, u, ds->mask, y, 0);
    return CheckLaunch("dsa_apply_static");
 }

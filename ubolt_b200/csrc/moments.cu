@@ -3,41 +3,61 @@
 
 namespace ubolt {
 
-// phi(node) = sum_a w_a psi(node, a): one warp per node, the node's angles
-// are one contiguous run (UboltAngularIntegral's gemm, sn_quadraturek.kokkos.cxx:400-427).
+// phi(node) = sum_a w_a psi(node, a) (UboltAngularIntegral's gemm,
+// sn_quadraturek.kokkos.cxx:400-427): a node-run kernel, accumulated in FP64
 template <typename T>
-__global__ void ScalarFluxKernel(const T *__restrict__ psi, const T *__restrict__ w, T *__restrict__ phi,
-                                 int64_t n_nodes, int A)
+__global__ void __launch_bounds__(256) ScalarFluxKernel(const T *__restrict__ psi, const T *__restrict__ w,
+                                                        T *__restrict__ phi, int64_t n_nodes, int A)
 {
-   const int64_t node = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-   const int lane = threadIdx.x & 31;
-   if (node >= n_nodes) return;
-   T s = T(0);
-   for (int a = lane; a < A; a += 32) s += w[a] * psi[node * A + a];
-#pragma unroll
-   for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-   if (lane == 0) phi[node] = s;
+   const int lane = threadIdx.x & 31, sub = lane & (kLpn - 1);
+   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+   const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+   for (int64_t n0 = warp * 4; n0 < n_nodes; n0 += n_warps * 4) {
+      const int64_t node = n0 + (lane >> 3);
+      const bool live = node < n_nodes;
+      double sum = 0.0;
+      if (live)
+         for (int a = sub; a < A; a += kLpn) sum += (double)w[a] * (double)psi[node * A + a];
+      sum = GroupSum(sum);
+      if (live && sub == 0) phi[node] = (T)sum;
+   }
 }
 
-// b(cell, basis 0, a) += q(cell) / W (AddIsotropicKernel, material_speck.kokkos.cxx:164-187)
-__global__ void AddSourceKernel(const DevGeom<double> g, const double *__restrict__ q, double *__restrict__ b)
+// b(cell, basis 0, a) += q(cell) / W (AddIsotropicKernel, material_speck.kokkos.cxx:164-187):
+// a run kernel over each cell's basis-0 run
+__global__ void __launch_bounds__(256) AddSourceKernel(const DevGeom<double> g, const double *__restrict__ q,
+                                                       double *__restrict__ b)
 {
-   const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-   if (tid >= g.n_cells * g.A) return;
-   const int64_t c = tid / g.A;
-   const int a = (int)(tid - c * g.A);
-   b[c * g.nb * g.A + a] += q[c] / g.sum_weights;
+   const int lane = threadIdx.x & 31, sub = lane & (kLpn - 1);
+   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+   const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+   const int A = g.A;
+   for (int64_t c0 = warp * 4; c0 < g.n_cells; c0 += n_warps * 4) {
+      const int64_t c = c0 + (lane >> 3);
+      if (c >= g.n_cells) continue;
+      const double v = q[c] / g.sum_weights;
+      double *run = b + c * g.nb * A;
+      for (int a = sub; a < A; a += kLpn) run[a] += v;
+   }
 }
 
 // b(node, a) += phi(node) (sigma_s(cell) / W) (GroupTransfer::add_transfer,
 // multigroupk.kokkos.cxx:329-362: scaled into scratch, then added)
-__global__ void AddTransferKernel(const DevGeom<double> g, const double *__restrict__ phi,
-                                  const double *__restrict__ sigma_s, double *__restrict__ b)
+__global__ void __launch_bounds__(256) AddTransferKernel(const DevGeom<double> g, const double *__restrict__ phi,
+                                                         const double *__restrict__ sigma_s, double *__restrict__ b)
 {
-   const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-   if (r >= g.n_cells * g.nb * g.A) return;
-   const int64_t node = r / g.A;
-   b[r] += phi[node] * (sigma_s[node / g.nb] / g.sum_weights);
+   const int lane = threadIdx.x & 31, sub = lane & (kLpn - 1);
+   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+   const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+   const int A = g.A;
+   const int64_t n_nodes = g.n_cells * g.nb;
+   for (int64_t n0 = warp * 4; n0 < n_nodes; n0 += n_warps * 4) {
+      const int64_t node = n0 + (lane >> 3);
+      if (node >= n_nodes) continue;
+      const double v = phi[node] * (sigma_s[node / g.nb] / g.sum_weights);
+      double *run = b + node * A;
+      for (int a = sub; a < A; a += kLpn) run[a] += v;
+   }
 }
 
 // Ghost-flux vacuum inflow, -(s / V) phi_i(x_f) inflow / W per entering face
@@ -81,8 +101,7 @@ static int ScalarFlux(ubolt_ctx *ctx, const T *psi, T *phi, void *stream)
    int rc = CheckReady(ctx, false);
    if (rc) return rc;
    if (!psi || !phi) return SetError(UBOLT_ERR_ARG, "scalar_flux: NULL array");
-   const int64_t threads = ctx->n_nodes * 32;
-   ScalarFluxKernel<T><<<(threads + 255) / 256, 256, 0, (cudaStream_t)stream>>>(psi, ctx->geom<T>().w, phi,
+   ScalarFluxKernel<T><<<RunGrid(ctx->n_nodes), 256, 0, (cudaStream_t)stream>>>(psi, ctx->geom<T>().w, phi,
                                                                                 ctx->n_nodes, ctx->A);
    return CheckLaunch("scalar_flux");
 }
@@ -90,8 +109,7 @@ static int ScalarFlux(ubolt_ctx *ctx, const T *psi, T *phi, void *stream)
 template <typename T>
 void LaunchScalarFlux(const ubolt_ctx *ctx, const T *psi, T *phi, cudaStream_t s)
 {
-   const int64_t threads = ctx->n_nodes * 32;
-   ScalarFluxKernel<T><<<(threads + 255) / 256, 256, 0, s>>>(psi, ctx->geom<T>().w, phi, ctx->n_nodes, ctx->A);
+   ScalarFluxKernel<T><<<RunGrid(ctx->n_nodes), 256, 0, s>>>(psi, ctx->geom<T>().w, phi, ctx->n_nodes, ctx->A);
 }
 template void LaunchScalarFlux<double>(const ubolt_ctx *, const double *, double *, cudaStream_t);
 template void LaunchScalarFlux<float>(const ubolt_ctx *, const float *, float *, cudaStream_t);
@@ -114,8 +132,7 @@ extern "C" int ubolt_add_source(ubolt_ctx *ctx, const double *q_cell, double *b,
    int rc = CheckReady(ctx, false);
    if (rc) return rc;
    if (!q_cell || !b) return SetError(UBOLT_ERR_ARG, "add_source: NULL array");
-   const int64_t n = ctx->n_cells * ctx->A;
-   AddSourceKernel<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(ctx->g64, q_cell, b);
+   AddSourceKernel<<<RunGrid(ctx->n_cells), 256, 0, (cudaStream_t)stream>>>(ctx->g64, q_cell, b);
    return CheckLaunch("add_source");
 }
 
@@ -125,8 +142,8 @@ extern "C" int ubolt_add_transfer(ubolt_ctx *ctx, const double *phi_from, const 
    int rc = CheckReady(ctx, false);
    if (rc) return rc;
    if (!phi_from || !sigma_s_from_to || !b) return SetError(UBOLT_ERR_ARG, "add_transfer: NULL array");
-   const int64_t n = ctx->n_rows;
-   AddTransferKernel<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(ctx->g64, phi_from, sigma_s_from_to, b);
+   AddTransferKernel<<<RunGrid(ctx->n_nodes), 256, 0, (cudaStream_t)stream>>>(ctx->g64, phi_from, sigma_s_from_to,
+                                                                              b);
    return CheckLaunch("add_transfer");
 }
 

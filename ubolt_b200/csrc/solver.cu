@@ -474,19 +474,7 @@ __device__ __forceinline__ T WarpSumSolver(T v)
    return v;
 }
 
-// The node kernels below take nodes 8 lanes at a time, 4 per warp: each lane
-// strides a node's A ordinates by 8, so every load of a warp covers four
-// runs of 8 consecutive values (whole sectors), and the warp's four nodes are
-// summed with 3 shuffle steps. All lanes of a warp run the same iterations.
-constexpr int kLpn = 8;
-
-__device__ __forceinline__ double GroupSum(double v)
-{
-   v += __shfl_xor_sync(0xffffffffu, v, 4);
-   v += __shfl_xor_sync(0xffffffffu, v, 2);
-   v += __shfl_xor_sync(0xffffffffu, v, 1);
-   return v;
-}
+// The node kernels below are node-run kernels (kLpn lanes per node).
 
 // rho(node) = R_u r0 (node) / kappa, and this block's share of |r0 - E_u rho|^2
 template <typename S>
