@@ -15,6 +15,7 @@ import subprocess
 import sys
 
 import numpy as np
+from types import SimpleNamespace
 import scipy.sparse as sp
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -92,12 +93,29 @@ def own_geometry(g):
 
 
 def own_quadrature(q):
-    """Likewise the ordinates: the reference's set of the same order."""
+    """Likewise the ordinates: the reference's set of the same order, its
+    ordinates listed in the caller's order (each of the caller's matched to
+    one of the oracle's by direction, to 1e-12)."""
     if not hasattr(q, "struct"):
         return q
     cached = q.__dict__.get("_oracle_quadrature")
     if cached is None:
-        cached = lqn(q.dim, q.sn)
+        own = lqn(q.dim, q.sn)
+        A = own.n_angles
+        given = np.asarray(q.omega, dtype=np.float64).reshape(-1, 3)
+        assert len(given) == A, "a quadrature of another size than the LQn set of its order"
+        dist = np.abs(given[:, None, :] - own.omega[None, :, :]).max(axis=2)
+        perm = dist.argmin(axis=1)
+        assert dist[np.arange(A), perm].max() <= 1e-12 and len(set(perm.tolist())) == A, \
+            "the ordinates are not the LQn set of their order"
+        if np.array_equal(perm, np.arange(A)):
+            cached = own
+        else:
+            inv = np.argsort(perm)
+            refl = np.full_like(own.reflect, -1)
+            refl[:own.dim] = inv[own.reflect[:own.dim][:, perm]]
+            cached = SimpleNamespace(dim=own.dim, sn=own.sn, omega=own.omega[perm], w=own.w[perm], reflect=refl,
+                                     sum_weights=own.sum_weights, n_angles=A)
         q.__dict__["_oracle_quadrature"] = cached
     return cached
 

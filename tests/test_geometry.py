@@ -50,6 +50,30 @@ def test_volume_weighted_opposite_ordinate_symmetry(case):
     assert rel < 1e-12, rel
 
 
+@pytest.mark.parametrize("case", CASES, ids=case_ids())
+def test_transpose_as_reversed_angle_operator_with_row_weighted_scatter(case):
+    """The form the transpose kernel computes: (L - S)^T x = P V L (P V^{-1} x)
+    - S^T x with (S^T x)(c, i, a) = sigma_s / W w_a sum_b x(c, i, b). The
+    scatter is not P-symmetric once the weights differ (S8 here): its weight
+    sits on the column, so its transpose carries it on the row."""
+    mesh, g, q, st, ss = build(case)
+    op = O.Operator(g, q, st, ss)
+    M = op.matrix()
+    L = O.Operator(g, q, st, np.zeros_like(st)).L
+    nc, nb, A = g.n_cells, g.n_basis, q.n_angles
+    V = np.repeat(g.volume, nb * A)
+    perm = np.arange(op.n).reshape(-1, A)[:, q.opposite()].ravel()
+    x = np.random.default_rng(8).standard_normal(op.n)
+    st_x = (ss[:, None, None] / q.sum_weights) * q.w[None, None, :] * x.reshape(nc, nb, A).sum(axis=2)[:, :, None]
+    y = (V * (L @ (x / V)[perm]))[perm] - st_x.ravel()
+    ref = M.T @ x
+    assert np.abs(y - ref).max() <= 1e-13 * np.abs(ref).max()
+    if len(set(q.w.tolist())) > 1:
+        # The whole operator, scatter included, is not P-symmetric
+        VA = sp.diags(V) @ M
+        assert sp.linalg.norm(VA.T - VA[perm][:, perm]) > 1e-6 * sp.linalg.norm(VA)
+
+
 def test_unweighted_symmetry_fails_on_irregular_mesh(rng):
     """On a mesh with varying cell areas the identity needs the volume weight:
     the unweighted A^T = P A P is off by far more than rounding."""

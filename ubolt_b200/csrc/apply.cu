@@ -129,11 +129,11 @@ constexpr int UpSlots() { return F * NB > 12 ? 2 : F; }
 // cells' own rows [K][NB][A], then for the scatter the node moments
 // [K][NB], sigma_s / W per cell [K] and the ordinate weights [A]
 template <typename T, int NB, int F, int AP>
-__host__ __device__ constexpr size_t ApplySmemElems(int K, int threads, int A)
+__host__ __device__ constexpr size_t ApplySmemElems(int K, int threads, int A, bool rev = false)
 {
    return (size_t)K * RecordLayout(NB, F, (int)sizeof(T)).size + (size_t)threads * UpSlots<NB, F>() * NB * AP +
           (size_t)K * NB * A +
-          (size_t)K * NB + (size_t)K + (size_t)A;
+          (size_t)K * NB + (size_t)K + (size_t)A + (rev ? (size_t)F * threads : 0);
 }
 
 // The register cap, as 256-thread blocks per SM: three (at most 80
@@ -142,7 +142,17 @@ __host__ __device__ constexpr size_t ApplySmemElems(int K, int threads, int A)
 template <typename T, int NB, int AP>
 constexpr int ApplyMinBlocks() { return (NB == 4 && AP > 1) ? 2 : 3; }
 
-template <typename T, int NB, int F, int AP, bool SCATTER>
+// REV: the transpose (L - S)^T = L^T - S^T, L^T as the reversed-angle
+// operator. (V L)^T = P (V L) P (V the cell volume on every row, P the swap
+// of each ordinate with its opposite) gives L^T x = P V L (P V^{-1} x): the
+// thread applies L, as above, to z = P V^{-1} x and writes P V of the
+// result. Its own terms take x at the opposite ordinates and need no
+// scaling (V_c / V_c); an interior inflow term takes the neighbour's x at
+// the opposite ordinates times V_c / V_neighbour. The scatter puts its
+// weight on the row: (S^T x)(a) = sigma_s / W w_a sum_b x(b). It needs every
+// aligned run of AP ordinates to map to a reversed aligned run under the
+// opposite (the launcher checks; the column kernel below serves otherwise).
+template <typename T, int NB, int F, int AP, bool SCATTER, bool REV = false>
 __global__ void __launch_bounds__(256, ApplyMinBlocks<T, NB, AP>()) ApplyKernel(const DevGeom<T> g, const T *__restrict__ x, T *__restrict__ y, int K)
 {
    constexpr RecordLayout L(NB, F, (int)sizeof(T));
@@ -158,10 +168,14 @@ __global__ void __launch_bounds__(256, ApplyMinBlocks<T, NB, AP>()) ApplyKernel(
    T *mom = xs + K * NB * A;  // scatter: [K][NB] sigma_s / W sum_b w_b x(node, b)
    T *ssw = mom + K * NB;     // scatter: [K] sigma_s / W
    T *ws = ssw + K;           // scatter: [A] the weights
+   T *rat = ws + A;           // REV: [F][threads] V_c / V_neighbour per face
    const int t = threadIdx.x;
    const int k = t / QA;
    const int q = t - k * QA;
    const int a0 = q * AP;
+   // The run of x read for this cell and its neighbours, and of y written:
+   // this thread's ordinates, or (REV) their opposites, the same run reversed
+   const int ar0 = REV ? g.opp[a0 + AP - 1] : a0;
    const int64_t c0 = (int64_t)blockIdx.x * K;
    const int64_t c = c0 + k;
    const int kc = (int)min((int64_t)K, g.n_cells - c0);
@@ -181,15 +195,18 @@ __global__ void __launch_bounds__(256, ApplyMinBlocks<T, NB, AP>()) ApplyKernel(
       const T *rec = g.rec + (int64_t)g.cls[c] * L.size;
       for (int u = q; u < RU; u += QA) CpAsync<16>(recs + k * L.size + u * (16 / (int)sizeof(T)), rec + u * (16 / (int)sizeof(T)));
       if constexpr (kRing) CpAsyncCommit();
+      T vc = T(0);
+      if constexpr (REV) vc = g.volume[c];
 #pragma unroll
       for (int f = 0; f < F; f++) {
          const int32_t cf = g.code[c * F + f];
          if (FaceInterior(cf)) {
             fcode |= 8u << (4 * f);
+            if constexpr (REV) rat[f * (int)blockDim.x + t] = vc * g.inv_vol[g.cls[cf]];
             if (!kRing || f < XS) {
 #pragma unroll
                for (int j = 0; j < NB; j++)
-                  CpAsyncRun<CU>(xup + ((f * NB + j) * (int)blockDim.x + t) * AP, x + ((int64_t)cf * NB + j) * A + a0);
+                  CpAsyncRun<CU>(xup + ((f * NB + j) * (int)blockDim.x + t) * AP, x + ((int64_t)cf * NB + j) * A + ar0);
             }
          } else {
             fcode |= (unsigned)FaceSide(cf) << (4 * f);
@@ -225,7 +242,7 @@ __global__ void __launch_bounds__(256, ApplyMinBlocks<T, NB, AP>()) ApplyKernel(
          const int n = idx / G, part = idx - (idx / G) * G;
          T m = T(0);
          if (n < nodes)
-            for (int b = part; b < A; b += G) m += ws[b] * xs[n * A + b];
+            for (int b = part; b < A; b += G) m += (REV ? T(1) : ws[b]) * xs[n * A + b];
          m += __shfl_xor_sync(0xffffffffu, m, 1);
          m += __shfl_xor_sync(0xffffffffu, m, 2);
          if (part == 0 && n < nodes) mom[n] = m * ssw[n / NB];
@@ -243,9 +260,9 @@ __global__ void __launch_bounds__(256, ApplyMinBlocks<T, NB, AP>()) ApplyKernel(
 #pragma unroll
       for (int j = 0; j < NB; j++) {
          T v[AP];
-         LoadShared<T, AP>(xk + j * A + a0, v);
+         LoadShared<T, AP>(xk + j * A + ar0, v);
 #pragma unroll
-         for (int p = 0; p < AP; p++) xo[p][j] = v[p];
+         for (int p = 0; p < AP; p++) xo[p][j] = REV ? v[AP - 1 - p] : v[p];
       }
       // Removal, and the volume term -(Omega . grad phi_i) x(c, 0, a) for i > 0
 #pragma unroll
@@ -282,24 +299,27 @@ __global__ void __launch_bounds__(256, ApplyMinBlocks<T, NB, AP>()) ApplyKernel(
                T v[AP];
                LoadShared<T, AP>(xup + ((slot * NB + j) * (int)blockDim.x + t) * AP, v);
 #pragma unroll
-               for (int p = 0; p < AP; p++) xn[p][j] = v[p];
+               for (int p = 0; p < AP; p++) xn[p][j] = REV ? v[AP - 1 - p] : v[p];
             }
          } else {
             const int side = (int)fc;
             const bool refl = g.side_bc[side] == UBOLT_BC_REFLECT;
 #pragma unroll
             for (int p = 0; p < AP; p++) {
-               const int ar = refl ? g.refl[(side >> 1) * A + a0 + p] : 0;
+               int ar = refl ? g.refl[(side >> 1) * A + a0 + p] : 0;
+               if (REV && refl) ar = g.opp[ar];
 #pragma unroll
                for (int j = 0; j < NB; j++) xn[p][j] = refl ? xk[j * A + ar] : T(0);
             }
          }
          T sp[AP], sm[AP];
+         const T ratio = (REV && (fc & 8u)) ? rat[f * (int)blockDim.x + t] : T(1);
 #pragma unroll
          for (int p = 0; p < AP; p++) {
             const T s = Dot3(om + 3 * p, na);
             sp[p] = fmax(s, T(0));
             sm[p] = fmin(s, T(0));
+            if constexpr (REV) sm[p] *= ratio;
          }
          if constexpr (NB == 1) {
 #pragma unroll
@@ -339,7 +359,7 @@ __global__ void __launch_bounds__(256, ApplyMinBlocks<T, NB, AP>()) ApplyKernel(
                if (FaceInterior(cf)) {
 #pragma unroll
                   for (int j = 0; j < NB; j++)
-                     CpAsyncRun<CU>(xup + ((slot * NB + j) * (int)blockDim.x + t) * AP, x + ((int64_t)cf * NB + j) * A + a0);
+                     CpAsyncRun<CU>(xup + ((slot * NB + j) * (int)blockDim.x + t) * AP, x + ((int64_t)cf * NB + j) * A + ar0);
                }
             }
             CpAsyncCommit();
@@ -350,9 +370,11 @@ __global__ void __launch_bounds__(256, ApplyMinBlocks<T, NB, AP>()) ApplyKernel(
       __syncthreads();
       if (live) {
 #pragma unroll
-         for (int p = 0; p < AP; p++)
+         for (int p = 0; p < AP; p++) {
+            const T wa = REV ? ws[a0 + p] : T(1);  // the transpose: w of the row's own ordinate (w_opp = w)
 #pragma unroll
-            for (int i = 0; i < NB; i++) acc[p][i] -= mom[k * NB + i];
+            for (int i = 0; i < NB; i++) acc[p][i] -= wa * mom[k * NB + i];
+         }
       }
    }
    if (!live) return;
@@ -360,8 +382,8 @@ __global__ void __launch_bounds__(256, ApplyMinBlocks<T, NB, AP>()) ApplyKernel(
    for (int i = 0; i < NB; i++) {
       T v[AP];
 #pragma unroll
-      for (int p = 0; p < AP; p++) v[p] = acc[p][i];
-      StoreRun<T, AP>(y + (c * NB + i) * A + a0, v);
+      for (int p = 0; p < AP; p++) v[REV ? AP - 1 - p : p] = acc[p][i];
+      StoreRun<T, AP>(y + (c * NB + i) * A + ar0, v);
    }
 }
 
@@ -538,28 +560,46 @@ static int ApplyCells(Kern kern, int QA, Smem smem_of)
    return best;
 }
 
+// True where the opposite maps every aligned run of ap ordinates onto an
+// aligned run in reverse order (the LQn sets, with the x sign fastest, do)
+static bool OppositeRunsReverse(const ubolt_ctx *ctx, int ap)
+{
+   const int A = ctx->A;
+   if ((int)ctx->h_opp.size() != A || A % ap != 0) return false;
+   for (int a0 = 0; a0 < A; a0 += ap) {
+      const int r0 = ctx->h_opp[a0 + ap - 1];
+      if (r0 % ap != 0) return false;
+      for (int p = 0; p < ap; p++)
+         if (ctx->h_opp[a0 + p] != r0 + (ap - 1 - p)) return false;
+   }
+   return true;
+}
+
 template <typename T, int NB, int F>
 int LaunchApply(const ubolt_ctx *ctx, const DevGeom<T> &g, const T *x, T *y, int mode, cudaStream_t s)
 {
    const int K = CellsPerBlock(g.A);
    const int threads = ((K * g.A + 31) / 32) * 32;
    const int64_t blocks = (g.n_cells + K - 1) / K;
-   if (mode == kAdjoint) {
+   // AP ordinates per thread as one 16-byte run where they fit evenly and
+   // both vectors are 16-byte aligned
+   constexpr int AV = 16 / (int)sizeof(T);
+   const bool vec = g.A % AV == 0 && (reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) % 16 == 0;
+   const bool rev = mode == kAdjoint && OppositeRunsReverse(ctx, vec ? AV : 1);
+   if (mode == kAdjoint && !rev) {
       const size_t smem = sizeof(T) * (size_t)(K * NB * g.A + K * NB);
       AdjointApplyKernel<T, NB, F><<<blocks, threads, smem, s>>>(g, x, y, K);
    } else {
-      // AP ordinates per thread as one 16-byte run where they fit evenly and
-      // both vectors are 16-byte aligned
-      constexpr int AV = 16 / (int)sizeof(T);
-      const bool vec = g.A % AV == 0 && (reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) % 16 == 0;
       const int AP = vec ? AV : 1;
       const int QA = g.A / AP;
       if (QA > 256) return SetError(UBOLT_ERR_ARG, "apply: %d ordinates need 16-byte aligned vectors", g.A);
-      auto kern = vec ? (mode == kFull ? ApplyKernel<T, NB, F, AV, true> : ApplyKernel<T, NB, F, AV, false>)
-                      : (mode == kFull ? ApplyKernel<T, NB, F, 1, true> : ApplyKernel<T, NB, F, 1, false>);
+      auto kern = rev ? (vec ? ApplyKernel<T, NB, F, AV, true, true> : ApplyKernel<T, NB, F, 1, true, true>)
+                  : vec ? (mode == kFull ? ApplyKernel<T, NB, F, AV, true> : ApplyKernel<T, NB, F, AV, false>)
+                        : (mode == kFull ? ApplyKernel<T, NB, F, 1, true> : ApplyKernel<T, NB, F, 1, false>);
       const int A = g.A;
-      auto smem_of = [vec, A](int K, int thr) {
-         return sizeof(T) * (vec ? ApplySmemElems<T, NB, F, AV>(K, thr, A) : ApplySmemElems<T, NB, F, 1>(K, thr, A));
+      auto smem_of = [vec, A, rev](int K, int thr) {
+         return sizeof(T) * (vec ? ApplySmemElems<T, NB, F, AV>(K, thr, A, rev)
+                                 : ApplySmemElems<T, NB, F, 1>(K, thr, A, rev));
       };
       const int Kt = ApplyCells(kern, QA, smem_of);
       const int64_t nblk = (g.n_cells + Kt - 1) / Kt;

@@ -294,6 +294,8 @@ extern "C" int ubolt_ctx_create(const ubolt_dg_geometry *geom, const ubolt_quadr
    h.sigma_t = ctx->sigma_t32;
    h.sigma_s = ctx->sigma_s32;
    if ((rc = Upload(ctx, ctx->h_volume, &ctx->d_volume))) return fail(rc);
+   g.volume = ctx->d_volume;
+   if ((rc = Upload(ctx, ToF32(ctx->h_volume), &h.volume))) return fail(rc);
    {
       // The opposite ordinate (every cosine negated), by exact search
       std::vector<int32_t> opp(A, -1);
@@ -308,6 +310,8 @@ extern "C" int ubolt_ctx_create(const ubolt_dg_geometry *geom, const ubolt_quadr
          if (opp[a] < 0 || ctx->h_w[opp[a]] != ctx->h_w[a])
             return fail(SetError(UBOLT_ERR_ARG, "ordinate %d has no opposite of equal weight", a));
       if ((rc = Upload(ctx, opp, &ctx->d_opp))) return fail(rc);
+      g.opp = h.opp = ctx->d_opp;
+      ctx->h_opp = opp;
    }
    if ((rc = CtxAlloc(ctx, 64 * sizeof(unsigned long long), &p))) return fail(rc);
    ctx->d_counters = static_cast<unsigned long long *>(p);

@@ -25,6 +25,7 @@ struct ubolt_ctx {
    std::vector<double> h_omega, h_w, h_volume, h_nA;
    std::vector<int32_t> h_refl, h_code, h_cls;
    std::vector<int8_t> h_mirror;
+   std::vector<int32_t> h_opp;  // the opposite ordinate of each ordinate
 
    // Device allocations (owned)
    std::vector<void *> owned;

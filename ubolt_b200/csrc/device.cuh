@@ -70,6 +70,8 @@ struct DevGeom {
    const T *w;             // [A]
    const int32_t *refl;    // [3][A]
    int32_t side_bc[6];     // UBOLT_BC_* per side
+   const int32_t *opp;     // [A] the opposite ordinate (every cosine negated)
+   const T *volume;        // [cell] cell volume
    // Group cross sections (per cell)
    const T *sigma_t;
    const T *sigma_s;

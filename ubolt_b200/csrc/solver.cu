@@ -276,17 +276,49 @@ static double Norm(const ubolt_solver *ws, const S *x, int64_t n, cudaStream_t s
    return std::sqrt(ws->mb_h[kMbScalars]);
 }
 
-// y(c, i, a) = scale(c) x(c, i, opp(a)): P (the swap of each ordinate with
-// its opposite) times V^{-1} (inverse = 1) or V (inverse = 0), V the cell volume
+// y(c, i, a) = x(c, i, opp(a)) / V_c: P V^{-1} (P the swap of each ordinate
+// with its opposite, V the cell volume). A node-run kernel.
 template <typename S>
-__global__ void OppositeScaleKernel(const S *__restrict__ x, S *__restrict__ y, const int32_t *__restrict__ opp,
-                                    const double *__restrict__ volume, int nb, int A, int64_t n, int inverse)
+__global__ void __launch_bounds__(256) OppositeScaleKernel(const S *__restrict__ x, S *__restrict__ y,
+                                                           const int32_t *__restrict__ opp,
+                                                           const double *__restrict__ volume, int nb, int A,
+                                                           int64_t n_nodes)
 {
-   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
-      const int64_t node = r / A;
-      const int a = (int)(r - node * A);
+   const int lane = threadIdx.x & 31, sub = lane & (kLpn - 1);
+   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+   const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+   for (int64_t n0 = warp * 4; n0 < n_nodes; n0 += n_warps * 4) {
+      const int64_t node = n0 + (lane >> 3);
+      if (node >= n_nodes) continue;
+      const double iv = 1.0 / volume[node / nb];
+      const S *xr = x + node * A;
+      S *yr = y + node * A;
+      for (int a = sub; a < A; a += kLpn) yr[a] = (S)((double)xr[opp[a]] * iv);
+   }
+}
+
+// y = V P y in place: each pair (a, opp(a)) swapped and scaled by V_c by the
+// lane that owns its lower index (the opposite is an involution). A node-run kernel.
+template <typename S>
+__global__ void __launch_bounds__(256) OppositeScaleInPlaceKernel(S *__restrict__ y, const int32_t *__restrict__ opp,
+                                                                  const double *__restrict__ volume, int nb, int A,
+                                                                  int64_t n_nodes)
+{
+   const int lane = threadIdx.x & 31, sub = lane & (kLpn - 1);
+   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+   const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+   for (int64_t n0 = warp * 4; n0 < n_nodes; n0 += n_warps * 4) {
+      const int64_t node = n0 + (lane >> 3);
+      if (node >= n_nodes) continue;
       const double v = volume[node / nb];
-      y[r] = (S)((double)x[node * A + opp[a]] * (inverse ? 1.0 / v : v));
+      S *yr = y + node * A;
+      for (int a = sub; a < A; a += kLpn) {
+         const int b = opp[a];
+         if (b < a) continue;
+         const double ya = (double)yr[a], yb = (double)yr[b];
+         yr[a] = (S)(yb * v);
+         if (b != a) yr[b] = (S)(ya * v);
+      }
    }
 }
 
@@ -314,14 +346,14 @@ static int Precondition(ubolt_ctx *ctx, int pc, bool adjoint, const T *x, T *y, 
 {
    cudaStream_t s = (cudaStream_t)stream;
    if (adjoint && (pc == UBOLT_PC_SWEEP || pc == UBOLT_PC_SWEEP_DSA)) {
-      const int grid = (int)std::min<int64_t>((n + 255) / 256, 148 * 8);
-      OppositeScaleKernel<T><<<grid, 256, 0, s>>>(x, tmp, ctx->d_opp, ctx->d_volume, ctx->nb, ctx->A, n, 1);
+      const int grid = RunGrid(ctx->n_nodes);
+      OppositeScaleKernel<T><<<grid, 256, 0, s>>>(x, tmp, ctx->d_opp, ctx->d_volume, ctx->nb, ctx->A, ctx->n_nodes);
       CountLaunch();
       int rc = Sweep<T>(ctx, tmp, y, stream);
       if (rc) return rc;
-      OppositeScaleKernel<T><<<grid, 256, 0, s>>>(y, tmp, ctx->d_opp, ctx->d_volume, ctx->nb, ctx->A, n, 0);
+      OppositeScaleInPlaceKernel<T><<<grid, 256, 0, s>>>(y, ctx->d_opp, ctx->d_volume, ctx->nb, ctx->A, ctx->n_nodes);
       CountLaunch();
-      return DeviceCopy<T>(y, tmp, n, s, "adjoint pc");
+      return CheckLaunch("adjoint pc");
    }
    switch (pc) {
    case UBOLT_PC_NONE:
@@ -518,7 +550,8 @@ template <typename S>
 __global__ void __launch_bounds__(256) IsoExpandKernel(const S *__restrict__ r0, const double *__restrict__ alpha_p,
                                                        const double *__restrict__ phi, const double *__restrict__ rho,
                                                        const S *__restrict__ u, int A, int64_t n_nodes,
-                                                       S *__restrict__ t)
+                                                       S *__restrict__ t, const int32_t *__restrict__ opp,
+                                                       const double *__restrict__ volume, int nb)
 {
    const int lane = threadIdx.x & 31, sub = lane & (kLpn - 1);
    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -527,13 +560,17 @@ __global__ void __launch_bounds__(256) IsoExpandKernel(const S *__restrict__ r0,
    for (int64_t nb0 = warp * 4; nb0 < n_nodes; nb0 += n_warps * 4) {
       const int64_t node = nb0 + (lane >> 3);
       if (node >= n_nodes) continue;
+      // With opp: P V^{-1} of the expansion (u is symmetric under the opposite)
+      const double sc = opp ? 1.0 / volume[node / nb] : 1.0;
       if (!r0) {  // r0 isotropic: alpha r_perp = 0
-         for (int a = sub; a < A; a += kLpn) t[node * A + a] = (S)((u ? (double)u[a] : 1.0) * phi[node]);
+         for (int a = sub; a < A; a += kLpn) t[node * A + a] = (S)((u ? (double)u[a] : 1.0) * phi[node] * sc);
          continue;
       }
       const double iso = phi[node] - al * rho[node];
-      for (int a = sub; a < A; a += kLpn)
-         t[node * A + a] = (S)(al * (double)r0[node * A + a] + (u ? (double)u[a] : 1.0) * iso);
+      for (int a = sub; a < A; a += kLpn) {
+         const int ar = opp ? opp[a] : a;
+         t[node * A + a] = (S)((al * (double)r0[node * A + ar] + (u ? (double)u[a] : 1.0) * iso) * sc);
+      }
    }
 }
 
@@ -584,9 +621,19 @@ static int IsoPrecondition(ubolt_ctx *ctx, bool adjoint, const S *r0, const doub
                            const double *rho, const S *u, S *t, S *z, S *tmp, int64_t n, int igrid, void *stream)
 {
    if (!adjoint) return SweepAffine<S>(ctx, r0, alpha, phi, rho, u, z, stream);
-   IsoExpandKernel<S><<<igrid, 256, 0, (cudaStream_t)stream>>>(r0, alpha, phi, rho, u, ctx->A, ctx->n_nodes, t);
+   // L^{-T} = V P L^{-1} P V^{-1}: the expansion and P V^{-1} in one pass,
+   // the sweep, then V P in place
+   IsoExpandKernel<S><<<igrid, 256, 0, (cudaStream_t)stream>>>(r0, alpha, phi, rho, u, ctx->A, ctx->n_nodes, t,
+                                                               ctx->d_opp, ctx->d_volume, ctx->nb);
    CountLaunch();
-   return Precondition<S>(ctx, UBOLT_PC_SWEEP, adjoint, t, z, tmp, n, stream);
+   int rc = Sweep<S>(ctx, t, z, stream);
+   if (rc) return rc;
+   OppositeScaleInPlaceKernel<S><<<RunGrid(ctx->n_nodes), 256, 0, (cudaStream_t)stream>>>(z, ctx->d_opp, ctx->d_volume,
+                                                                                       ctx->nb, ctx->A, ctx->n_nodes);
+   CountLaunch();
+   (void)tmp;
+   (void)n;
+   return CheckLaunch("adjoint pc");
 }
 
 static int IsoGrid(int64_t n_nodes)
