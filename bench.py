@@ -56,7 +56,8 @@ def _args():
                    help="tri256 is the headline line; hex128 (4 groups) and tet44 time the other solve configs")
     p.add_argument("--restart", type=int, default=0, help="GMRES restart (0: 30, or 10 for hex128)")
     p.add_argument("--profile", default="",
-                   choices=["", "apply", "apply32", "sweep", "sweep32", "wave", "wave32", "adjoint", "dsa_spmv"],
+                   choices=["", "apply", "apply32", "sweep", "sweep32", "wave", "wave32", "adjoint", "adjoint32",
+                            "dsa_spmv", "block", "gradient", "scalar_flux"],
                    help="run only this kernel, --warmup + --steps launches on the workload, for a profiler")
     return p.parse_args()
 
@@ -240,6 +241,15 @@ def profile_kernel(args, ctx, T, stream):
         u = dsa.restrict(xr)
         v = torch.empty_like(u)
         fn = lambda: dsa.spmv(u, v)
+    elif kind == "block":
+        blk = T.ElementBlockInverse(ctx)
+        fn = lambda: blk.apply(xr, yr)
+    elif kind == "gradient":
+        lam = torch.rand_like(xr)
+        fn = lambda: T.gradient(ctx, xr, lam)
+    elif kind == "scalar_flux":
+        phi = torch.empty(ctx.n_nodes, dtype=xr.dtype, device="cuda")
+        fn = lambda: T.angular_integral(ctx, xr, phi)
     else:
         A = T.TransportOperator(ctx)
         fn = (lambda: A.mult(xr, yr)) if kind == "apply" else (lambda: A.mult_transpose(xr, yr))

@@ -199,6 +199,17 @@ int ubolt_block_inverse(ubolt_ctx *ctx, double *inv, void *stream);
  * sn_quadrature.hpp:163-171, src/sn_quadraturek.kokkos.cxx:400-427. */
 int ubolt_scalar_flux(ubolt_ctx *ctx, const double *psi, double *phi, void *stream);
 int ubolt_scalar_flux_f32(ubolt_ctx *ctx, const float *psi, float *phi, void *stream);
+/* The current J(node, d) = sum_a w_a Omega_a,d psi(node, a), d < dim, into
+ * current[node * dim + d] (n_nodes dim values). IntegrateCurrent, under
+ * GroupTransfer::set_scalar_flux, src/multigroupk.kokkos.cxx:275-279. */
+int ubolt_current(ubolt_ctx *ctx, const double *psi, double *current, void *stream);
+/* psi(node, a) = phi(node) / W + sum_d p1(a, d) J(node, d), the P1
+ * expansion of a scalar flux and current, p1(a) = T^{-1} Omega_a with
+ * T = sum_a w_a Omega_a Omega_a^T (the inverse of the moments of a P1
+ * field). The moments store's starting psi: GroupTransfer::enable_current
+ * and expand_p1, src/multigroupk.kokkos.cxx:373-499. UBOLT_ERR_ARG where the
+ * ordinates' weighted directions do not sum to zero. */
+int ubolt_expand_p1(ubolt_ctx *ctx, const double *phi, const double *current, double *psi, void *stream);
 /* b(cell, basis 0, a) += q(cell) / W, q the angle-integrated isotropic
  * source per cell (device, n_cells). MaterialSourceTable::add_isotropic,
  * src/material_speck.kokkos.cxx:164-213. */

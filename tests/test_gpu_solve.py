@@ -462,14 +462,46 @@ def test_upscatter_outer_iteration_matches_the_coupled_solve():
     phi_ref = [O.angular_integral(psi_ref[gg], nc * nb, q) for gg in range(G)]
 
     ctx = T.Context(g, q)
-    info = {}
-    phis, stats = T.solve_groups(ctx, st, ss, src, rtol=1e-12, max_it=2000, outer_rtol=1e-10, outer_info=info)
-    assert info["upscatter"] and info["g_up"] == 1 and info["converged"] and info["outer_iterations"] >= 3
-    assert info["error_estimate"] < 1e-10
-    for gg in range(G):
-        err = np.linalg.norm(phis[gg].cpu().numpy() - phi_ref[gg]) / np.linalg.norm(phi_ref[gg])
-        assert err <= 1e-9, (gg, err)
+    # The angular store, and the moments store with and without the
+    # reconstruction steps: the same coupled solution
+    for store, recon in (("angular", "tol"), ("moments", "tol"), ("moments", "none")):
+        info = {}
+        phis, stats = T.solve_groups(ctx, st, ss, src, rtol=1e-12, max_it=2000, outer_rtol=1e-10,
+                                     outer_store=store, outer_recon=recon, outer_info=info)
+        assert info["upscatter"] and info["g_up"] == 1 and info["converged"] and info["outer_iterations"] >= 3
+        assert info["error_estimate"] < 1e-10
+        if store == "moments":
+            assert info["reconstructed_solves"] > 0
+            assert (info["reconstruction_steps"] > 0) == (recon == "tol")
+        for gg in range(G):
+            err = np.linalg.norm(phis[gg].cpu().numpy() - phi_ref[gg]) / np.linalg.norm(phi_ref[gg])
+            assert err <= 1e-9, (store, recon, gg, err)
     # An outer tolerance below the inner one is refused, as the reference does
     with pytest.raises(Exception):
         T.solve_groups(ctx, st, ss, src, rtol=1e-8, outer_rtol=1e-10)
+    ctx.close()
+
+
+@pytest.mark.parametrize("case", [c for c in CASES if c[0] in ("tri_dg1_refl", "hex_dg1_refl")],
+                         ids=["tri_dg1_refl", "hex_dg1_refl"])
+def test_current_and_p1_expansion_round_trip(case):
+    """A P1 field psi = phi / W + Omega . c: its scalar flux and current are
+    phi and T c (T = sum_a w_a Omega_a Omega_a^T), and the expansion of those
+    moments gives psi back; the current of any psi matches its definition."""
+    mesh, g, q, st, ss = build(case)
+    ctx, keep = ctx_for(g, q, st, ss)
+    nn, A, D = g.n_cells * g.n_basis, q.n_angles, g.dim
+    rng = np.random.default_rng(13)
+    phi = rng.uniform(0.5, 1.5, nn)
+    c = rng.standard_normal((nn, D))
+    om = q.omega[:, :D]
+    psi = phi[:, None] / q.sum_weights + c @ om.T                 # (nn, A)
+    Tm = (q.w[:, None, None] * om[:, :, None] * om[:, None, :]).sum(axis=0)
+    J = T.current(ctx, dev(psi.ravel()))
+    assert np.abs(J.cpu().numpy() - c @ Tm.T).max() <= 1e-12 * np.abs(c @ Tm.T).max()
+    back = T.expand_p1(ctx, dev(phi), J)
+    assert np.abs(back.cpu().numpy() - psi.ravel()).max() <= 1e-12 * np.abs(psi).max()
+    x = rng.standard_normal(nn * A)
+    Jx = T.current(ctx, dev(x)).cpu().numpy()
+    assert np.abs(Jx - (x.reshape(nn, A) * q.w) @ om).max() <= 1e-12 * np.abs(x).max() * q.sum_weights
     ctx.close()

@@ -78,6 +78,8 @@ for _n in ("ubolt_apply", "ubolt_apply_f32", "ubolt_apply_unscattered", "ubolt_a
 _sig("ubolt_diagonal", C.c_int, vp, vp, vp)
 _sig("ubolt_block_setup", C.c_int, vp, i64p, vp)
 _sig("ubolt_block_inverse", C.c_int, vp, vp, vp)
+_sig("ubolt_current", C.c_int, vp, vp, vp, vp)
+_sig("ubolt_expand_p1", C.c_int, vp, vp, vp, vp, vp)
 _sig("ubolt_add_transfer", C.c_int, vp, vp, vp, vp, vp)
 _sig("ubolt_add_ghost_inflow", C.c_int, vp, dp, vp, vp)
 

@@ -2,6 +2,8 @@
 // FP32 mirror, and the per-group cross-section pointers.
 #include "ctx.h"
 
+#include <cmath>
+
 #include <atomic>
 #include <cstring>
 #include <unordered_map>
@@ -312,6 +314,57 @@ extern "C" int ubolt_ctx_create(const ubolt_dg_geometry *geom, const ubolt_quadr
       if ((rc = Upload(ctx, opp, &ctx->d_opp))) return fail(rc);
       g.opp = h.opp = ctx->d_opp;
       ctx->h_opp = opp;
+   }
+   {
+      // The P1 expansion's tables: w_a Omega_a, and p1(a) = T^{-1} Omega_a
+      // with T = sum_a w_a Omega_a Omega_a^T, inverted by Gauss-Jordan
+      // (dim <= 3); usable where sum_a w_a Omega_a vanishes
+      const int D = ctx->dim;
+      double t[3][3] = {}, first[3] = {}, inv[3][3] = {};
+      for (int a = 0; a < A; a++)
+         for (int d = 0; d < D; d++) {
+            first[d] += ctx->h_w[a] * ctx->h_omega[3 * a + d];
+            for (int e = 0; e < D; e++) t[d][e] += ctx->h_w[a] * ctx->h_omega[3 * a + d] * ctx->h_omega[3 * a + e];
+         }
+      bool ok = true;
+      for (int d = 0; d < D; d++) ok &= std::fabs(first[d]) <= 1e-12 * std::fabs(ctx->sum_weights);
+      for (int d = 0; d < D; d++) inv[d][d] = 1.0;
+      for (int k = 0; k < D && ok; k++) {
+         int piv = k;
+         for (int i = k + 1; i < D; i++)
+            if (std::fabs(t[i][k]) > std::fabs(t[piv][k])) piv = i;
+         if (!(std::fabs(t[piv][k]) > 0.0)) {
+            ok = false;
+            break;
+         }
+         for (int j = 0; j < 3; j++) {
+            std::swap(t[k][j], t[piv][j]);
+            std::swap(inv[k][j], inv[piv][j]);
+         }
+         const double r = 1.0 / t[k][k];
+         for (int j = 0; j < D; j++) {
+            t[k][j] *= r;
+            inv[k][j] *= r;
+         }
+         for (int i = 0; i < D; i++) {
+            if (i == k) continue;
+            const double f = t[i][k];
+            for (int j = 0; j < D; j++) {
+               t[i][j] -= f * t[k][j];
+               inv[i][j] -= f * inv[k][j];
+            }
+         }
+      }
+      std::vector<double> p1((size_t)A * D, 0.0), wom((size_t)A * D, 0.0);
+      for (int a = 0; a < A; a++)
+         for (int d = 0; d < D; d++) {
+            wom[(size_t)a * D + d] = ctx->h_w[a] * ctx->h_omega[3 * a + d];
+            double sum = 0.0;
+            for (int e = 0; e < D; e++) sum += inv[d][e] * ctx->h_omega[3 * a + e];
+            p1[(size_t)a * D + d] = sum;
+         }
+      if ((rc = Upload(ctx, p1, &ctx->d_p1)) || (rc = Upload(ctx, wom, &ctx->d_w_omega))) return fail(rc);
+      ctx->p1_ok = ok;
    }
    if ((rc = CtxAlloc(ctx, 64 * sizeof(unsigned long long), &p))) return fail(rc);
    ctx->d_counters = static_cast<unsigned long long *>(p);

@@ -34,6 +34,9 @@ struct ubolt_ctx {
    float *sigma_t32 = nullptr, *sigma_s32 = nullptr;
    const double *d_volume = nullptr;           // [n_cells] FP64 cell volumes
    const int32_t *d_opp = nullptr;             // [A] the ordinate opposite each ordinate
+   const double *d_p1 = nullptr;               // [A][dim] T^{-1} Omega_a, T = sum_a w_a Omega_a Omega_a^T
+   bool p1_ok = false;                         // sum_a w_a Omega_a = 0 and T regular (the P1 expansion exists)
+   const double *d_w_omega = nullptr;          // [A][dim] w_a Omega_a
    unsigned long long *d_counters = nullptr;   // 64 counters/flags for set-up calls
    bool group_set = false;
    uint64_t group_epoch = 0;  // bumped by every ubolt_set_group: caches keyed on the cross sections

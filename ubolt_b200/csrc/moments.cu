@@ -95,6 +95,50 @@ __global__ void GhostInflowKernel(const DevGeom<double> g, const double *__restr
    for (int i = 0; i < g.nb; i++) b[(c * g.nb + i) * g.A + a] += add[i];
 }
 
+// J(node, d) = sum_a w_a Omega_a,d psi(node, a): a node-run kernel
+__global__ void __launch_bounds__(256) CurrentKernel(const double *__restrict__ psi, const double *__restrict__ w_omega,
+                                                     double *__restrict__ cur, int64_t n_nodes, int A, int dim)
+{
+   const int lane = threadIdx.x & 31, sub = lane & (kLpn - 1);
+   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+   const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+   for (int64_t n0 = warp * 4; n0 < n_nodes; n0 += n_warps * 4) {
+      const int64_t node = n0 + (lane >> 3);
+      const bool live = node < n_nodes;
+      double s[3] = {0.0, 0.0, 0.0};
+      if (live)
+         for (int a = sub; a < A; a += kLpn) {
+            const double v = psi[node * A + a];
+            for (int d = 0; d < dim; d++) s[d] += w_omega[a * dim + d] * v;
+         }
+      for (int d = 0; d < 3; d++) s[d] = GroupSum(s[d]);
+      if (live && sub == 0)
+         for (int d = 0; d < dim; d++) cur[node * dim + d] = s[d];
+   }
+}
+
+// psi(node, a) = phi(node) / W + sum_d p1(a, d) J(node, d): a node-run kernel
+__global__ void __launch_bounds__(256) ExpandP1Kernel(const double *__restrict__ phi, const double *__restrict__ cur,
+                                                      const double *__restrict__ p1, double inv_w,
+                                                      double *__restrict__ psi, int64_t n_nodes, int A, int dim)
+{
+   const int lane = threadIdx.x & 31, sub = lane & (kLpn - 1);
+   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+   const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+   for (int64_t n0 = warp * 4; n0 < n_nodes; n0 += n_warps * 4) {
+      const int64_t node = n0 + (lane >> 3);
+      if (node >= n_nodes) continue;
+      double j[3] = {0.0, 0.0, 0.0};
+      for (int d = 0; d < dim; d++) j[d] = cur[node * dim + d];
+      const double base = phi[node] * inv_w;
+      for (int a = sub; a < A; a += kLpn) {
+         double v = base;
+         for (int d = 0; d < dim; d++) v += p1[a * dim + d] * j[d];
+         psi[node * A + a] = v;
+      }
+   }
+}
+
 template <typename T>
 static int ScalarFlux(ubolt_ctx *ctx, const T *psi, T *phi, void *stream)
 {
@@ -125,6 +169,30 @@ extern "C" int ubolt_scalar_flux(ubolt_ctx *ctx, const double *psi, double *phi,
 extern "C" int ubolt_scalar_flux_f32(ubolt_ctx *ctx, const float *psi, float *phi, void *stream)
 {
    return ScalarFlux<float>(ctx, psi, phi, stream);
+}
+
+extern "C" int ubolt_current(ubolt_ctx *ctx, const double *psi, double *current, void *stream)
+{
+   int rc = CheckReady(ctx, false);
+   if (rc) return rc;
+   if (!psi || !current) return SetError(UBOLT_ERR_ARG, "current: NULL array");
+   CurrentKernel<<<RunGrid(ctx->n_nodes), 256, 0, (cudaStream_t)stream>>>(psi, ctx->d_w_omega, current, ctx->n_nodes,
+                                                                          ctx->A, ctx->dim);
+   return CheckLaunch("current");
+}
+
+extern "C" int ubolt_expand_p1(ubolt_ctx *ctx, const double *phi, const double *current, double *psi, void *stream)
+{
+   int rc = CheckReady(ctx, false);
+   if (rc) return rc;
+   if (!phi || !current || !psi) return SetError(UBOLT_ERR_ARG, "expand_p1: NULL array");
+   if (!ctx->p1_ok)
+      return SetError(UBOLT_ERR_ARG, "expand_p1: the ordinates' weighted directions do not sum to zero, or their "
+                                     "second moment is singular");
+   ExpandP1Kernel<<<RunGrid(ctx->n_nodes), 256, 0, (cudaStream_t)stream>>>(phi, current, ctx->d_p1,
+                                                                           1.0 / ctx->sum_weights, psi, ctx->n_nodes,
+                                                                           ctx->A, ctx->dim);
+   return CheckLaunch("expand_p1");
 }
 
 extern "C" int ubolt_add_source(ubolt_ctx *ctx, const double *q_cell, double *b, void *stream)

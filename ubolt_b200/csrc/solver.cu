@@ -352,7 +352,6 @@ static int Precondition(ubolt_ctx *ctx, int pc, bool adjoint, const T *x, T *y, 
       int rc = Sweep<T>(ctx, tmp, y, stream);
       if (rc) return rc;
       OppositeScaleInPlaceKernel<T><<<grid, 256, 0, s>>>(y, ctx->d_opp, ctx->d_volume, ctx->nb, ctx->A, ctx->n_nodes);
-      CountLaunch();
       return CheckLaunch("adjoint pc");
    }
    switch (pc) {
@@ -630,7 +629,6 @@ static int IsoPrecondition(ubolt_ctx *ctx, bool adjoint, const S *r0, const doub
    if (rc) return rc;
    OppositeScaleInPlaceKernel<S><<<RunGrid(ctx->n_nodes), 256, 0, (cudaStream_t)stream>>>(z, ctx->d_opp, ctx->d_volume,
                                                                                        ctx->nb, ctx->A, ctx->n_nodes);
-   CountLaunch();
    (void)tmp;
    (void)n;
    return CheckLaunch("adjoint pc");

@@ -293,7 +293,6 @@ int LaunchWaveSweepT(const WaveDev &w, const T *q, T *psi, const void *fac, cons
    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, w.smem) != cudaSuccess)
       return CudaCheck(cudaGetLastError(), "wave sweep shared memory");
    kern<<<w.A, THREADS, w.smem, st>>>(w, q, psi, static_cast<const unsigned char *>(fac), inp);
-   CountLaunch();
    return CheckLaunch("wave sweep");
 }
 
@@ -309,13 +308,11 @@ int WaveFactors(ubolt_ctx *ctx, const WaveDev &w, void *fac, int elem, cudaStrea
    if (elem == 8) {
       UBOLT_DISPATCH(ctx->nb, ctx->F, {
          WaveFactorKernel<double, NB_, F_><<<grid, 128, 0, st>>>(ctx->geom<double>(), w, f, total_levels);
-         CountLaunch();
          return CheckLaunch("wave factors");
       });
    } else {
       UBOLT_DISPATCH(ctx->nb, ctx->F, {
          WaveFactorKernel<float, NB_, F_><<<grid, 128, 0, st>>>(ctx->geom<float>(), w, f, total_levels);
-         CountLaunch();
          return CheckLaunch("wave factors");
       });
    }

@@ -142,6 +142,20 @@ def angular_integral(ctx, psi, phi=None, stream=None):
     return phi
 
 
+def current(ctx, psi, cur=None, stream=None):
+    """J(node, d) = sum_a w_a Omega_a,d psi(node, a), as (n_nodes, dim)."""
+    cur = torch.empty(ctx.n_nodes, ctx.geometry.dim, dtype=torch.float64, device=psi.device) if cur is None else cur
+    check(lib.ubolt_current(ctx.handle, _p(psi), _p(cur), _stream(stream)))
+    return cur
+
+
+def expand_p1(ctx, phi, cur, psi=None, stream=None):
+    """psi(node, a) = phi(node) / W + T^{-1} Omega_a . J(node): the P1 field with these moments."""
+    psi = ctx.vector() if psi is None else psi
+    check(lib.ubolt_expand_p1(ctx.handle, _p(phi), _p(cur), _p(psi), _stream(stream)))
+    return psi
+
+
 def fill_inflow(ctx, side_inflow, b, stream=None):
     """b += the ghost-flux vacuum inflow (side_inflow: angle-integrated, per side)."""
     s = np.zeros(6)
@@ -338,7 +352,8 @@ def group_tables(ctx, sigma_t, sigma_s, source):
 
 
 def solve_groups(ctx, sigma_t, sigma_s, source, side_inflow=None, dsa=None, keep_psi=False, solver=None,
-                 outer_rtol=1e-8, outer_max_it=1000, outer_inner_gamma=0.01, outer_info=None, **solver_opts):
+                 outer_rtol=1e-8, outer_max_it=1000, outer_inner_gamma=0.01, outer_store="angular",
+                 outer_recon="tol", outer_info=None, **solver_opts):
     """The group loop of the reference driver (tests/transportk.kokkos.cxx:
     1036-1208): per group g, point the operator (and the DSA) at g's cross
     sections, build b = inflow + source + the transfer out of the other
@@ -362,6 +377,17 @@ def solve_groups(ctx, sigma_t, sigma_s, source, side_inflow=None, dsa=None, keep
     test first passes, then one more pass at rtol. outer_rtol below the
     solver's rtol is refused (a warm start that moves by less than its rtol
     takes no iterations, and the outer test would pass falsely).
+
+    outer_store "moments" (-outer_store moments) keeps, in place of one psi
+    per group, each thermal group's scalar flux and current and ONE psi that
+    every solve reuses: a thermal solve after the first pass starts from the
+    P1 expansion of the group's last moments, then (outer_recon) Richardson
+    steps on L_g psi = c, c = b + the within-group scatter of the group's last
+    phi, each step psi += sweep(c - L_g psi) - "tol": until ||c - L_g psi|| <=
+    rtol ||c||, at most 40 steps; "none": the P1 guess alone; an int: that
+    many steps. A step that does not reduce the residual is reverted and ends
+    the reconstruction (tests/transportk.kokkos.cxx:282-334, 650-720). With the
+    exact sweep as the streaming stage, one step solves L_g psi = c.
 
     sigma_t: (G, n_cells), sigma_s: (G, G, n_cells) [from, to], source:
     (G, n_cells) - NumPy arrays, or device tensors (used in place, as from
@@ -411,19 +437,75 @@ def solve_groups(ctx, sigma_t, sigma_s, source, side_inflow=None, dsa=None, keep
             outer_info.update(upscatter=False, outer_iterations=1, converged=True)
         return (phis, stats, psis) if keep_psi else (phis, stats)
 
+    if outer_store not in ("angular", "moments"):
+        raise _lib.UboltError(1, f"outer_store is angular or moments, was given {outer_store!r}")
+    if outer_recon == "tol":
+        recon_steps, recon_tol = 40, True
+    elif outer_recon == "none":
+        recon_steps, recon_tol = 0, False
+    elif isinstance(outer_recon, int) and outer_recon >= 0:
+        recon_steps, recon_tol = outer_recon, False
+    else:
+        raise _lib.UboltError(1, f"outer_recon is 'tol', 'none' or a step count, was given {outer_recon!r}")
+    moments = outer_store == "moments"
     inner_rtol = solver.opts.rtol
     if outer_rtol < inner_rtol:
         raise _lib.UboltError(1, f"outer_rtol {outer_rtol:g} is below the solver's rtol {inner_rtol:g}: a warm start "
                                  "that moves by less than its rtol takes no iterations and the outer test would pass "
                                  "falsely")
-    psis = [ctx.vector(fill=0.0) for _ in range(G)]
+    if moments:
+        # One psi for every solve, the three reconstruction vectors, and each
+        # thermal group's current
+        one = ctx.vector(fill=0.0)
+        psis = [one] * G
+        rv, tv, dz = (ctx.vector() for _ in range(3)) if recon_steps > 0 else (None, None, None)
+        cur = [torch.zeros(ctx.n_nodes, ctx.geometry.dim, dtype=torch.float64, device=ctx.device)
+               for _ in range(G)]
+        op = TransportOperator(ctx)
+        sw = Sweep.__new__(Sweep)
+        sw.ctx = ctx
+    else:
+        psis = [ctx.vector(fill=0.0) for _ in range(G)]
     for g in range(g_up, G):
         transfer.phi[g] = torch.zeros(ctx.n_nodes, dtype=torch.float64, device=ctx.device)
     new_phi = torch.empty(ctx.n_nodes, dtype=torch.float64, device=ctx.device)
     stats = [None] * G
     outer_change, final_sweep, converged = 0.0, False, False
     changes, inner_its = [], 0
+    recon = {"steps": 0, "solves": 0, "safeguarded": 0}
     err = float("inf")
+
+    def reconstruct(g, rtol):
+        """The moments store's starting psi for thermal group g (into psis[g]):
+        Reconstruct, tests/transportk.kokkos.cxx:282-334."""
+        psi = psis[g]
+        expand_p1(ctx, transfer.phi[g], cur[g], psi)
+        recon["solves"] += 1
+        if recon_steps == 0:
+            return
+        # r = c - L psi, c = b + the within-group scatter at the last phi
+        rv.copy_(b)
+        transfer.add_transfer(g, g, rv)
+        target = rtol * float(torch.linalg.norm(rv)) if recon_tol else -1.0
+        op.mult_unscattered(psi, tv)
+        rv.sub_(tv)
+        r_norm = float(torch.linalg.norm(rv))
+        k = 0
+        while k < recon_steps and r_norm > target:
+            sw.apply(rv, dz)          # dz = L^{-1} r (r is rebuilt below)
+            k += 1
+            torch.add(psi, dz, out=tv)
+            op.mult_unscattered(tv, rv)
+            torch.sub(b, rv, out=rv)
+            transfer.add_transfer(g, g, rv)
+            new_norm = float(torch.linalg.norm(rv))
+            if not new_norm < r_norm:  # NaN too: the step is dropped
+                recon["safeguarded"] += 1
+                break
+            psi.copy_(tv)
+            r_norm = new_norm
+        recon["steps"] += k
+
     try:
         for outer in range(outer_max_it):
             sweep_rtol = inner_rtol
@@ -434,7 +516,11 @@ def solve_groups(ctx, sigma_t, sigma_s, source, side_inflow=None, dsa=None, keep
                 thermal = g >= g_up
                 rhs(g, thermal)
                 solver.opts.rtol = sweep_rtol if thermal else inner_rtol
-                psis[g], s = solver.solve(b, psis[g], x_zero=(outer == 0))
+                if moments and thermal and outer >= 1:
+                    reconstruct(g, solver.opts.rtol)
+                # From the second pass a thermal solve starts from its last psi
+                # (angular) or the reconstruction (moments); the first from zero
+                psis[g], s = solver.solve(b, psis[g], x_zero=(outer == 0 or not thermal))
                 stats[g] = s
                 inner_its += s["iterations"]
                 if thermal:
@@ -442,6 +528,8 @@ def solve_groups(ctx, sigma_t, sigma_s, source, side_inflow=None, dsa=None, keep
                     sums[0] += torch.sum((new_phi - transfer.phi[g]) ** 2)
                     sums[1] += torch.sum(new_phi * new_phi)
                     transfer.phi[g].copy_(new_phi)
+                    if moments:
+                        current(ctx, psis[g], cur[g])
                 else:
                     transfer.set_scalar_flux(g, psis[g])
             change_sq, norm_sq = sums.tolist()
@@ -460,7 +548,9 @@ def solve_groups(ctx, sigma_t, sigma_s, source, side_inflow=None, dsa=None, keep
         solver.opts.rtol = inner_rtol
     if outer_info is not None:
         outer_info.update(upscatter=True, g_up=g_up, outer_iterations=len(changes), changes=changes,
-                          error_estimate=err, inner_iterations=inner_its, converged=converged)
+                          error_estimate=err, inner_iterations=inner_its, converged=converged, store=outer_store,
+                          reconstruction_steps=recon["steps"], reconstructed_solves=recon["solves"],
+                          reconstruction_safeguarded=recon["safeguarded"])
     if not converged:
         raise _lib.UboltError(5, f"outer iteration not converged after {len(changes)} passes: error estimate "
                                  f"{err:.3e}, outer_rtol {outer_rtol:g}")
