@@ -505,3 +505,28 @@ def test_current_and_p1_expansion_round_trip(case):
     Jx = T.current(ctx, dev(x)).cpu().numpy()
     assert np.abs(Jx - (x.reshape(nn, A) * q.w) @ om).max() <= 1e-12 * np.abs(x).max() * q.sum_weights
     ctx.close()
+
+
+def test_sweep_kernel_choice_is_checked():
+    """An unknown kernel id is an argument error; the wave kernel where an
+    ordinate's upwind graph has a cycle (jittered tets) is a state error, and
+    the task kernel keeps running there."""
+    from ubolt_b200 import _lib
+    rng = np.random.default_rng(4)
+    mesh = P.box_tets(3, 3, 3, jitter=0.25, rng=rng)
+    g = P.build_geometry(mesh, 1)
+    q = P.lqn(3, 4)
+    st = rng.uniform(0.5, 2.0, g.n_cells)
+    ctx, keep = ctx_for(g, q, st, np.zeros(g.n_cells))
+    sw = T.Sweep(ctx)
+    with pytest.raises(_lib.UboltError) as e:
+        _lib.check(_lib.lib.ubolt_sweep_set_kernel(ctx.handle, 7))
+    assert e.value.status == 1
+    if not _lib.wave_plan(g, q)["acyclic"]:
+        with pytest.raises(_lib.UboltError) as e:
+            sw.set_kernel("wave")
+        assert e.value.status == 4
+    sw.set_kernel("tasks")
+    psi = sw.apply(dev(rng.standard_normal(ctx.n_rows)))
+    assert torch.isfinite(psi).all() and sw.status()["kernel"] == _lib.SWEEP_TASKS
+    ctx.close()
