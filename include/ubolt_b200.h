@@ -138,6 +138,94 @@ int ubolt_ctx_destroy(ubolt_ctx *ctx);
 int ubolt_ctx_sizes(const ubolt_ctx *ctx, int64_t *rows, int64_t *nodes, int64_t *cells, int32_t *n_basis,
                     int32_t *n_angles);
 
+/* ~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~
+ * The CG-SUPG backend (include/ubolt/unstructured_cg.hpp:11-263): continuous
+ * P1 (triangles, tetrahedra) or Q1 (quadrilaterals, hexahedra) Galerkin with
+ * consistent SUPG, one unknown per (VERTEX, ordinate). A context created by
+ * ubolt_ctx_create_cg has n_basis 1, nodes = the mesh's vertices (rows =
+ * vertex * n_angles + angle) and cells = the mesh's ELEMENTS, the unit cross
+ * sections, sources and materials are given on. Its row (i, a) is divided by
+ * the lumped mass m_i and reads
+ *   1/m_i sum_{e in star(i)} sum_j [Omega.G_ij + tau Omega Omega : K_ij
+ *                                   + sigma_t (M_ij + tau Omega.G_ji)] psi(j, a)
+ *   + per inflow boundary face |Omega . nA_f| / (m_i n_face_vertices) psi(i, a)
+ *     (minus the same at the mirrored ordinate on a reflective face)
+ *   - 1/m_i sum_e sigma_s / W sum_j (M_ij + tau Omega.G_ji) phi(j),
+ * tau = min(1 / sigma_t, 2 / (zeta sum_j |Omega . grad phi_j(x_c)|)) per
+ * (element, ordinate). On such a context:
+ *   ubolt_set_group        sigma_t, sigma_s per element
+ *   ubolt_apply[_f32], ubolt_apply_unscattered[_f32], ubolt_diagonal
+ *                          the operator above (SUPGTermCG + ScatteringTermCG,
+ *                          src/terms_cgk.kokkos.cxx:41-101, 203-221)
+ *   ubolt_block_setup / ubolt_block_apply[_f32]
+ *                          point Jacobi, the element-block inverse at one dof
+ *                          per vertex
+ *   ubolt_add_source       q per element, SUPG-weighted (UboltFillSourceCG)
+ *   ubolt_add_transfer     phi_from per vertex, sigma_s(g'->g) per element,
+ *                          tau of the current group (GroupTransferCG)
+ *   ubolt_add_ghost_inflow the weak vacuum inflow (unstructured_cgk:508-520)
+ *   ubolt_scalar_flux, ubolt_current, ubolt_expand_p1   per vertex
+ *   ubolt_dsa_setup(ctx, NULL, opts) and the DSA calls: the CG weak
+ *                          diffusion operator on the vertices (DSACG,
+ *                          src/dsa_cgk.kokkos.cxx)
+ *   ubolt_solve            with UBOLT_PC_NONE, UBOLT_PC_BLOCK or
+ *                          UBOLT_PC_BLOCK_DSA
+ * The sweep, the transpose and the gradient give UBOLT_ERR_STATE: the SUPG
+ * operator is neither block lower-triangular in any ordering nor
+ * adjoint-consistent (unstructured_cg.hpp:73-74).
+ * ~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~ */
+typedef struct {
+   int32_t dim;                    /* 2 or 3 */
+   int32_t n_element_vertices;     /* nv: 3 / 4 (tri / quad), 4 / 8 (tet / hex) */
+   int32_t faces_per_element;      /* F */
+   int32_t pad_;
+   int64_t n_vertices, n_elements, n_star, n_bfaces;
+   const int64_t *elem_vertex;     /* [n_elements * nv] the vertex of each basis function */
+   const double *mass;             /* [n_elements * nv * nv] M_ij = int phi_i phi_j */
+   const double *grad;             /* [n_elements * nv * nv * 3] G^d_ij = int phi_i d_d phi_j */
+   const double *stiff;            /* [n_elements * nv * nv * 9] K^{dd'}_ij = int d_d phi_i d_d' phi_j */
+   const double *centre_grad;      /* [n_elements * nv * 3] grad phi_j at the reference centroid */
+   const double *volume;           /* [n_elements] */
+   const double *centroid;         /* [n_elements * 3] */
+   const double *lumped_mass;      /* [n_vertices] m_i = sum_e sum_j M_ij */
+   const double *vertex_coord;     /* [n_vertices * 3] */
+   const int64_t *star_offset;     /* [n_vertices + 1] CSR over each vertex's elements */
+   const int64_t *star_elem;       /* [n_star] */
+   const int32_t *star_li;         /* [n_star] the vertex's basis index in that element */
+   const int64_t *bface_offset;    /* [n_vertices + 1] CSR over each vertex's boundary faces */
+   const double *bface_nA;         /* [n_bfaces * 3] outward area-weighted normal */
+   const double *bface_mass;       /* [n_bfaces] 1 / (m_i n_face_vertices) */
+   const int32_t *bface_side;      /* [n_bfaces] box side 2 * axis + (0 low | 1 high) */
+   const int32_t *bface_bc;        /* [n_bfaces] UBOLT_BC_* of that side */
+   const int64_t *elem_face_neighbour; /* [n_elements * F] the element across, -1 on the boundary */
+   const double *elem_face_area;   /* [n_elements * F] */
+   const int32_t *elem_face_bc;    /* [n_elements * F] UBOLT_BC_* on the boundary, -1 inside */
+} ubolt_cg_geometry;
+
+typedef struct ubolt_cg_geometry_owned ubolt_cg_geometry_owned;
+
+/* The CG-SUPG tables of a conforming one-shape mesh (the same vertex and cell
+ * layouts as ubolt_geometry_build; the basis functions follow the cell's
+ * vertex order). Simplices are integrated in closed form (affine: every
+ * table is a polynomial), quads and hexes by the tensor 4-point
+ * Gauss-Legendre rule. Reflective sides must be axis-aligned. Restates
+ * UnstructuredCG::build_element_tables and ::create
+ * (src/unstructured_cgk.kokkos.cxx:52-255, 276-561) with this library's own
+ * face matching in place of DMPlex. */
+int ubolt_cg_geometry_build(int dim, int cell_type, int64_t n_vertices, const double *vertices, int64_t n_elements,
+                            const int64_t *cell_vertices, const int32_t *side_bc, ubolt_cg_geometry_owned **out);
+int ubolt_cg_geometry_view(const ubolt_cg_geometry_owned *g, ubolt_cg_geometry *view);
+void ubolt_cg_geometry_free(ubolt_cg_geometry_owned *g);
+
+/* Upload the CG tables and ordinates; zeta > 0 is the thin-cell SUPG
+ * parameter (0.5 in the reference). Replaces the device half of
+ * UnstructuredCG::create (src/unstructured_cgk.kokkos.cxx:592-616) and the
+ * CG term creates (src/terms_cgk.kokkos.cxx:8-27, 157-183). */
+int ubolt_ctx_create_cg(const ubolt_cg_geometry *geom, const ubolt_quadrature *quad, double zeta, ubolt_ctx **ctx);
+
+/* 1 for a CG-SUPG context, 0 for a DG one. */
+int ubolt_ctx_is_cg(const ubolt_ctx *ctx);
+
 /* Point the operator at a group's cross sections: DEVICE arrays of n_cells
  * doubles, not owned, which must outlive their use (RemovalTerm::set_group /
  * ScatteringTerm::set_group, src/termsk.kokkos.cxx:437-443, 574-579;
@@ -374,7 +462,10 @@ void ubolt_dsa_defaults(ubolt_dsa_options *opts);
 /* Keep the host geometry the diffusion operator is built from and allocate
  * its device storage (DSAPrecon::create on an UnstructuredDG,
  * src/dsak.kokkos.cxx:113-121, src/dsa_plexk.kokkos.cxx:68-209). The
- * geometry must be the context's. */
+ * geometry must be the context's. On a CG-SUPG context pass NULL: the
+ * context holds the tables, and the operator is DSACG's weak form on the
+ * vertices (src/dsa_cgk.kokkos.cxx:114-203), R scaled by the lumped mass,
+ * no masking (an unbridged void keeps the SUPG operator's own tensor D). */
 int ubolt_dsa_setup(ubolt_ctx *ctx, const ubolt_dg_geometry *geom, const ubolt_dsa_options *opts);
 /* Refill the diffusion matrix for the context's current group - host
  * assembly, then upload (DSAPrecon::set_group, src/dsak.kokkos.cxx:216-226:
@@ -429,7 +520,9 @@ int ubolt_dsa_matrix(ubolt_ctx *ctx, double *blocks);
 /* ~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~
  * The solve
  * ~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~ */
-enum { UBOLT_PC_NONE = 0, UBOLT_PC_BLOCK = 1, UBOLT_PC_SWEEP = 2, UBOLT_PC_SWEEP_DSA = 3 };
+/* UBOLT_PC_BLOCK_DSA: the element-block inverse, then the multiplicative
+ * DSA stage (the preconditioner of a backend without a sweep: CG-SUPG). */
+enum { UBOLT_PC_NONE = 0, UBOLT_PC_BLOCK = 1, UBOLT_PC_SWEEP = 2, UBOLT_PC_SWEEP_DSA = 3, UBOLT_PC_BLOCK_DSA = 4 };
 enum { UBOLT_PRECISION_FP64 = 0, UBOLT_PRECISION_MIXED = 1 };
 /* UBOLT_KRYLOV_AUTO: with the sweep preconditioner and an exact sweep (no
  * reflective side, no lagged coupling), A M^{-1} = I - S L^{-1}, and every

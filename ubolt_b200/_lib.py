@@ -47,6 +47,17 @@ class DGGeometry(C.Structure):
                 ("face_neighbour_grad", dp), ("face_basis_value", dp)]
 
 
+class CGGeometry(C.Structure):
+    _fields_ = [("dim", C.c_int32), ("n_element_vertices", C.c_int32), ("faces_per_element", C.c_int32),
+                ("pad_", C.c_int32), ("n_vertices", C.c_int64), ("n_elements", C.c_int64), ("n_star", C.c_int64),
+                ("n_bfaces", C.c_int64),
+                ("elem_vertex", i64p), ("mass", dp), ("grad", dp), ("stiff", dp), ("centre_grad", dp),
+                ("volume", dp), ("centroid", dp), ("lumped_mass", dp), ("vertex_coord", dp),
+                ("star_offset", i64p), ("star_elem", i64p), ("star_li", i32p),
+                ("bface_offset", i64p), ("bface_nA", dp), ("bface_mass", dp), ("bface_side", i32p),
+                ("bface_bc", i32p), ("elem_face_neighbour", i64p), ("elem_face_area", dp), ("elem_face_bc", i32p)]
+
+
 class Quadrature(C.Structure):
     _fields_ = [("dim", C.c_int32), ("n_angles", C.c_int32), ("sum_weights", C.c_double),
                 ("omega", dp), ("w", dp), ("reflect", i32p)]
@@ -68,6 +79,11 @@ _sig("ubolt_geometry_build", C.c_int, C.c_int, C.c_int, C.c_int64, dp, C.c_int64
 _sig("ubolt_geometry_view", C.c_int, vp, C.POINTER(DGGeometry))
 _sig("ubolt_geometry_free", None, vp)
 _sig("ubolt_ctx_create", C.c_int, C.POINTER(DGGeometry), C.POINTER(Quadrature), C.POINTER(vp))
+_sig("ubolt_cg_geometry_build", C.c_int, C.c_int, C.c_int, C.c_int64, dp, C.c_int64, i64p, i32p, C.POINTER(vp))
+_sig("ubolt_cg_geometry_view", C.c_int, vp, C.POINTER(CGGeometry))
+_sig("ubolt_cg_geometry_free", None, vp)
+_sig("ubolt_ctx_create_cg", C.c_int, C.POINTER(CGGeometry), C.POINTER(Quadrature), C.c_double, C.POINTER(vp))
+_sig("ubolt_ctx_is_cg", C.c_int, vp)
 _sig("ubolt_ctx_destroy", C.c_int, vp)
 _sig("ubolt_ctx_sizes", C.c_int, vp, i64p, i64p, i64p, i32p, i32p)
 _sig("ubolt_set_group", C.c_int, vp, vp, vp, vp)
@@ -111,7 +127,7 @@ class SolveStats(C.Structure):
                 ("residual", C.c_double), ("rnorm0", C.c_double), ("seconds", C.c_double)]
 
 
-PC_NONE, PC_BLOCK, PC_SWEEP, PC_SWEEP_DSA = 0, 1, 2, 3
+PC_NONE, PC_BLOCK, PC_SWEEP, PC_SWEEP_DSA, PC_BLOCK_DSA = 0, 1, 2, 3, 4
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 
 _sig("ubolt_sweep_setup", C.c_int, vp, C.c_int)
@@ -231,7 +247,7 @@ class DsaOptions(C.Structure):
 
 
 _sig("ubolt_dsa_defaults", None, C.POINTER(DsaOptions))
-_sig("ubolt_dsa_setup", C.c_int, vp, C.POINTER(DGGeometry), C.POINTER(DsaOptions))
+_sig("ubolt_dsa_setup", C.c_int, vp, C.c_void_p, C.POINTER(DsaOptions))
 _sig("ubolt_dsa_set_group", C.c_int, vp, vp)
 _sig("ubolt_dsa_void_info", C.c_int, vp, i64p, C.POINTER(C.c_int32), dp)
 _sig("ubolt_dsa_apply", C.c_int, vp, vp, vp, vp)

@@ -71,6 +71,7 @@ extern "C" int ubolt_add_response_source(ubolt_ctx *ctx, const double *detector,
    int rc = CheckReady(ctx, false);
    if (rc) return rc;
    if (!detector || !g) return SetError(UBOLT_ERR_ARG, "add_response_source: NULL array");
+   if ((rc = RequireDg(ctx, "add_response_source"))) return rc;
    ResponseSourceKernel<<<RunGrid(ctx->n_cells), 256, 0, (cudaStream_t)stream>>>(ctx->g64, ctx->d_volume, detector,
                                                                                  g);
    return CheckLaunch("add_response_source");
@@ -82,6 +83,7 @@ extern "C" int ubolt_gradient(ubolt_ctx *ctx, const double *psi, const double *l
    int rc = CheckReady(ctx, false);
    if (rc) return rc;
    if (!psi || !lambda || (!grad_sigma_t && !grad_sigma_s)) return SetError(UBOLT_ERR_ARG, "gradient: NULL array");
+   if ((rc = RequireDg(ctx, "the gradient"))) return rc;
    GradientKernel<<<RunGrid(ctx->n_cells), 256, 0, (cudaStream_t)stream>>>(ctx->g64, psi, lambda, grad_sigma_t,
                                                                             grad_sigma_s);
    return CheckLaunch("gradient");

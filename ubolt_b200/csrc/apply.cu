@@ -29,6 +29,7 @@
 // Adjoint ((L - S)^T): a column also needs the NEIGHBOUR's shape data (its
 // face slot and matrix for the shared face), so that kernel gathers class
 // data straight from L1/L2, one thread per (cell, ordinate).
+#include "cg.h"
 #include "ctx.h"
 
 #include <cstdlib>
@@ -633,6 +634,10 @@ static int Apply(ubolt_ctx *ctx, const T *x, T *y, int mode, void *stream)
    if (rc) return rc;
    if (!x || !y || (const void *)x == (const void *)y)
       return SetError(UBOLT_ERR_ARG, "apply: x and y must be distinct device arrays");
+   if (ctx->cg) {
+      if (mode == kAdjoint) return RequireDg(ctx, "the transpose apply");
+      return CgApply<T>(ctx, x, y, mode == kFull, stream);
+   }
    const DevGeom<T> &g = ctx->geom<T>();
    cudaStream_t s = (cudaStream_t)stream;
    UBOLT_DISPATCH(ctx->nb, ctx->F, return (LaunchApply<T, NB_, F_>(ctx, g, x, y, mode, s)));
@@ -673,6 +678,7 @@ extern "C" int ubolt_diagonal(ubolt_ctx *ctx, double *d, void *stream)
    int rc = CheckReady(ctx, true);
    if (rc) return rc;
    if (!d) return SetError(UBOLT_ERR_ARG, "diagonal: d is NULL");
+   if (ctx->cg) return CgDiagonal(ctx, d, stream);
    const DevGeom<double> &g = ctx->geom<double>();
    UBOLT_DISPATCH(ctx->nb, ctx->F, return (LaunchDiagonal<double, NB_, F_>(g, d, (cudaStream_t)stream)));
    return SetError(UBOLT_ERR_STATE, "no kernel for n_basis %d with %d faces", ctx->nb, ctx->F);

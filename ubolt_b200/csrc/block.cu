@@ -3,6 +3,7 @@
 // registers. ElementBlockInverse (src/block_inversek.kokkos.cxx) stores
 // n_cells * A * nb^2 inverted blocks instead - 86 GB at 128^3 hexes, S8, FP64 -
 // and reads them on every apply.
+#include "cg.h"
 #include "ctx.h"
 
 namespace ubolt {
@@ -84,6 +85,10 @@ int BlockApply(ubolt_ctx *ctx, const T *x, T *y, bool trans, void *stream)
    if (rc) return rc;
    if (!x || !y || (const void *)x == (const void *)y)
       return SetError(UBOLT_ERR_ARG, "block apply: x and y must be distinct device arrays");
+   if (ctx->cg) {
+      if (trans) return RequireDg(ctx, "the transposed block apply");
+      return CgJacobiApply<T>(ctx, x, y, stream);
+   }
    UBOLT_DISPATCH(ctx->nb, ctx->F,
                   return (LaunchBlockApply<T, NB_, F_>(ctx->geom<T>(), x, y, trans, (cudaStream_t)stream)));
    return SetError(UBOLT_ERR_STATE, "no kernel for this shape");
@@ -113,6 +118,7 @@ extern "C" int ubolt_block_setup(ubolt_ctx *ctx, int64_t *n_singular, void *stre
 {
    int rc = CheckReady(ctx, true);
    if (rc) return rc;
+   if (ctx->cg) return CgJacobiSetup(ctx, n_singular, stream);
    unsigned long long *d = ctx->d_counters, h = 0;
    cudaStream_t s = (cudaStream_t)stream;
    cudaMemsetAsync(d, 0, sizeof *d, s);
@@ -132,6 +138,7 @@ extern "C" int ubolt_block_inverse(ubolt_ctx *ctx, double *inv, void *stream)
    int rc = CheckReady(ctx, true);
    if (rc) return rc;
    if (!inv) return SetError(UBOLT_ERR_ARG, "block_inverse: NULL output");
+   if ((rc = RequireDg(ctx, "block_inverse"))) return rc;
    const int64_t n = ctx->n_cells * ctx->A;
    cudaStream_t s = (cudaStream_t)stream;
    UBOLT_DISPATCH(ctx->nb, ctx->F, (BlockInverseKernel<double, NB_, F_><<<(n + 255) / 256, 256, 0, s>>>(ctx->g64, inv)));

@@ -40,6 +40,14 @@ int CheckReady(const ubolt_ctx *ctx, bool need_group)
    return UBOLT_OK;
 }
 
+int RequireDg(const ubolt_ctx *ctx, const char *what)
+{
+   if (ctx && ctx->cg)
+      return SetError(UBOLT_ERR_STATE, "%s is not defined on the CG-SUPG backend (no upwind sweep, no transpose)",
+                      what);
+   return UBOLT_OK;
+}
+
 int CtxAlloc(ubolt_ctx *ctx, size_t bytes, void **p)
 {
    *p = nullptr;
@@ -87,6 +95,106 @@ __global__ void ToFloatKernel(const T *__restrict__ in, float *__restrict__ out,
 {
    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
    if (i < n) out[i] = (float)in[i];
+}
+
+// The ordinates in both precisions (omega, w, the reflection maps), the
+// opposite of each ordinate, the P1 expansion's tables, the per-group FP32
+// cross-section slots (n_cells each) and the set-up counters: what every
+// context holds whatever its discretisation.
+int UploadOrdinates(ubolt_ctx *ctx, const ubolt_quadrature *quad)
+{
+   const int A = quad->n_angles, dim = ctx->dim;
+   int rc = 0;
+   DevGeom<double> &g = ctx->g64;
+   DevGeom<float> &h = ctx->g32;
+   ctx->h_omega.assign(quad->omega, quad->omega + 3 * A);
+   ctx->h_w.assign(quad->w, quad->w + A);
+   ctx->h_refl.assign(3 * A, 0);
+   for (int d = 0; d < 3 * A; d++) ctx->h_refl[d] = (d < dim * A) ? quad->reflect[d] : 0;
+   for (int d = 0; d < dim * A; d++)
+      if (ctx->h_refl[d] < 0 || ctx->h_refl[d] >= A) return SetError(UBOLT_ERR_ARG, "bad reflection map");
+   if ((rc = Upload(ctx, ctx->h_omega, &g.omega)) || (rc = Upload(ctx, ToF32(ctx->h_omega), &h.omega))) return rc;
+   if ((rc = Upload(ctx, ctx->h_w, &g.w)) || (rc = Upload(ctx, ToF32(ctx->h_w), &h.w))) return rc;
+   if ((rc = Upload(ctx, ctx->h_refl, &g.refl))) return rc;
+   h.refl = g.refl;
+   void *p = nullptr;
+   if ((rc = CtxAlloc(ctx, ctx->n_cells * sizeof(float), &p))) return rc;
+   ctx->sigma_t32 = static_cast<float *>(p);
+   if ((rc = CtxAlloc(ctx, ctx->n_cells * sizeof(float), &p))) return rc;
+   ctx->sigma_s32 = static_cast<float *>(p);
+   h.sigma_t = ctx->sigma_t32;
+   h.sigma_s = ctx->sigma_s32;
+   {
+      // The opposite ordinate (every cosine negated), by exact search
+      std::vector<int32_t> opp(A, -1);
+      for (int a = 0; a < A; a++)
+         for (int b = 0; b < A; b++)
+            if (ctx->h_omega[3 * b] == -ctx->h_omega[3 * a] && ctx->h_omega[3 * b + 1] == -ctx->h_omega[3 * a + 1] &&
+                ctx->h_omega[3 * b + 2] == -ctx->h_omega[3 * a + 2]) {
+               opp[a] = b;
+               break;
+            }
+      for (int a = 0; a < A; a++)
+         if (opp[a] < 0 || ctx->h_w[opp[a]] != ctx->h_w[a])
+            return SetError(UBOLT_ERR_ARG, "ordinate %d has no opposite of equal weight", a);
+      if ((rc = Upload(ctx, opp, &ctx->d_opp))) return rc;
+      g.opp = h.opp = ctx->d_opp;
+      ctx->h_opp = opp;
+   }
+   {
+      // The P1 expansion's tables: w_a Omega_a, and p1(a) = T^{-1} Omega_a
+      // with T = sum_a w_a Omega_a Omega_a^T, inverted by Gauss-Jordan
+      // (dim <= 3); usable where sum_a w_a Omega_a vanishes
+      const int D = ctx->dim;
+      double t[3][3] = {}, first[3] = {}, inv[3][3] = {};
+      for (int a = 0; a < A; a++)
+         for (int d = 0; d < D; d++) {
+            first[d] += ctx->h_w[a] * ctx->h_omega[3 * a + d];
+            for (int e = 0; e < D; e++) t[d][e] += ctx->h_w[a] * ctx->h_omega[3 * a + d] * ctx->h_omega[3 * a + e];
+         }
+      bool ok = true;
+      for (int d = 0; d < D; d++) ok &= std::fabs(first[d]) <= 1e-12 * std::fabs(ctx->sum_weights);
+      for (int d = 0; d < D; d++) inv[d][d] = 1.0;
+      for (int k = 0; k < D && ok; k++) {
+         int piv = k;
+         for (int i = k + 1; i < D; i++)
+            if (std::fabs(t[i][k]) > std::fabs(t[piv][k])) piv = i;
+         if (!(std::fabs(t[piv][k]) > 0.0)) {
+            ok = false;
+            break;
+         }
+         for (int j = 0; j < 3; j++) {
+            std::swap(t[k][j], t[piv][j]);
+            std::swap(inv[k][j], inv[piv][j]);
+         }
+         const double r = 1.0 / t[k][k];
+         for (int j = 0; j < D; j++) {
+            t[k][j] *= r;
+            inv[k][j] *= r;
+         }
+         for (int i = 0; i < D; i++) {
+            if (i == k) continue;
+            const double f = t[i][k];
+            for (int j = 0; j < D; j++) {
+               t[i][j] -= f * t[k][j];
+               inv[i][j] -= f * inv[k][j];
+            }
+         }
+      }
+      std::vector<double> p1((size_t)A * D, 0.0), wom((size_t)A * D, 0.0);
+      for (int a = 0; a < A; a++)
+         for (int d = 0; d < D; d++) {
+            wom[(size_t)a * D + d] = ctx->h_w[a] * ctx->h_omega[3 * a + d];
+            double sum = 0.0;
+            for (int e = 0; e < D; e++) sum += inv[d][e] * ctx->h_omega[3 * a + e];
+            p1[(size_t)a * D + d] = sum;
+         }
+      if ((rc = Upload(ctx, p1, &ctx->d_p1)) || (rc = Upload(ctx, wom, &ctx->d_w_omega))) return rc;
+      ctx->p1_ok = ok;
+   }
+   if ((rc = CtxAlloc(ctx, 64 * sizeof(unsigned long long), &p))) return rc;
+   ctx->d_counters = static_cast<unsigned long long *>(p);
+   return UBOLT_OK;
 }
 
 }  // namespace ubolt
@@ -221,14 +329,6 @@ extern "C" int ubolt_ctx_create(const ubolt_dg_geometry *geom, const ubolt_quadr
    ctx->h_volume.assign(geom->volume, geom->volume + nc);
    ctx->h_nA.assign(geom->face_nA, geom->face_nA + nc * s_nA);
 
-   // ~~~~~ Quadrature
-   ctx->h_omega.assign(quad->omega, quad->omega + 3 * A);
-   ctx->h_w.assign(quad->w, quad->w + A);
-   ctx->h_refl.assign(3 * A, 0);
-   for (int d = 0; d < 3 * A; d++) ctx->h_refl[d] = (d < dim * A) ? quad->reflect[d] : 0;
-   for (int d = 0; d < dim * A; d++)
-      if (ctx->h_refl[d] < 0 || ctx->h_refl[d] >= A) return fail(SetError(UBOLT_ERR_ARG, "bad reflection map"));
-
    // ~~~~~ Upload, FP64 and FP32
    int rc = 0;
    DevGeom<double> &g = ctx->g64;
@@ -284,90 +384,10 @@ extern "C" int ubolt_ctx_create(const ubolt_dg_geometry *geom, const ubolt_quadr
    h.cls = g.cls;
    h.code = g.code;
    h.mirror = g.mirror;
-   if ((rc = Upload(ctx, ctx->h_omega, &g.omega)) || (rc = Upload(ctx, ToF32(ctx->h_omega), &h.omega))) return fail(rc);
-   if ((rc = Upload(ctx, ctx->h_w, &g.w)) || (rc = Upload(ctx, ToF32(ctx->h_w), &h.w))) return fail(rc);
-   if ((rc = Upload(ctx, ctx->h_refl, &g.refl))) return fail(rc);
-   h.refl = g.refl;
-   void *p = nullptr;
-   if ((rc = CtxAlloc(ctx, nc * sizeof(float), &p))) return fail(rc);
-   ctx->sigma_t32 = static_cast<float *>(p);
-   if ((rc = CtxAlloc(ctx, nc * sizeof(float), &p))) return fail(rc);
-   ctx->sigma_s32 = static_cast<float *>(p);
-   h.sigma_t = ctx->sigma_t32;
-   h.sigma_s = ctx->sigma_s32;
+   if ((rc = UploadOrdinates(ctx, quad))) return fail(rc);
    if ((rc = Upload(ctx, ctx->h_volume, &ctx->d_volume))) return fail(rc);
    g.volume = ctx->d_volume;
    if ((rc = Upload(ctx, ToF32(ctx->h_volume), &h.volume))) return fail(rc);
-   {
-      // The opposite ordinate (every cosine negated), by exact search
-      std::vector<int32_t> opp(A, -1);
-      for (int a = 0; a < A; a++)
-         for (int b = 0; b < A; b++)
-            if (ctx->h_omega[3 * b] == -ctx->h_omega[3 * a] && ctx->h_omega[3 * b + 1] == -ctx->h_omega[3 * a + 1] &&
-                ctx->h_omega[3 * b + 2] == -ctx->h_omega[3 * a + 2]) {
-               opp[a] = b;
-               break;
-            }
-      for (int a = 0; a < A; a++)
-         if (opp[a] < 0 || ctx->h_w[opp[a]] != ctx->h_w[a])
-            return fail(SetError(UBOLT_ERR_ARG, "ordinate %d has no opposite of equal weight", a));
-      if ((rc = Upload(ctx, opp, &ctx->d_opp))) return fail(rc);
-      g.opp = h.opp = ctx->d_opp;
-      ctx->h_opp = opp;
-   }
-   {
-      // The P1 expansion's tables: w_a Omega_a, and p1(a) = T^{-1} Omega_a
-      // with T = sum_a w_a Omega_a Omega_a^T, inverted by Gauss-Jordan
-      // (dim <= 3); usable where sum_a w_a Omega_a vanishes
-      const int D = ctx->dim;
-      double t[3][3] = {}, first[3] = {}, inv[3][3] = {};
-      for (int a = 0; a < A; a++)
-         for (int d = 0; d < D; d++) {
-            first[d] += ctx->h_w[a] * ctx->h_omega[3 * a + d];
-            for (int e = 0; e < D; e++) t[d][e] += ctx->h_w[a] * ctx->h_omega[3 * a + d] * ctx->h_omega[3 * a + e];
-         }
-      bool ok = true;
-      for (int d = 0; d < D; d++) ok &= std::fabs(first[d]) <= 1e-12 * std::fabs(ctx->sum_weights);
-      for (int d = 0; d < D; d++) inv[d][d] = 1.0;
-      for (int k = 0; k < D && ok; k++) {
-         int piv = k;
-         for (int i = k + 1; i < D; i++)
-            if (std::fabs(t[i][k]) > std::fabs(t[piv][k])) piv = i;
-         if (!(std::fabs(t[piv][k]) > 0.0)) {
-            ok = false;
-            break;
-         }
-         for (int j = 0; j < 3; j++) {
-            std::swap(t[k][j], t[piv][j]);
-            std::swap(inv[k][j], inv[piv][j]);
-         }
-         const double r = 1.0 / t[k][k];
-         for (int j = 0; j < D; j++) {
-            t[k][j] *= r;
-            inv[k][j] *= r;
-         }
-         for (int i = 0; i < D; i++) {
-            if (i == k) continue;
-            const double f = t[i][k];
-            for (int j = 0; j < D; j++) {
-               t[i][j] -= f * t[k][j];
-               inv[i][j] -= f * inv[k][j];
-            }
-         }
-      }
-      std::vector<double> p1((size_t)A * D, 0.0), wom((size_t)A * D, 0.0);
-      for (int a = 0; a < A; a++)
-         for (int d = 0; d < D; d++) {
-            wom[(size_t)a * D + d] = ctx->h_w[a] * ctx->h_omega[3 * a + d];
-            double sum = 0.0;
-            for (int e = 0; e < D; e++) sum += inv[d][e] * ctx->h_omega[3 * a + e];
-            p1[(size_t)a * D + d] = sum;
-         }
-      if ((rc = Upload(ctx, p1, &ctx->d_p1)) || (rc = Upload(ctx, wom, &ctx->d_w_omega))) return fail(rc);
-      ctx->p1_ok = ok;
-   }
-   if ((rc = CtxAlloc(ctx, 64 * sizeof(unsigned long long), &p))) return fail(rc);
-   ctx->d_counters = static_cast<unsigned long long *>(p);
    if ((rc = CudaCheck(cudaDeviceSynchronize(), "ctx_create"))) return fail(rc);
    *out = ctx;
    return UBOLT_OK;
@@ -376,6 +396,7 @@ extern "C" int ubolt_ctx_create(const ubolt_dg_geometry *geom, const ubolt_quadr
 void UboltSweepFree(ubolt_ctx *ctx);
 void UboltDsaFree(ubolt_ctx *ctx);
 void UboltSolverFree(ubolt_ctx *ctx);
+void UboltCgFree(ubolt_ctx *ctx);
 
 extern "C" uint64_t ubolt_launch_count(void) { return g_launches.load(); }
 
@@ -387,6 +408,7 @@ extern "C" int ubolt_ctx_destroy(ubolt_ctx *ctx)
    UboltSolverFree(ctx);
    UboltDsaFree(ctx);
    UboltSweepFree(ctx);
+   UboltCgFree(ctx);
    for (void *p : ctx->owned) cudaFree(p);
    delete ctx;
    return UBOLT_OK;

@@ -12,6 +12,7 @@
 struct ubolt_sweep_plan;
 struct ubolt_dsa;
 struct ubolt_solver;
+struct ubolt_cg;
 
 struct ubolt_ctx {
    int device = 0;
@@ -32,7 +33,7 @@ struct ubolt_ctx {
    ubolt::DevGeom<double> g64{};
    ubolt::DevGeom<float> g32{};
    float *sigma_t32 = nullptr, *sigma_s32 = nullptr;
-   const double *d_volume = nullptr;           // [n_cells] FP64 cell volumes
+   const double *d_volume = nullptr;           // [n_cells] FP64 cell volumes (CG-SUPG: [n_nodes] lumped masses)
    const int32_t *d_opp = nullptr;             // [A] the ordinate opposite each ordinate
    const double *d_p1 = nullptr;               // [A][dim] T^{-1} Omega_a, T = sum_a w_a Omega_a Omega_a^T
    bool p1_ok = false;                         // sum_a w_a Omega_a = 0 and T regular (the P1 expansion exists)
@@ -44,6 +45,10 @@ struct ubolt_ctx {
    ubolt_sweep_plan *sweep = nullptr;
    ubolt_dsa *dsa = nullptr;
    ubolt_solver *solver = nullptr;
+   // The CG-SUPG backend's tables, or NULL for a DG context. A CG context's
+   // nodes are the mesh's vertices (nb 1) and its cells the elements, the
+   // unit cross sections are given on; the DG geometry above is unset.
+   ubolt_cg *cg = nullptr;
 
    template <typename T>
    const ubolt::DevGeom<T> &geom() const;
@@ -70,6 +75,12 @@ int CudaCheck(cudaError_t e, const char *what);
 int CheckReady(const ubolt_ctx *ctx, bool need_group);
 // Device allocation owned by the context, freed by ubolt_ctx_destroy
 int CtxAlloc(ubolt_ctx *ctx, size_t bytes, void **p);
+// The ordinates, the opposite map, the P1 tables, the FP32 cross-section
+// slots (ctx->n_cells each) and the counters; ctx->dim, n_cells and
+// sum_weights set first
+int UploadOrdinates(ubolt_ctx *ctx, const ubolt_quadrature *quad);
+// A context of the DG backend: UBOLT_ERR_STATE naming `what` on a CG-SUPG one
+int RequireDg(const ubolt_ctx *ctx, const char *what);
 
 }  // namespace ubolt
 

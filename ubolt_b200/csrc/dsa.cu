@@ -25,8 +25,18 @@
 // dsak.kokkos.cxx:197-212) with a fixed number of block-Jacobi PCG
 // iterations run entirely on the device (scalars stay in device memory, no
 // host round trip), in FP64 whatever the outer precision.
+//
+// On a CG-SUPG context the operator is DSACG's (src/dsa_cgk.kokkos.cxx): one
+// unknown per vertex, the weak form
+//    sum_e int_e D_e grad u . grad v + sigma_a u v + per vacuum face its
+//    incoming half-range current times the lumped face mass on the diagonal,
+// in CSR; R weighs by the lumped mass instead of the volume, P is the same,
+// nothing is masked, and an unbridged void keeps the SUPG operator's own
+// tensor D_e = (1/W) sum_a w_a tau_a Omega_a Omega_a^T (CGSupgDKernel, :66-84).
+#include "cg.h"
 #include "ctx.h"
 
+#include <algorithm>
 #include <cmath>
 #include <mutex>
 #include <vector>
@@ -52,8 +62,15 @@ struct ubolt_dsa {
    std::vector<int64_t> nbr;
    std::vector<int32_t> bc;
    std::vector<double> h_val, h_jinv;
+   // CG-SUPG: the vertex CSR, and per (element, li, j) its entry
+   bool cg = false;
+   std::vector<int64_t> rp, entry;
+   std::vector<int32_t> col;
+   std::vector<double> vacuum_weight;  // per vertex
+   int64_t *d_rp = nullptr;
+   int32_t *d_col = nullptr;
    // Device
-   double *val = nullptr, *jinv = nullptr;          // [nc][F+1][nb][nb], [nc][nb][nb]
+   double *val = nullptr, *jinv = nullptr;          // [nc][F+1][nb][nb], [nc][nb][nb] (CG: [nnz], [n_nodes])
    double *rhs = nullptr, *u = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *q = nullptr;
    // [0] rho, [1] rho_new, [2] pq, [3] the grid sums' block counter (an
    // unsigned int in a double's slot), then one partial per block
@@ -131,6 +148,34 @@ __global__ void DsaSpmvKernel(int64_t n_nodes, int nb, int F, const int32_t *__r
    }
    // scal[2] = (dotw, v), when asked
    if (scal) GridSum(d, scal + kDsaScalars, GridCount(scal), &scal[2]);
+}
+
+// v = D u over CSR rows (the CG-SUPG vertices), one thread per row
+__global__ void DsaCsrSpmvKernel(int64_t n_nodes, const int64_t *__restrict__ rp, const int32_t *__restrict__ col,
+                                 const double *__restrict__ val, const double *__restrict__ u, double *__restrict__ v,
+                                 const double *__restrict__ dotw, double *scal)
+{
+   const int64_t node = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+   double d = 0.0;
+   if (node < n_nodes) {
+      double s = 0.0;
+      for (int64_t k = rp[node]; k < rp[node + 1]; k++) s += val[k] * u[col[k]];
+      v[node] = s;
+      if (dotw) d = dotw[node] * s;
+   }
+   if (scal) GridSum(d, scal + kDsaScalars, GridCount(scal), &scal[2]);
+}
+
+// v = D u in whichever storage the context's DSA has; with scal, also (dotw, v) into scal[2]
+static void DsaSpmvLaunch(const ubolt_ctx *ctx, const ubolt_dsa *ds, const double *u, double *v, const double *dotw,
+                          double *scal, cudaStream_t s)
+{
+   const int64_t grid = (ds->n_nodes + kDsaThreads - 1) / kDsaThreads;
+   if (ds->cg)
+      DsaCsrSpmvKernel<<<grid, kDsaThreads, 0, s>>>(ds->n_nodes, ds->d_rp, ds->d_col, ds->val, u, v, dotw, scal);
+   else
+      DsaSpmvKernel<<<grid, kDsaThreads, 0, s>>>(ds->n_nodes, ds->nb, ds->F, ctx->g64.code, ds->val, u, v, dotw,
+                                                 scal);
 }
 
 // rhs(node) = V_c sum_a w_a (x(node, a) - ax(node, a)); ax may be NULL. A
@@ -289,8 +334,10 @@ static double BlendD(double d, double m, double p)
 // The void policy for one group (DSAPrecon::assemble, dsak.kokkos.cxx:233-345,
 // with DSAPlex::void_volume_surface, dsa_plexk.kokkos.cxx:243-262): the
 // census, the bridge decision and the voids' mean chord, D per cell and the
-// mask, and the guard against a singular operator.
-static int VoidPolicy(ubolt_dsa *ds, const double *st, const double *ss)
+// mask, and the guard against a singular operator. A backend that cannot
+// mask (CG-SUPG) checks the guard first, without counting on a void, and
+// bridges whenever there is a void.
+static int VoidPolicy(ubolt_dsa *ds, const double *st, const double *ss, bool can_mask = true)
 {
    const int F = ds->F;
    const int64_t nc = ds->nc;
@@ -307,12 +354,17 @@ static int VoidPolicy(ubolt_dsa *ds, const double *st, const double *ss)
       else max_sa_solid = std::max(max_sa_solid, sa);
       max_sa_all = std::max(max_sa_all, sa);
    }
+   if (!can_mask && !(ds->any_vacuum || max_sa_all > 0.0))
+      return SetError(UBOLT_ERR_ARG,
+                      "the DSA diffusion operator is singular: every face is reflective and sigma_a = sigma_t - "
+                      "sigma_s is zero everywhere in this group");
    // Bridge when asked, some cell is void and some is not, and a vacuum face
    // or some absorption holds the bridged operator; bridged iff a face ends
    // a flight through the voids (their chord is positive)
    ds->bridged = 0;
    ds->chord = 0.0;
-   if (ds->void_bridge && n_void > 0 && n_void < nc && (ds->any_vacuum || max_sa_all > 0.0)) {
+   if (ds->void_bridge && n_void > 0 &&
+       (!can_mask || (n_void < nc && (ds->any_vacuum || max_sa_all > 0.0)))) {
       double vol = 0.0, surf = 0.0;
       for (int64_t c = 0; c < nc; c++) {
          if (!ds->h_void[c]) continue;
@@ -332,9 +384,10 @@ static int VoidPolicy(ubolt_dsa *ds, const double *st, const double *ss)
       if (!ds->h_void[c]) ds->h_d[c] = 1.0 / (3.0 * st[c]);
       else if (ds->bridged)
          ds->h_d[c] = ds->void_d > 0.0 ? ds->void_d : 1.0 / (3.0 * (std::max(st[c], 0.0) + 1.0 / ds->chord));
-      ds->h_mask[c] = ds->h_void[c] && !ds->bridged;
+      ds->h_mask[c] = can_mask && ds->h_void[c] && !ds->bridged;
    }
    ds->n_void = n_void;
+   if (!can_mask) return UBOLT_OK;
    // Every face reflective (pure Neumann): only absorption, or a masked void
    // (whose faces are Marshak faces), keeps the operator nonsingular
    const double sa = ds->bridged ? max_sa_all : max_sa_solid;
@@ -452,6 +505,61 @@ static int Assemble(ubolt_dsa *ds, const double *st, const double *ss)
    return UBOLT_OK;
 }
 
+// The CG-SUPG vertex operator for one group (DSACG::assemble,
+// dsa_cgk.kokkos.cxx:247-281): per element (sigma_t - sigma_s) M_ij + D_e : K_ij
+// into its (li, j) entries, D_e isotropic from the void policy or, in an
+// unbridged void, the SUPG operator's own tensor; then the vacuum faces on the
+// diagonal. Point-Jacobi inverses.
+static int AssembleCg(const ubolt_ctx *ctx, ubolt_dsa *ds, const double *st, const double *ss)
+{
+   const ubolt_cg *cg = ctx->cg;
+   int rc = VoidPolicy(ds, st, ss, false);
+   if (rc) return rc;
+   const int nv = cg->nv, A = ctx->A, dim = ctx->dim;
+   const int64_t ne = cg->n_elements;
+   const size_t n2 = (size_t)nv * nv;
+   ds->h_val.assign(ds->col.size(), 0.0);
+   std::vector<double> De(9);
+   for (int64_t e = 0; e < ne; e++) {
+      for (int k = 0; k < 9; k++) De[k] = (k % 4 == 0) ? ds->h_d[e] : 0.0;
+      if (ds->h_void[e] && !ds->bridged) {
+         // (1/W) sum_a w_a tau_a Omega_a Omega_a^T with the transport's own tau
+         for (int k = 0; k < 9; k++) De[k] = 0.0;
+         for (int a = 0; a < A; a++) {
+            const double *om = &ctx->h_omega[3 * a];
+            double sum = 0.0;
+            for (int j = 0; j < nv; j++) {
+               double s = 0.0;
+               for (int c = 0; c < dim; c++) s += om[c] * cg->centre_grad[(e * nv + j) * 3 + c];
+               sum += std::fabs(s);
+            }
+            const double thin = 2.0 / (cg->zeta * sum);
+            const double tau = st[e] > 0.0 ? std::min(1.0 / st[e], thin) : thin;
+            const double wt = ctx->h_w[a] * tau / ctx->sum_weights;
+            for (int c = 0; c < 3; c++)
+               for (int c2 = 0; c2 < 3; c2++) De[3 * c + c2] += wt * om[c] * om[c2];
+         }
+      }
+      const double sa = st[e] - ss[e];
+      for (size_t ij = 0; ij < n2; ij++) {
+         double v = sa * cg->mass[e * n2 + ij];
+         for (int k = 0; k < 9; k++) v += De[k] * cg->stiff[(e * n2 + ij) * 9 + k];
+         ds->h_val[ds->entry[e * n2 + ij]] += v;
+      }
+   }
+   ds->h_jinv.assign(ds->n_nodes, 0.0);
+   for (int64_t i = 0; i < ds->n_nodes; i++) {
+      double diag = 0.0;
+      for (int64_t k = ds->rp[i]; k < ds->rp[i + 1]; k++)
+         if (ds->col[k] == i) {
+            ds->h_val[k] += ds->vacuum_weight[i];
+            diag = ds->h_val[k];
+         }
+      ds->h_jinv[i] = diag != 0.0 ? 1.0 / diag : 0.0;
+   }
+   return UBOLT_OK;
+}
+
 int DsaSolveOnDevice(ubolt_ctx *ctx, cudaStream_t s)
 {
    ubolt_dsa *ds = ctx->dsa;
@@ -462,7 +570,7 @@ int DsaSolveOnDevice(ubolt_ctx *ctx, cudaStream_t s)
    CgStartKernel<<<grid, bl, 0, s>>>(nn, ds->nb, ds->jinv, ds->rhs, ds->u, ds->r, ds->z, ds->p, ds->scal);
    CountLaunch();
    for (int it = 0; it < ds->inner_its; it++) {
-      DsaSpmvKernel<<<grid, bl, 0, s>>>(nn, ds->nb, ds->F, ctx->g64.code, ds->val, ds->p, ds->q, ds->p, ds->scal);
+      DsaSpmvLaunch(ctx, ds, ds->p, ds->q, ds->p, ds->scal, s);
       CgUpdateKernel<<<grid, bl, 0, s>>>(nn, ds->p, ds->q, ds->u, ds->r, ds->scal);
       CgPrecondKernel<<<grid, bl, 0, s>>>(nn, ds->nb, ds->jinv, ds->r, ds->z, ds->scal);
       CgDirectionKernel<<<grid, bl, 0, s>>>(nn, ds->z, ds->p, ds->scal);
@@ -519,7 +627,8 @@ void UboltDsaFree(ubolt_ctx *ctx)
    ubolt_dsa *ds = ctx->dsa;
    if (!ds) return;
    for (void *p : {(void *)ds->val, (void *)ds->jinv, (void *)ds->rhs, (void *)ds->u, (void *)ds->r, (void *)ds->z,
-                   (void *)ds->p, (void *)ds->q, (void *)ds->scal, (void *)ds->mask})
+                   (void *)ds->p, (void *)ds->q, (void *)ds->scal, (void *)ds->mask, (void *)ds->d_rp,
+                   (void *)ds->d_col})
       if (p) cudaFree(p);
    delete ds;
    ctx->dsa = nullptr;
@@ -538,10 +647,129 @@ extern "C" void ubolt_dsa_defaults(ubolt_dsa_options *o)
    o->pad_ = 0;
 }
 
+// Device storage of one DSA: the operator's values (n_val), the Jacobi
+// inverses (n_jinv) and the inner solve's vectors and scalars
+static int AllocDsa(ubolt_dsa *ds, size_t n_val, size_t n_jinv)
+{
+   auto alloc = [&](double **p, size_t n) -> int {
+      const cudaError_t e = cudaMalloc((void **)p, std::max<size_t>(n, 1) * sizeof(double));
+      if (e != cudaSuccess) {
+         cudaGetLastError();
+         return SetError(UBOLT_ERR_NOMEM, "DSA workspace: %s", cudaGetErrorString(e));
+      }
+      return UBOLT_OK;
+   };
+   const size_t nn = (size_t)ds->n_nodes;
+   int rc = 0;
+   if ((rc = alloc(&ds->val, n_val)) || (rc = alloc(&ds->jinv, n_jinv)) || (rc = alloc(&ds->rhs, nn)) ||
+       (rc = alloc(&ds->u, nn)) || (rc = alloc(&ds->r, nn)) || (rc = alloc(&ds->z, nn)) || (rc = alloc(&ds->p, nn)) ||
+       (rc = alloc(&ds->q, nn)) || (rc = alloc(&ds->scal, kDsaScalars + (nn + kDsaThreads - 1) / kDsaThreads)))
+      return rc;
+   return UBOLT_OK;
+}
+
+// DSACG::create (dsa_cgk.kokkos.cxx:114-203) on the context's CG tables: the
+// vertex CSR pattern (each vertex's star vertices, sorted), the entry of
+// every (element, li, j), and each vertex's vacuum weight - over its vacuum
+// boundary faces, the incoming half-range current times A_f / n_fv
+static int CgDsaSetup(ubolt_ctx *ctx, const ubolt_dsa_options &o)
+{
+   UboltDsaFree(ctx);
+   auto ds = new ubolt_dsa();
+   ctx->dsa = ds;
+   const ubolt_cg *cg = ctx->cg;
+   const int nv = cg->nv, F = cg->F, A = ctx->A;
+   const int64_t ne = cg->n_elements, nvx = cg->n_vertices;
+   const size_t n2 = (size_t)nv * nv;
+   ds->cg = true;
+   ds->nb = 1;
+   ds->F = F;
+   ds->nc = ne;
+   ds->n_nodes = nvx;
+   ds->inner_its = o.inner_iterations;
+   ds->void_sigma_t = o.void_sigma_t;
+   ds->void_d = o.void_d;
+   ds->void_bridge = o.void_bridge != 0;
+   ds->volume = cg->volume;
+   ds->nbr = cg->elem_face_neighbour;
+   ds->bc = cg->elem_face_bc;
+   ds->area = cg->elem_face_area;
+   for (int64_t k = 0; k < ne * F; k++)
+      if (ds->nbr[k] < 0 && ds->bc[k] == UBOLT_BC_VACUUM) ds->any_vacuum = true;
+   std::vector<std::vector<int32_t>> cols(nvx);
+   for (int64_t e = 0; e < ne; e++)
+      for (int li = 0; li < nv; li++)
+         for (int j = 0; j < nv; j++) cols[cg->elem_vertex[e * nv + li]].push_back((int32_t)cg->elem_vertex[e * nv + j]);
+   ds->rp.assign(nvx + 1, 0);
+   for (int64_t i = 0; i < nvx; i++) {
+      std::sort(cols[i].begin(), cols[i].end());
+      cols[i].erase(std::unique(cols[i].begin(), cols[i].end()), cols[i].end());
+      ds->rp[i + 1] = ds->rp[i] + (int64_t)cols[i].size();
+   }
+   ds->col.resize(ds->rp[nvx]);
+   for (int64_t i = 0; i < nvx; i++) std::copy(cols[i].begin(), cols[i].end(), ds->col.begin() + ds->rp[i]);
+   ds->entry.resize(ne * n2);
+   for (int64_t e = 0; e < ne; e++)
+      for (int li = 0; li < nv; li++) {
+         const int64_t i = cg->elem_vertex[e * nv + li];
+         for (int j = 0; j < nv; j++) {
+            const int32_t c = (int32_t)cg->elem_vertex[e * nv + j];
+            ds->entry[e * n2 + li * nv + j] = std::lower_bound(cols[i].begin(), cols[i].end(), c) - cols[i].begin() +
+                                              ds->rp[i];
+         }
+      }
+   ds->vacuum_weight.assign(nvx, 0.0);
+   for (int64_t i = 0; i < nvx; i++)
+      for (int64_t f = cg->bface_offset[i]; f < cg->bface_offset[i + 1]; f++) {
+         if (cg->bface_bc[f] != UBOLT_BC_VACUUM) continue;
+         const double *nA = &cg->bface_nA[3 * f];
+         const double area = std::sqrt(nA[0] * nA[0] + nA[1] * nA[1] + nA[2] * nA[2]);
+         double m = 0.0;
+         for (int a = 0; a < A; a++) {
+            const double *om = &ctx->h_omega[3 * a];
+            const double cosv = -(om[0] * nA[0] + om[1] * nA[1] + om[2] * nA[2]) / area;
+            if (cosv > 0.0) m += ctx->h_w[a] * cosv;
+         }
+         m /= ctx->sum_weights;
+         ds->vacuum_weight[i] += m * cg->bface_mass[f] * cg->lumped[i] * area;
+      }
+   int rc = AllocDsa(ds, ds->col.size(), (size_t)nvx);
+   if (!rc && (cudaMalloc((void **)&ds->d_rp, ds->rp.size() * sizeof(int64_t)) != cudaSuccess ||
+               cudaMalloc((void **)&ds->d_col, std::max<size_t>(ds->col.size(), 1) * sizeof(int32_t)) != cudaSuccess)) {
+      cudaGetLastError();
+      rc = SetError(UBOLT_ERR_NOMEM, "DSA pattern");
+   }
+   if (!rc)
+      rc = CudaCheck(cudaMemcpy(ds->d_rp, ds->rp.data(), ds->rp.size() * sizeof(int64_t), cudaMemcpyHostToDevice),
+                     "dsa_setup");
+   if (!rc)
+      rc = CudaCheck(cudaMemcpy(ds->d_col, ds->col.data(), ds->col.size() * sizeof(int32_t), cudaMemcpyHostToDevice),
+                     "dsa_setup");
+   if (rc) UboltDsaFree(ctx);
+   return rc;
+}
+
+static int DsaOptions(const ubolt_dsa_options *opts, ubolt_dsa_options *o)
+{
+   ubolt_dsa_defaults(o);
+   if (opts) *o = *opts;
+   if (!(o->penalty > 0.0)) return SetError(UBOLT_ERR_ARG, "dsa penalty must be positive, got %g", o->penalty);
+   if (!(o->consistent_power >= 1.0)) return SetError(UBOLT_ERR_ARG, "consistent-D power must be >= 1");
+   if (o->inner_iterations < 1 || o->inner_iterations > 10000) return SetError(UBOLT_ERR_ARG, "inner iterations");
+   if (!(o->void_d >= 0.0)) return SetError(UBOLT_ERR_ARG, "void D must be >= 0 (0: from the voids' chord)");
+   return UBOLT_OK;
+}
+
 extern "C" int ubolt_dsa_setup(ubolt_ctx *ctx, const ubolt_dg_geometry *g, const ubolt_dsa_options *opts)
 {
    int rc = CheckReady(ctx, false);
    if (rc) return rc;
+   if (ctx->cg) {
+      if (g) return SetError(UBOLT_ERR_ARG, "dsa_setup: a CG-SUPG context holds its own tables - pass NULL");
+      ubolt_dsa_options o;
+      if ((rc = DsaOptions(opts, &o))) return rc;
+      return CgDsaSetup(ctx, o);
+   }
    if (!g) return SetError(UBOLT_ERR_ARG, "dsa_setup: NULL geometry");
    if (g->n_cells != ctx->n_cells || g->n_basis != ctx->nb || g->faces_per_cell != ctx->F)
       return SetError(UBOLT_ERR_ARG, "dsa_setup: the geometry is not the context's");
@@ -549,12 +777,7 @@ extern "C" int ubolt_dsa_setup(ubolt_ctx *ctx, const ubolt_dg_geometry *g, const
       return SetError(UBOLT_ERR_ARG, "dsa_setup: DG1 needs face matrices and basis gradients");
    if (!g->face_distance) return SetError(UBOLT_ERR_ARG, "dsa_setup: face distances missing");
    ubolt_dsa_options o;
-   ubolt_dsa_defaults(&o);
-   if (opts) o = *opts;
-   if (!(o.penalty > 0.0)) return SetError(UBOLT_ERR_ARG, "dsa penalty must be positive, got %g", o.penalty);
-   if (!(o.consistent_power >= 1.0)) return SetError(UBOLT_ERR_ARG, "consistent-D power must be >= 1");
-   if (o.inner_iterations < 1 || o.inner_iterations > 10000) return SetError(UBOLT_ERR_ARG, "inner iterations");
-   if (!(o.void_d >= 0.0)) return SetError(UBOLT_ERR_ARG, "void D must be >= 0 (0: from the voids' chord)");
+   if ((rc = DsaOptions(opts, &o))) return rc;
    UboltDsaFree(ctx);
    auto ds = new ubolt_dsa();
    ctx->dsa = ds;
@@ -604,18 +827,8 @@ extern "C" int ubolt_dsa_setup(ubolt_ctx *ctx, const ubolt_dg_geometry *g, const
          ds->half_range[k] = sum / ctx->sum_weights;
       }
    }
-   auto alloc = [&](double **p, size_t n) -> int {
-      const cudaError_t e = cudaMalloc((void **)p, std::max<size_t>(n, 1) * sizeof(double));
-      if (e != cudaSuccess) {
-         cudaGetLastError();
-         return SetError(UBOLT_ERR_NOMEM, "DSA workspace: %s", cudaGetErrorString(e));
-      }
-      return UBOLT_OK;
-   };
-   const size_t bs = (size_t)nb * nb, nn = (size_t)ds->n_nodes;
-   if ((rc = alloc(&ds->val, nc * (F + 1) * bs)) || (rc = alloc(&ds->jinv, nc * bs)) || (rc = alloc(&ds->rhs, nn)) ||
-       (rc = alloc(&ds->u, nn)) || (rc = alloc(&ds->r, nn)) || (rc = alloc(&ds->z, nn)) || (rc = alloc(&ds->p, nn)) ||
-       (rc = alloc(&ds->q, nn)) || (rc = alloc(&ds->scal, kDsaScalars + (nn + kDsaThreads - 1) / kDsaThreads))) {
+   const size_t bs = (size_t)nb * nb;
+   if ((rc = AllocDsa(ds, nc * (F + 1) * bs, nc * bs))) {
       UboltDsaFree(ctx);
       return rc;
    }
@@ -640,10 +853,10 @@ extern "C" int ubolt_dsa_set_group(ubolt_ctx *ctx, void *stream)
    cudaMemcpyAsync(st.data(), ctx->g64.sigma_t, ds->nc * 8, cudaMemcpyDeviceToHost, s);
    cudaMemcpyAsync(ss.data(), ctx->g64.sigma_s, ds->nc * 8, cudaMemcpyDeviceToHost, s);
    if ((rc = CudaCheck(cudaStreamSynchronize(s), "dsa_set_group"))) return rc;
-   if ((rc = Assemble(ds, st.data(), ss.data()))) return rc;
+   if ((rc = ds->cg ? AssembleCg(ctx, ds, st.data(), ss.data()) : Assemble(ds, st.data(), ss.data()))) return rc;
    cudaMemcpyAsync(ds->val, ds->h_val.data(), ds->h_val.size() * 8, cudaMemcpyHostToDevice, s);
    cudaMemcpyAsync(ds->jinv, ds->h_jinv.data(), ds->h_jinv.size() * 8, cudaMemcpyHostToDevice, s);
-   cudaMemcpyAsync(ds->mask, ds->h_mask.data(), ds->nc, cudaMemcpyHostToDevice, s);
+   if (ds->mask) cudaMemcpyAsync(ds->mask, ds->h_mask.data(), ds->nc, cudaMemcpyHostToDevice, s);
    if ((rc = CudaCheck(cudaStreamSynchronize(s), "dsa upload"))) return rc;
    ds->assembled = true;
    return UBOLT_OK;
@@ -664,10 +877,7 @@ extern "C" int ubolt_dsa_spmv(ubolt_ctx *ctx, const double *u, double *v, void *
    int rc = CheckReady(ctx, false);
    if (rc || (rc = CheckDsa(ctx))) return rc;
    if (!u || !v || u == v) return SetError(UBOLT_ERR_ARG, "dsa_spmv: u and v must be distinct device arrays");
-   ubolt_dsa *ds = ctx->dsa;
-   DsaSpmvKernel<<<(ds->n_nodes + 255) / 256, 256, 0, (cudaStream_t)stream>>>(ds->n_nodes, ds->nb, ds->F,
-                                                                              ctx->g64.code, ds->val, u, v, nullptr,
-                                                                              nullptr);
+   DsaSpmvLaunch(ctx, ctx->dsa, u, v, nullptr, nullptr, (cudaStream_t)stream);
    return CheckLaunch("dsa_spmv");
 }
 
@@ -712,6 +922,7 @@ extern "C" int ubolt_dsa_matrix(ubolt_ctx *ctx, double *blocks)
    int rc = CheckReady(ctx, false);
    if (rc || (rc = CheckDsa(ctx))) return rc;
    if (!blocks) return SetError(UBOLT_ERR_ARG, "dsa_matrix: NULL output");
+   if (ctx->dsa->cg) return SetError(UBOLT_ERR_STATE, "dsa_matrix: the CG-SUPG operator is CSR, read it by ubolt_dsa_spmv");
    std::copy(ctx->dsa->h_val.begin(), ctx->dsa->h_val.end(), blocks);
    return UBOLT_OK;
 }
@@ -785,7 +996,7 @@ extern "C" int ubolt_dsa_apply_static(ubolt_ctx *ctx, const double *x, double *y
    CgStartKernel<<<grid, 256, 0, s>>>(nodes, ds->nb, ds->jinv, rhs, u, r, z, p, scal);
    CountLaunch();
    for (int it = 0; it < ds->inner_its; it++) {
-      DsaSpmvKernel<<<grid, 256, 0, s>>>(nodes, ds->nb, ds->F, ctx->g64.code, ds->val, p, q, p, scal);
+      DsaSpmvLaunch(ctx, ds, p, q, p, scal, s);
       CgUpdateKernel<<<grid, 256, 0, s>>>(nodes, p, q, u, r, scal);
       CgPrecondKernel<<<grid, 256, 0, s>>>(nodes, ds->nb, ds->jinv, r, z, scal);
       CgDirectionKernel<<<grid, 256, 0, s>>>(nodes, z, p, scal);

@@ -1,4 +1,5 @@
 // The angular moment and the right-hand-side fills.
+#include "cg.h"
 #include "ctx.h"
 
 namespace ubolt {
@@ -200,6 +201,11 @@ extern "C" int ubolt_add_source(ubolt_ctx *ctx, const double *q_cell, double *b,
    int rc = CheckReady(ctx, false);
    if (rc) return rc;
    if (!q_cell || !b) return SetError(UBOLT_ERR_ARG, "add_source: NULL array");
+   if (ctx->cg) {
+      // SUPG-weighted: tau needs the group's sigma_t
+      if ((rc = CheckReady(ctx, true))) return rc;
+      return CgAddSource(ctx, q_cell, b, stream);
+   }
    AddSourceKernel<<<RunGrid(ctx->n_cells), 256, 0, (cudaStream_t)stream>>>(ctx->g64, q_cell, b);
    return CheckLaunch("add_source");
 }
@@ -210,6 +216,10 @@ extern "C" int ubolt_add_transfer(ubolt_ctx *ctx, const double *phi_from, const 
    int rc = CheckReady(ctx, false);
    if (rc) return rc;
    if (!phi_from || !sigma_s_from_to || !b) return SetError(UBOLT_ERR_ARG, "add_transfer: NULL array");
+   if (ctx->cg) {
+      if ((rc = CheckReady(ctx, true))) return rc;
+      return CgAddTransfer(ctx, phi_from, sigma_s_from_to, b, stream);
+   }
    AddTransferKernel<<<RunGrid(ctx->n_nodes), 256, 0, (cudaStream_t)stream>>>(ctx->g64, phi_from, sigma_s_from_to,
                                                                               b);
    return CheckLaunch("add_transfer");
@@ -227,6 +237,7 @@ extern "C" int ubolt_add_ghost_inflow(ubolt_ctx *ctx, const double *side_inflow,
       if (in.v[s] != 0.0 && ctx->side_bc[s] == UBOLT_BC_VACUUM) any = true;
    }
    if (!any) return UBOLT_OK;
+   if (ctx->cg) return CgGhostInflow(ctx, side_inflow, b, stream);
    const int64_t n = ctx->n_cells * ctx->A;
    GhostInflowKernel<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(ctx->g64, ctx->d_volume, in, b);
    return CheckLaunch("add_ghost_inflow");

@@ -364,6 +364,12 @@ static int Precondition(ubolt_ctx *ctx, int pc, bool adjoint, const T *x, T *y, 
       if (rc) return rc;
       return DsaCorrect<T>(ctx, x, y, tmp, stream);
    }
+   case UBOLT_PC_BLOCK_DSA: {
+      if (adjoint) return SetError(UBOLT_ERR_ARG, "the DSA stage has no transpose here");
+      int rc = BlockApply<T>(ctx, x, y, false, stream);
+      if (rc) return rc;
+      return DsaCorrect<T>(ctx, x, y, tmp, stream);
+   }
    default: return SetError(UBOLT_ERR_ARG, "unknown preconditioner %d", pc);
    }
 }
@@ -799,7 +805,8 @@ static void FreeWorkspace(ubolt_ctx *ctx)
 static int EnsureWorkspace(ubolt_ctx *ctx, const ubolt_solve_options *o)
 {
    const bool mixed = o->precision == UBOLT_PRECISION_MIXED;
-   const bool flexible = o->pc == UBOLT_PC_SWEEP_DSA;
+   // A DSA stage whose inner solve is PCG is not a fixed linear map: flexible GMRES
+   const bool flexible = o->pc == UBOLT_PC_SWEEP_DSA || o->pc == UBOLT_PC_BLOCK_DSA;
    const int m = o->restart > 0 ? o->restart : 30;
    ubolt_solver *ws = ctx->solver;
    if (ws && ws->restart == m && ws->mixed == mixed && ws->flexible == flexible) return UBOLT_OK;
@@ -886,6 +893,7 @@ extern "C" int ubolt_solver_setup(ubolt_ctx *ctx, const ubolt_solve_options *opt
    ubolt_solve_defaults(&o);
    if (opts) o = *opts;
    if (o.restart < 1 || o.restart > 200) return SetError(UBOLT_ERR_ARG, "restart %d (1..200)", o.restart);
+   if (o.pc < UBOLT_PC_NONE || o.pc > UBOLT_PC_BLOCK_DSA) return SetError(UBOLT_ERR_ARG, "preconditioner %d", o.pc);
    if ((rc = EnsureWorkspace(ctx, &o))) return rc;
    if ((o.pc == UBOLT_PC_SWEEP || o.pc == UBOLT_PC_SWEEP_DSA) && !ctx->sweep) return ubolt_sweep_setup(ctx, 0);
    return UBOLT_OK;

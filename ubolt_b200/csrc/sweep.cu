@@ -573,6 +573,7 @@ static int BuildWavePlan(ubolt_ctx *ctx, ubolt_sweep_plan *plan)
 
 int BuildSweepPlan(ubolt_ctx *ctx, int patch_size)
 {
+   if (int rc = RequireDg(ctx, "the sweep")) return rc;
    const int64_t nc = ctx->n_cells;
    int P = patch_size > 0 ? patch_size : kDefaultPatch;
    if (P > 256) P = 256;

@@ -258,6 +258,80 @@ def build_geometry(mesh, order, side_bc=None):
         lib.ubolt_geometry_free(h)
 
 
+_CG_ARRAYS = [("elem_vertex", np.int64, "env"), ("mass", np.float64, "enn"), ("grad", np.float64, "enn3"),
+              ("stiff", np.float64, "enn9"), ("centre_grad", np.float64, "en3"), ("volume", np.float64, "e"),
+              ("centroid", np.float64, "e3"), ("lumped_mass", np.float64, "v"), ("vertex_coord", np.float64, "v3"),
+              ("star_offset", np.int64, "v1"), ("star_elem", np.int64, "s"), ("star_li", np.int32, "s"),
+              ("bface_offset", np.int64, "v1"), ("bface_nA", np.float64, "b3"), ("bface_mass", np.float64, "b"),
+              ("bface_side", np.int32, "b"), ("bface_bc", np.int32, "b"),
+              ("elem_face_neighbour", np.int64, "eF"), ("elem_face_area", np.float64, "eF"),
+              ("elem_face_bc", np.int32, "eF")]
+
+
+@dataclass
+class CGGeometry:
+    """The CG-SUPG tables (ubolt_cg_geometry_build), NumPy-owned, in the C
+    ABI's flat layouts: per element the mass, gradient and stiffness matrices
+    of the degree-1 Lagrange basis; per vertex its star, lumped mass and
+    boundary faces."""
+    dim: int
+    n_element_vertices: int
+    faces_per_element: int
+    n_vertices: int
+    n_elements: int
+    arrays: dict = field(default_factory=dict)
+
+    @property
+    def n_cells(self):
+        return self.n_elements
+
+    def __getattr__(self, name):
+        arrays = self.__dict__.get("arrays", {})
+        if name in arrays:
+            return arrays[name]
+        raise AttributeError(name)
+
+    def struct(self):
+        _lib, _, _ = _native()
+        g = _lib.CGGeometry()
+        g.dim, g.n_element_vertices, g.faces_per_element = self.dim, self.n_element_vertices, self.faces_per_element
+        g.n_vertices, g.n_elements = self.n_vertices, self.n_elements
+        g.n_star, g.n_bfaces = len(self.arrays["star_elem"]), len(self.arrays["bface_mass"])
+        for name, dt, _ in _CG_ARRAYS:
+            ptr_t = {np.float64: _lib.dp, np.int64: _lib.i64p, np.int32: _lib.i32p}[dt]
+            setattr(g, name, self.arrays[name].ctypes.data_as(ptr_t))
+        return g
+
+
+def build_cg_geometry(mesh, side_bc=None):
+    """ubolt_cg_geometry_build on a Mesh; side_bc[2 * dim] are UBOLT_BC_* (default vacuum)."""
+    _lib, lib, check = _native()
+    dim = mesh.dim
+    sbc = np.zeros(2 * dim, dtype=np.int32) if side_bc is None else np.asarray(side_bc, dtype=np.int32)
+    v = np.ascontiguousarray(mesh.vertices, dtype=np.float64)
+    cells = np.ascontiguousarray(mesh.cells, dtype=np.int64)
+    h = _lib.vp()
+    check(lib.ubolt_cg_geometry_build(dim, mesh.cell_type, len(v), v.ctypes.data_as(_lib.dp), len(cells),
+                                      cells.ctypes.data_as(_lib.i64p), sbc.ctypes.data_as(_lib.i32p), C.byref(h)))
+    try:
+        view = _lib.CGGeometry()
+        check(lib.ubolt_cg_geometry_view(h, C.byref(view)))
+        ne, nvx, nv, F = view.n_elements, view.n_vertices, view.n_element_vertices, view.faces_per_element
+        sizes = {"env": ne * nv, "enn": ne * nv * nv, "enn3": ne * nv * nv * 3, "enn9": ne * nv * nv * 9,
+                 "en3": ne * nv * 3, "e": ne, "e3": ne * 3, "v": nvx, "v3": nvx * 3, "v1": nvx + 1,
+                 "s": view.n_star, "b": view.n_bfaces, "b3": view.n_bfaces * 3, "eF": ne * F}
+        arrays = {}
+        for name, dt, sz in _CG_ARRAYS:
+            n = sizes[sz]
+            arrays[name] = (np.ctypeslib.as_array(getattr(view, name), shape=(n,)).astype(dt, copy=True) if n
+                            else np.zeros(0, dtype=dt))
+        geo = CGGeometry(view.dim, nv, F, nvx, ne, arrays)
+        geo.source = (mesh, sbc.copy())
+        return geo
+    finally:
+        lib.ubolt_cg_geometry_free(h)
+
+
 # ~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~
 # Problems
 # ~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~~

@@ -34,13 +34,22 @@ def _stream(stream=None):
 
 
 class Context:
-    """ubolt_ctx: geometry and ordinates on one device (the current one)."""
+    """ubolt_ctx: geometry and ordinates on one device (the current one).
 
-    def __init__(self, geometry, quad):
+    A problem.Geometry gives the DG backend (UnstructuredDG); a
+    problem.CGGeometry the CG-SUPG one (UnstructuredCG, zeta its thin-cell
+    SUPG parameter), whose nodes are the mesh's vertices and whose cells -
+    what cross sections and sources are given on - are its elements."""
+
+    def __init__(self, geometry, quad, zeta=0.5):
         self.geometry, self.quad = geometry, quad
         h = _lib.vp()
         gs, qs = geometry.struct(), quad.struct()
-        check(lib.ubolt_ctx_create(C.byref(gs), C.byref(qs), C.byref(h)))
+        self.is_cg = isinstance(geometry.struct(), _lib.CGGeometry)
+        if self.is_cg:
+            check(lib.ubolt_ctx_create_cg(C.byref(gs), C.byref(qs), float(zeta), C.byref(h)))
+        else:
+            check(lib.ubolt_ctx_create(C.byref(gs), C.byref(qs), C.byref(h)))
         self.handle = h
         self.device = torch.device("cuda", torch.cuda.current_device())
         rows, nodes, cells = C.c_int64(), C.c_int64(), C.c_int64()
@@ -233,7 +242,7 @@ class TransportSolver:
         o.krylov = {"auto": 0, "full": 1}[krylov]
         o.precision = {"fp64": _lib.PRECISION_FP64, "mixed": _lib.PRECISION_MIXED}[precision]
         o.pc = {"none": _lib.PC_NONE, "block": _lib.PC_BLOCK, "sweep": _lib.PC_SWEEP,
-                "sweep+dsa": _lib.PC_SWEEP_DSA}[pc]
+                "sweep+dsa": _lib.PC_SWEEP_DSA, "block+dsa": _lib.PC_BLOCK_DSA}[pc]
         self.opts = o
         check(lib.ubolt_solver_setup(ctx.handle, C.byref(o)))
 
@@ -569,8 +578,13 @@ class DSAPrecon:
         o.penalty, o.consistent_d, o.consistent_power = penalty, int(consistent_d), consistent_power
         o.inner_iterations = inner_iterations
         o.void_sigma_t, o.void_bridge, o.void_d = void_sigma_t, int(void_bridge), void_d
-        gs = ctx.geometry.struct()
-        check(lib.ubolt_dsa_setup(ctx.handle, C.byref(gs), C.byref(o)))
+        if ctx.is_cg:
+            # DSACG on the context's own tables (the penalty and consistent-D
+            # options are the DG operators' and do not apply)
+            check(lib.ubolt_dsa_setup(ctx.handle, None, C.byref(o)))
+        else:
+            gs = ctx.geometry.struct()
+            check(lib.ubolt_dsa_setup(ctx.handle, C.byref(gs), C.byref(o)))
 
     def set_group(self, stream=None):
         """Refill D for the context's current group (call after Context.set_group)."""
