@@ -121,7 +121,10 @@ def test_cg_rhs_fills_match_oracle(case):
     phi = case.rng.uniform(0.0, 1.0, pr.n_vertices)
     sig = case.rng.uniform(0.0, 0.5, pr.T.cells.shape[0])
     b.zero_()
-    check(lib.ubolt_add_transfer(ctx.handle, T._p(dev(phi)), T._p(dev(sig)), T._p(b), T._stream()))
+    # Both inputs stay referenced until the launch: a temporary freed after
+    # its pointer is taken can hand its block to the next allocation
+    phi_t, sig_t = dev(phi), dev(sig)
+    check(lib.ubolt_add_transfer(ctx.handle, T._p(phi_t), T._p(sig_t), T._p(b), T._stream()))
     assert rel(b, pr.transfer(phi, sig)) < TOL64
     side_in = np.arange(1, 2 * pr.dim + 1, dtype=float) * 0.7
     b.zero_()
