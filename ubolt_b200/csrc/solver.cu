@@ -29,7 +29,9 @@ int DsaCorrect(ubolt_ctx *ctx, const T *r, T *y, T *tmp, void *stream);
 bool SweepIsExact(ubolt_ctx *ctx);
 template <typename T>
 int SweepAffine(ubolt_ctx *ctx, const T *r0, const double *alpha, const double *phi, const double *rho, const T *u,
-                T *psi, void *stream);
+                T *psi, void *stream, bool ordinate_major);
+template <typename T>
+bool SweepWritesOrdinateMajor(ubolt_ctx *ctx);
 }  // namespace ubolt
 
 struct ubolt_solver {
@@ -601,6 +603,58 @@ __global__ void __launch_bounds__(256) IsoScatterKernel(const S *__restrict__ z,
    }
 }
 
+// The same from z ordinate-major (z[a n_nodes + node]): one thread per node,
+// each warp's loads of one ordinate coalesced
+template <typename S>
+__global__ void __launch_bounds__(256) IsoScatterOmKernel(const S *__restrict__ z, const S *__restrict__ w,
+                                                          const S *__restrict__ sigma_s, double inv_W, int nb, int A,
+                                                          int64_t n_nodes, const double *__restrict__ phi_in,
+                                                          double *__restrict__ phi_out)
+{
+   for (int64_t node = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; node < n_nodes;
+        node += (int64_t)gridDim.x * blockDim.x) {
+      double sum = 0.0;
+      const S *zn = z + node;
+#pragma unroll 8
+      for (int a = 0; a < A; a++) sum += (double)w[a] * (double)zn[(int64_t)a * n_nodes];
+      phi_out[node] = phi_in[node] - (double)sigma_s[node / nb] * inv_W * sum;
+   }
+}
+
+// x(node, a) += sum_i c[i] Z_i(a, node): the update from ordinate-major
+// vectors into UBOLT's row layout, through a 32 x 32 shared-memory tile per
+// block so that both the reads (nodes fastest) and the writes (ordinates
+// fastest) are coalesced
+template <typename S>
+__global__ void __launch_bounds__(256) MultiAxpyOmKernel(const S *__restrict__ Z, int64_t n, int nv,
+                                                         const double *__restrict__ c, int64_t n_nodes, int A,
+                                                         S *__restrict__ x)
+{
+   __shared__ double tile[32][33];
+   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+   const int64_t node0 = (int64_t)blockIdx.x * 32;
+   const int a0 = blockIdx.y * 32;
+#pragma unroll
+   for (int r = 0; r < 4; r++) {
+      const int a = a0 + ty + 8 * r;
+      const int64_t node = node0 + tx;
+      double v = 0.0;
+      if (a < A && node < n_nodes)
+         for (int i = 0; i < nv; i++) v += c[i] * (double)Z[(int64_t)i * n + (int64_t)a * n_nodes + node];
+      tile[ty + 8 * r][tx] = v;
+   }
+   __syncthreads();
+#pragma unroll
+   for (int r = 0; r < 4; r++) {
+      const int64_t node = node0 + ty + 8 * r;
+      const int a = a0 + tx;
+      if (a < A && node < n_nodes) {
+         const int64_t k = node * A + a;
+         x[k] = (S)((double)x[k] + tile[tx][ty + 8 * r]);
+      }
+   }
+}
+
 // h[i] = alpha[i] alpha_w |r_perp|^2 + kappa d[i] for i < j1 (in place over
 // d), then alpha[j1] = alpha_w - sum_i h[i] alpha[i]: one Gram-Schmidt
 // pass's scalars. alpha_w is alpha[j1], or on the first pass alpha[j1 - 1]
@@ -623,9 +677,10 @@ __global__ void IsoCombineKernel(double *__restrict__ d, double *__restrict__ al
 // it reads it; the adjoint's reversed-ordinate sweep takes it expanded in t.
 template <typename S>
 static int IsoPrecondition(ubolt_ctx *ctx, bool adjoint, const S *r0, const double *alpha, const double *phi,
-                           const double *rho, const S *u, S *t, S *z, S *tmp, int64_t n, int igrid, void *stream)
+                           const double *rho, const S *u, S *t, S *z, S *tmp, int64_t n, int igrid, void *stream,
+                           bool ordinate_major)
 {
-   if (!adjoint) return SweepAffine<S>(ctx, r0, alpha, phi, rho, u, z, stream);
+   if (!adjoint) return SweepAffine<S>(ctx, r0, alpha, phi, rho, u, z, stream, ordinate_major);
    // L^{-T} = V P L^{-1} P V^{-1}: the expansion and P V^{-1} in one pass,
    // the sweep, then V P in place
    IsoExpandKernel<S><<<igrid, 256, 0, (cudaStream_t)stream>>>(r0, alpha, phi, rho, u, ctx->A, ctx->n_nodes, t,
@@ -664,7 +719,10 @@ static int GmresIso(ubolt_ctx *ctx, const ubolt_solver *ws, S *work, const S *b,
       kappa = (double)A;
    // Full-length vectors live in the (unused) plain basis: r0, t, tmp, then
    // the preconditioned vectors z_j = M^{-1} v_j of the cycle, kept so the
-   // update x += sum_j y_j z_j needs no further sweep
+   // update x += sum_j y_j z_j needs no further sweep. The forward sweep
+   // writes them ordinate-major (each task's psi contiguous, whole sectors
+   // written), read back by the scatter and the update
+   const bool om = !adjoint && SweepWritesOrdinateMajor<S>(ctx);
    S *r0 = work, *t = work + n, *tmp = work + 2 * n, *Zb = work + 3 * n;
    double *Phi = ws->Phi, *alpha = ws->alpha, *scal = ws->scal;
    std::vector<double> H((size_t)(m + 1) * m, 0.0), cs(m), sn(m), gv(m + 1), y(m), h1(m + 1), h2(m + 2),
@@ -719,9 +777,14 @@ static int GmresIso(ubolt_ctx *ctx, const ubolt_solver *ws, S *work, const S *b,
          double *pj = Phi + (int64_t)j * nn, *pn = Phi + (int64_t)(j + 1) * nn;
          S *z = Zb + (int64_t)j * n;
          // w = v_j - E_u m(M^{-1} v_j): alpha_w = alpha_j, phi_w = phi_j - m
-         if ((rc = IsoPrecondition<S>(ctx, adjoint, r0_in, alpha + j, pj, ws->rho, u, t, z, tmp, n, igrid, stream)))
+         if ((rc = IsoPrecondition<S>(ctx, adjoint, r0_in, alpha + j, pj, ws->rho, u, t, z, tmp, n, igrid, stream,
+                                      om)))
             return rc;
-         IsoScatterKernel<S><<<igrid, 256, 0, s>>>(z, wgt, sig_s, 1.0 / ctx->sum_weights, ctx->nb, A, nn, pj, pn);
+         if (om)
+            IsoScatterOmKernel<S><<<(int)std::min<int64_t>((nn + 255) / 256, 148 * 16), 256, 0, s>>>(z, wgt, sig_s, 1.0 / ctx->sum_weights, ctx->nb, A, nn,
+                                                              pj, pn);
+         else
+            IsoScatterKernel<S><<<igrid, 256, 0, s>>>(z, wgt, sig_s, 1.0 / ctx->sum_weights, ctx->nb, A, nn, pj, pn);
          CountLaunch();
          // Classical Gram-Schmidt, twice, in the compressed inner product
          for (int pass = 0; pass < 2; pass++) {
@@ -774,7 +837,11 @@ static int GmresIso(ubolt_ctx *ctx, const ubolt_solver *ws, S *work, const S *b,
          y[i] = tt / H[i * m + i];
       }
       ToDevice(ws, y.data(), dy, kMbH1, j, s);
-      MultiAxpyKernel<S><<<grid, 256, 0, s>>>(Zb, n, j, dy, 1.0, x, 1);
+      if (om)
+         MultiAxpyOmKernel<S><<<dim3((unsigned)((nn + 31) / 32), (unsigned)((A + 31) / 32)), 256, 0, s>>>(Zb, n, j, dy,
+                                                                                                         nn, A, x);
+      else
+         MultiAxpyKernel<S><<<grid, 256, 0, s>>>(Zb, n, j, dy, 1.0, x, 1);
       CountLaunch();
       if (out->converged) break;
    }

@@ -160,6 +160,10 @@ struct SweepDev {
    const double *aff_alpha, *aff_phi, *aff_rho;
    const void *aff_u;
    int32_t aff_iso;  // r0 is isotropic (r0 = E rho): the input is u_a phi(node), q is not read
+   // psi(c, j, a) at psi[c os_c + j os_j + a os_a]: UBOLT's row layout
+   // (NB A, A, 1), or ordinate-major (NB, 1, n_cells NB), where a task's
+   // cells of one ordinate are contiguous and it writes whole sectors
+   int64_t os_c, os_j, os_a;
 };
 
 // Per-warp shared-memory slice, for P cells and S gathered faces per cell
@@ -328,7 +332,9 @@ __global__ void __launch_bounds__(128, SweepMinBlocks<T, NB, PL>()) SweepKernel(
    };
    for (;;) {
       // A task is claimed only when the warp is free: a task claimed while
-      // the warp still walks (and waits in) another would sit idle behind it
+      // the warp still walks (and waits in) another would sit idle behind it,
+      // and the tasks downstream of it would wait too (claiming even two
+      // levels before the walk ends measured slower)
       int64_t t = 0;
       if (lane == 0) t = (int64_t)atomicAdd(&s.ctrl[kCtrlCounter], 1u);
       t = __shfl_sync(0xffffffffu, t, 0);
@@ -390,8 +396,9 @@ __global__ void __launch_bounds__(128, SweepMinBlocks<T, NB, PL>()) SweepKernel(
             for (int sl = 0; sl < SM; sl++)
 #pragma unroll
                for (int j = 0; j < NB; j++)
-                  xp[k][sl][j] = (my_up[k][sl] >= 0 && !hook) ? LoadRelaxed(psi + ((int64_t)my_up[k][sl] * NB + j) * A + a)
-                                                             : Sentinel<T>();
+                  xp[k][sl][j] = (my_up[k][sl] >= 0 && !hook)
+                                    ? LoadRelaxed(psi + (int64_t)my_up[k][sl] * s.os_c + j * s.os_j + a * s.os_a)
+                                    : Sentinel<T>();
          }
       }
 #pragma unroll
@@ -482,8 +489,8 @@ __global__ void __launch_bounds__(128, SweepMinBlocks<T, NB, PL>()) SweepKernel(
 #pragma unroll
             for (int sl = 0; sl < SM; sl++) {
                if (my_up[k][sl] < 0) continue;
-               const T *src = psi + (int64_t)my_up[k][sl] * NB * A + a;
-               int stride = A;
+               const T *src = psi + (int64_t)my_up[k][sl] * s.os_c + a * s.os_a;
+               int stride = (int)s.os_j;
                if (hook_left) {
                   src = never;  // test hook: this wait can never be met
                   stride = 0;
@@ -505,7 +512,7 @@ __global__ void __launch_bounds__(128, SweepMinBlocks<T, NB, PL>()) SweepKernel(
 #pragma unroll
             for (int j = 0; j < NB; j++) {
                loc[local * NB + j] = y[j];
-               StoreRelaxed(&psi[(c * NB + j) * A + a], Publishable(y[j]));
+               StoreRelaxed(&psi[c * s.os_c + j * s.os_j + a * s.os_a], Publishable(y[j]));
             }
          }
          __syncwarp();
@@ -671,6 +678,21 @@ static SweepDev DevPlan(const ubolt_sweep_plan *pl)
    return s;
 }
 
+// psi's layout for the task kernel
+static void SetLayout(SweepDev &s, const ubolt_ctx *ctx, bool ordinate_major)
+{
+   const int64_t nb = ctx->nb, A = ctx->A;
+   if (ordinate_major) {
+      s.os_c = nb;
+      s.os_j = 1;
+      s.os_a = ctx->n_cells * nb;
+   } else {
+      s.os_c = nb * A;
+      s.os_j = A;
+      s.os_a = 1;
+   }
+}
+
 // Bytes of the factor store for one precision
 static int64_t FactorBytes(const ubolt_ctx *ctx, const ubolt_sweep_plan *pl, size_t elem)
 {
@@ -754,7 +776,8 @@ static T *EnsureFactors(ubolt_ctx *ctx, cudaStream_t st)
 }
 
 template <typename T, int NB, int F>
-static int LaunchSweep(ubolt_ctx *ctx, const T *q, T *psi, cudaStream_t st, const SweepDev *affine = nullptr)
+static int LaunchSweep(ubolt_ctx *ctx, const T *q, T *psi, cudaStream_t st, const SweepDev *affine = nullptr,
+                       bool ordinate_major = false)
 {
    ubolt_sweep_plan *pl = ctx->sweep;
    const int which = sizeof(T) == 8 ? 0 : 1;
@@ -762,6 +785,7 @@ static int LaunchSweep(ubolt_ctx *ctx, const T *q, T *psi, cudaStream_t st, cons
    if (pl->fac_wave[which]) {
       // One block per ordinate over the store in wave order (no sentinel fill)
       if (!fac) return UBOLT_ERR_CUDA;  // the failed launch set the message
+      if (ordinate_major) return SetError(UBOLT_ERR_STATE, "the wave sweep writes the row layout only");
       WaveDev w = pl->wave[which];
       w.ctrl = pl->ctrl;
       w.spin_limit = pl->spin_limit;
@@ -797,6 +821,7 @@ static int LaunchSweep(ubolt_ctx *ctx, const T *q, T *psi, cudaStream_t st, cons
    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)std::max(per_sm, 1) * n_sm, want));
    pl->grid = grid;
    SweepDev s = DevPlan(pl);
+   SetLayout(s, ctx, ordinate_major);
    if (affine) {
       s.aff_alpha = affine->aff_alpha;
       s.aff_phi = affine->aff_phi;
@@ -838,7 +863,7 @@ bool SweepIsExact(ubolt_ctx *ctx)
 // r0 == nullptr: r0 is isotropic, r0 = E_u rho, and the input is E_u phi.
 template <typename T>
 int SweepAffine(ubolt_ctx *ctx, const T *r0, const double *alpha, const double *phi, const double *rho, const T *u,
-                T *psi, void *stream)
+                T *psi, void *stream, bool ordinate_major)
 {
    int rc = CheckReady(ctx, true);
    if (rc) return rc;
@@ -849,14 +874,27 @@ int SweepAffine(ubolt_ctx *ctx, const T *r0, const double *alpha, const double *
    aff.aff_rho = rho;
    aff.aff_u = u;
    aff.aff_iso = r0 == nullptr;
-   UBOLT_DISPATCH(ctx->nb, ctx->F, return (LaunchSweep<T, NB_, F_>(ctx, r0, psi, (cudaStream_t)stream, &aff)));
+   UBOLT_DISPATCH(ctx->nb, ctx->F,
+                  return (LaunchSweep<T, NB_, F_>(ctx, r0, psi, (cudaStream_t)stream, &aff, ordinate_major)));
    return SetError(UBOLT_ERR_STATE, "no sweep kernel for this shape");
 }
 
+// True where the next sweep in precision T runs the task kernel (which can
+// write psi ordinate-major); false where the wave kernel runs
+template <typename T>
+bool SweepWritesOrdinateMajor(ubolt_ctx *ctx)
+{
+   if (!ctx->sweep && BuildSweepPlan(ctx, 0)) return false;
+   const int which = sizeof(T) == 8 ? 0 : 1;
+   return !(ctx->sweep->fac[which] && ctx->sweep->fac_wave[which]);
+}
+
 template int SweepAffine<double>(ubolt_ctx *, const double *, const double *, const double *, const double *,
-                                 const double *, double *, void *);
+                                 const double *, double *, void *, bool);
 template int SweepAffine<float>(ubolt_ctx *, const float *, const double *, const double *, const double *,
-                                const float *, float *, void *);
+                                const float *, float *, void *, bool);
+template bool SweepWritesOrdinateMajor<double>(ubolt_ctx *);
+template bool SweepWritesOrdinateMajor<float>(ubolt_ctx *);
 template int Sweep<double>(ubolt_ctx *, const double *, double *, void *);
 template int Sweep<float>(ubolt_ctx *, const float *, float *, void *);
 
