@@ -56,7 +56,7 @@ def _args():
                    help="tri256 is the headline line; hex128 (4 groups) and tet44 time the other solve configs")
     p.add_argument("--restart", type=int, default=0, help="GMRES restart (0: 30, or 10 for hex128)")
     p.add_argument("--profile", default="",
-                   choices=["", "apply", "apply32", "sweep", "sweep32", "wave", "wave32", "adjoint", "adjoint32",
+                   choices=["", "apply", "apply32", "sweep", "sweep32", "sweep_iso", "sweep_iso32", "wave", "wave32", "adjoint", "adjoint32",
                             "dsa_spmv", "block", "gradient", "scalar_flux"],
                    help="run only this kernel, --warmup + --steps launches on the workload, for a profiler")
     return p.parse_args()
@@ -235,6 +235,11 @@ def profile_kernel(args, ctx, T, stream):
         sw = T.Sweep(ctx, 0)
         sw.set_kernel("tasks" if kind == "sweep" else "wave")
         fn = lambda: sw.apply(xr, yr)
+    elif kind == "sweep_iso":
+        sw = T.Sweep(ctx, 0)
+        sw.set_kernel("tasks")
+        phr = torch.rand(ctx.n_nodes, dtype=torch.float64, device="cuda", generator=g)
+        fn = lambda: sw.apply_iso(phr, yr, ordinate_major=True)
     elif kind == "dsa_spmv":
         dsa = T.DSAPrecon(ctx)
         dsa.set_group()
@@ -590,23 +595,35 @@ def main():
         t_apply32 = timed(lambda: A.mult(xf, yf))
         t_sweep64 = timed(lambda: sw.apply(xr, yr))
         t_sweep32 = timed(lambda: sw.apply(xf, yf))
+        # The form the compressed solve runs every iteration: an isotropic
+        # source (a node vector) in, psi out ordinate-major
+        phr = torch.randn(ctx.n_nodes, dtype=torch.float64, device="cuda")
+        t_iso64 = timed(lambda: sw.apply_iso(phr, yr, ordinate_major=True))
+        t_iso32 = timed(lambda: sw.apply_iso(phr, yf, ordinate_major=True))
         apply_bytes64 = 2 * n * 8 + 2 * ctx.n_cells * 8
         apply_bytes32 = 2 * n * 4 + 2 * ctx.n_cells * 4
         sweep_bytes64 = 2 * n * 8 + ctx.n_cells * 8
+        iso_bytes64 = n * 8 + ctx.n_nodes * 8 + ctx.n_cells * 8
         extra["apply_gbs"] = {"fp64": apply_bytes64 / t_apply64 / 1e6, "fp32": apply_bytes32 / t_apply32 / 1e6,
                               "fp64_us": t_apply64 * 1e3, "fp32_us": t_apply32 * 1e3}
         peak, peak_kind = _peaks()
         extra["kernels"] = kernel_map(ctx, T, prob, stream, peak, peak_kind)
         ctx.set_group(st, ss)
-        extra["sweep_us"] = {"fp64": t_sweep64 * 1e3, "fp32": t_sweep32 * 1e3}
+        extra["sweep_us"] = {"fp64": t_sweep64 * 1e3, "fp32": t_sweep32 * 1e3,
+                             "fp64_iso_ordinate_major": t_iso64 * 1e3, "fp32_iso_ordinate_major": t_iso32 * 1e3}
         # Dominant kernel of the solve: one sweep per iteration; the full basis
         # adds one apply per iteration and a sweep per cycle
         compressed = stats[-1]["krylov"] == 2
         sweeps = its if compressed else its + 1
         applies = 2 if compressed else its + 1
-        dom_sweep = t_sweep64 * sweeps >= t_apply64 * applies
+        t_dom_sweep = t_iso64 if compressed else t_sweep64
+        dom_sweep = t_dom_sweep * sweeps >= t_apply64 * applies
         peak, peak_kind = _peaks()
-        if dom_sweep:
+        if dom_sweep and compressed:
+            # phi in (node vector), psi out, sigma_t
+            ach = iso_bytes64 / t_iso64 / 1e6
+            kernel, traffic_key = "SweepKernel<double,3,3> (isotropic source, psi ordinate-major)", "sweep_iso_fp64"
+        elif dom_sweep:
             ach = sweep_bytes64 / t_sweep64 / 1e6
             kernel, traffic_key = "SweepKernel<double,3,3>", "sweep_fp64"
         else:
@@ -626,7 +643,7 @@ def main():
         extra["roofline"] = {"bound": "hbm", "kernel": kernel, "achieved": ach, "peak": peak, "unit": "GB/s",
                              "frac": ach / peak, "peak_source": peak_kind, "traffic": traffic,
                              "traffic_unit": "bytes per launch", "traffic_source": traffic_source,
-                             "share_of_solve": (t_sweep64 * sweeps if dom_sweep else t_apply64 * applies) / ms}
+                             "share_of_solve": (t_dom_sweep * sweeps if dom_sweep else t_apply64 * applies) / ms}
 
         # ~~~ Mixed precision: FP32 operator / sweep / Krylov storage + FP64 refinement
         mixed = T.TransportSolver(ctx, rtol=1e-8, precision="mixed", pc="sweep", restart=30, max_it=500,

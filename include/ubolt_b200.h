@@ -361,6 +361,18 @@ int ubolt_sweep_set_kernel(ubolt_ctx *ctx, int kernel);
  * bounded; check ubolt_sweep_status. */
 int ubolt_sweep(ubolt_ctx *ctx, const double *q, double *psi, void *stream);
 int ubolt_sweep_f32(ubolt_ctx *ctx, const float *q, float *psi, void *stream);
+/* psi = L^{-1} (u_a phi(node)) for every ordinate: the streaming stage on an
+ * isotropic source (u = NULL: u_a = 1), the form the compressed GMRES
+ * applies at every iteration (no reference counterpart: PCAIR is applied to
+ * whole vectors). phi is FP64 per node (n_cells n_basis); u and psi in the
+ * call's precision. ordinate_major: psi[(a n_cells + c) n_basis + i], each
+ * ordinate's values contiguous (the task kernel; where the wave kernel runs
+ * it gives UBOLT_ERR_STATE), else UBOLT's row layout. As ubolt_sweep
+ * otherwise. */
+int ubolt_sweep_iso(ubolt_ctx *ctx, const double *phi, const double *u, double *psi, int ordinate_major,
+                    void *stream);
+int ubolt_sweep_iso_f32(ubolt_ctx *ctx, const double *phi, const float *u, float *psi, int ordinate_major,
+                        void *stream);
 /* The factor stores: each cell-ordinate's B^{-1} and upwind couplings
  * G_f = B^{-1} s_f face_up_f, which depend on geometry and sigma_t but not on
  * q, rebuilt by one kernel launch on the first sweep after ubolt_set_group

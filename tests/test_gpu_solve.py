@@ -530,3 +530,36 @@ def test_sweep_kernel_choice_is_checked():
     psi = sw.apply(dev(rng.standard_normal(ctx.n_rows)))
     assert torch.isfinite(psi).all() and sw.status()["kernel"] == _lib.SWEEP_TASKS
     ctx.close()
+
+
+@pytest.mark.parametrize("case", [c for c in ACYCLIC if c[0].startswith(("tri", "hex"))][:4],
+                         ids=[c[0] for c in ACYCLIC if c[0].startswith(("tri", "hex"))][:4])
+def test_isotropic_sweep_in_both_layouts(case):
+    """ubolt_sweep_iso: L^{-1} of an isotropic source u_a phi(node) is the
+    sweep of the expanded source, in UBOLT's row layout and ordinate-major
+    (the layout the compressed GMRES keeps), FP64 bit for bit, FP32 to its
+    rounding; the oracle's sweep of the same source to 1e-12."""
+    mesh, g, q, st, ss = build(case)
+    ctx, keep = ctx_for(g, q, st, ss)
+    try:
+        sw = T.Sweep(ctx, 0)
+        sw.set_kernel("tasks")
+        nn, A, nc, nb = ctx.n_nodes, q.n_angles, g.n_cells, g.n_basis
+        rng = np.random.default_rng(5)
+        phi = rng.standard_normal(nn)
+        u = rng.uniform(0.5, 1.5, A)
+        full = (phi[:, None] * u[None, :]).ravel()
+        ref = O.Operator(g, q, st, ss).sweep(full)
+        plain = sw.apply(dev(full))
+        row = sw.apply_iso(dev(phi), torch.empty_like(plain), u=dev(u))
+        om = sw.apply_iso(dev(phi), torch.empty_like(plain), u=dev(u), ordinate_major=True)
+        assert torch.equal(row, plain)
+        assert torch.equal(om.view(A, nc, nb).permute(1, 2, 0).reshape(-1), plain)
+        assert np.abs(plain.cpu().numpy() - ref).max() <= 1e-12 * np.abs(ref).max()
+        om32 = sw.apply_iso(dev(phi), torch.empty(ctx.n_rows, dtype=torch.float32, device="cuda"),
+                            u=dev(u, torch.float32), ordinate_major=True)
+        r32 = om32.view(A, nc, nb).permute(1, 2, 0).reshape(-1).double().cpu().numpy()
+        assert np.abs(r32 - ref).max() <= 1e-4 * np.abs(ref).max()
+        assert sw.status()["timeouts"] == 0
+    finally:
+        ctx.close()

@@ -133,6 +133,8 @@ PRECISION_FP64, PRECISION_MIXED = 0, 1
 _sig("ubolt_sweep_setup", C.c_int, vp, C.c_int)
 _sig("ubolt_sweep", C.c_int, vp, vp, vp, vp)
 _sig("ubolt_sweep_f32", C.c_int, vp, vp, vp, vp)
+_sig("ubolt_sweep_iso", C.c_int, vp, vp, vp, vp, C.c_int, vp)
+_sig("ubolt_sweep_iso_f32", C.c_int, vp, vp, vp, vp, C.c_int, vp)
 _sig("ubolt_sweep_status", C.c_int, vp, C.POINTER(SweepInfo), vp)
 _sig("ubolt_sweep_test_wait", C.c_int, vp, C.c_uint32, C.c_int)
 _sig("ubolt_sweep_set_factor_limit", C.c_int, vp, C.c_int64)

@@ -154,7 +154,7 @@ struct SweepDev {
    uint32_t spin_limit;
    int32_t slots;
    int64_t unmet_task;
-   // Affine input: when aff_alpha is set the sweep reads
+   // Affine input: when aff_phi is set the sweep reads
    // q(node, a) = alpha r0(node, a) + u_a (phi(node) - alpha rho(node)),
    // u_a = aff_u[a] or 1, with r0 passed as q (compressed GMRES's Arnoldi vector)
    const double *aff_alpha, *aff_phi, *aff_rho;
@@ -408,8 +408,8 @@ __global__ void __launch_bounds__(128, SweepMinBlocks<T, NB, PL>()) SweepKernel(
          const int local = my_local[k];
          const int64_t c = base + local;
          T r[NB];
-         if (s.aff_alpha) {
-            const double al = *s.aff_alpha;
+         if (s.aff_phi) {
+            const double al = s.aff_iso ? 0.0 : *s.aff_alpha;
             const double ua = s.aff_u ? (double)static_cast<const T *>(s.aff_u)[a] : 1.0;
 #pragma unroll
             for (int j = 0; j < NB; j++) {
@@ -940,6 +940,29 @@ extern "C" int ubolt_sweep(ubolt_ctx *ctx, const double *q, double *psi, void *s
 extern "C" int ubolt_sweep_f32(ubolt_ctx *ctx, const float *q, float *psi, void *stream)
 {
    return Sweep<float>(ctx, q, psi, stream);
+}
+
+template <typename T>
+static int SweepIso(ubolt_ctx *ctx, const double *phi, const T *u, T *psi, int ordinate_major, void *stream)
+{
+   int rc = CheckReady(ctx, true);
+   if (rc) return rc;
+   if (!phi || !psi) return SetError(UBOLT_ERR_ARG, "sweep_iso: NULL array");
+   if (ordinate_major && !SweepWritesOrdinateMajor<T>(ctx))
+      return SetError(UBOLT_ERR_STATE, "sweep_iso: the wave kernel runs here, and it writes the row layout only");
+   return SweepAffine<T>(ctx, nullptr, nullptr, phi, nullptr, u, psi, stream, ordinate_major != 0);
+}
+
+extern "C" int ubolt_sweep_iso(ubolt_ctx *ctx, const double *phi, const double *u, double *psi, int ordinate_major,
+                               void *stream)
+{
+   return SweepIso<double>(ctx, phi, u, psi, ordinate_major, stream);
+}
+
+extern "C" int ubolt_sweep_iso_f32(ubolt_ctx *ctx, const double *phi, const float *u, float *psi, int ordinate_major,
+                                   void *stream)
+{
+   return SweepIso<float>(ctx, phi, u, psi, ordinate_major, stream);
 }
 
 extern "C" int ubolt_sweep_set_factor_limit(ubolt_ctx *ctx, int64_t bytes)

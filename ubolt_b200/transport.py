@@ -224,6 +224,12 @@ class Sweep:
         check(fn(self.ctx.handle, _p(q), _p(psi), _stream(stream)))
         return psi
 
+    def apply_iso(self, phi, psi, u=None, ordinate_major=False, stream=None):
+        """psi = L^{-1} (u_a phi(node)): phi FP64 per node, psi in its own precision."""
+        fn = lib.ubolt_sweep_iso if psi.dtype == torch.float64 else lib.ubolt_sweep_iso_f32
+        check(fn(self.ctx.handle, _p(phi), _p(u), _p(psi), int(bool(ordinate_major)), _stream(stream)))
+        return psi
+
     def status(self, stream=None):
         info = _lib.SweepInfo()
         check(lib.ubolt_sweep_status(self.ctx.handle, C.byref(info), _stream(stream)))
