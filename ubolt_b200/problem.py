@@ -183,8 +183,8 @@ def box_hexes(nx, ny, nz, lx=1.0, ly=1.0, lz=1.0, jitter=0.0, rng=None, tile=4):
 _KUHN = [(0, 1, 2, 6), (0, 1, 5, 6), (0, 3, 2, 6), (0, 3, 7, 6), (0, 4, 5, 6), (0, 4, 7, 6)]
 
 
-def box_tets(nx, ny, nz, jitter=0.0, rng=None, tile=4):
-    hx = box_hexes(nx, ny, nz, jitter=jitter, rng=rng, tile=tile)
+def box_tets(nx, ny, nz, jitter=0.0, rng=None, tile=4, lx=1.0, ly=1.0, lz=1.0):
+    hx = box_hexes(nx, ny, nz, lx, ly, lz, jitter=jitter, rng=rng, tile=tile)
     cells = np.concatenate([hx.cells[:, list(t)][:, None, :] for t in _KUHN], axis=1).reshape(-1, 4)
     return Mesh(3, TET, hx.vertices, cells, (nx, ny, nz))
 
