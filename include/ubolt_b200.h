@@ -328,6 +328,7 @@ typedef struct {
    uint32_t timeouts;     /* bounded waits that gave up since the last status */
    int32_t kernel;        /* UBOLT_SWEEP_TASKS or UBOLT_SWEEP_WAVE: what ubolt_sweep (FP64) runs now */
    int64_t factor_bytes;  /* device bytes held by the factor stores (FP64 + FP32) */
+   int64_t factor_bytes_fp64;  /* of which the FP64 store (what one FP64 sweep reads) */
 } ubolt_sweep_info;
 
 /* The two sweep kernels. TASKS: persistent warps over (patch, ordinate)

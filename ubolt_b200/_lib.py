@@ -113,7 +113,7 @@ class SweepInfo(C.Structure):
     _fields_ = [("patch_size", C.c_int32), ("n_patches", C.c_int32), ("n_tasks", C.c_int64),
                 ("n_lagged", C.c_int64), ("n_split", C.c_int64), ("max_levels", C.c_int32), ("grid", C.c_int32),
                 ("total_levels", C.c_int64), ("timeouts", C.c_uint32), ("kernel", C.c_int32),
-                ("factor_bytes", C.c_int64)]
+                ("factor_bytes", C.c_int64), ("factor_bytes_fp64", C.c_int64)]
 
 
 class SolveOptions(C.Structure):

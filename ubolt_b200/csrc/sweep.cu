@@ -998,9 +998,13 @@ extern "C" int ubolt_sweep_status(ubolt_ctx *ctx, ubolt_sweep_info *info, void *
       info->timeouts = h[1];
       info->kernel = (pl->fac[0] && pl->fac_wave[0]) ? UBOLT_SWEEP_WAVE : UBOLT_SWEEP_TASKS;
       info->factor_bytes = 0;
+      info->factor_bytes_fp64 = 0;
       for (int which = 0; which < 2; which++)
-         if (pl->fac[which])
-            info->factor_bytes += pl->fac_wave[which] ? pl->wave_bytes[which] : FactorBytes(ctx, pl, which ? 4 : 8);
+         if (pl->fac[which]) {
+            const int64_t b = pl->fac_wave[which] ? pl->wave_bytes[which] : FactorBytes(ctx, pl, which ? 4 : 8);
+            info->factor_bytes += b;
+            if (which == 0) info->factor_bytes_fp64 = b;
+         }
    }
    if (h[0]) {
       cudaMemsetAsync(pl->ctrl + kCtrlError, 0, 2 * sizeof(uint32_t), s);
