@@ -29,7 +29,9 @@ int DsaCorrect(ubolt_ctx *ctx, const T *r, T *y, T *tmp, void *stream);
 bool SweepIsExact(ubolt_ctx *ctx);
 template <typename T>
 int SweepAffine(ubolt_ctx *ctx, const T *r0, const double *alpha, const double *phi, const double *rho, const T *u,
-                T *psi, void *stream, bool ordinate_major);
+                T *psi, void *stream, bool ordinate_major, bool inv_volume);
+template <typename T>
+int Sweep(ubolt_ctx *ctx, const T *q, T *psi, void *stream, bool ordinate_major);
 template <typename T>
 bool SweepWritesOrdinateMajor(ubolt_ctx *ctx);
 }  // namespace ubolt
@@ -324,6 +326,28 @@ __global__ void __launch_bounds__(256) OppositeScaleInPlaceKernel(S *__restrict_
    }
 }
 
+// The same on psi ordinate-major (y[a n_nodes + node]): each ordinate's run
+// swapped with its opposite's and scaled by the cell volume, one thread per
+// (pair, node), coalesced along the nodes
+template <typename S>
+__global__ void __launch_bounds__(256) OppositeScaleInPlaceOmKernel(S *__restrict__ y, const int32_t *__restrict__ opp,
+                                                                    const double *__restrict__ volume, int nb, int A,
+                                                                    int64_t n_nodes)
+{
+   const int64_t total = (int64_t)A * n_nodes;
+   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < total; k += (int64_t)gridDim.x * blockDim.x) {
+      const int a = (int)(k / n_nodes);
+      const int b = opp[a];
+      if (b < a) continue;
+      const int64_t node = k - (int64_t)a * n_nodes;
+      const double v = volume[node / nb];
+      S *ya = y + (int64_t)a * n_nodes + node, *yb = y + (int64_t)b * n_nodes + node;
+      const double va = (double)*ya, vb = (double)*yb;
+      *ya = (S)(vb * v);
+      if (b != a) *yb = (S)(va * v);
+   }
+}
+
 // The system GMRES iterates on: A = L - S, or its transpose for the adjoint
 template <typename T>
 int OperatorApply(ubolt_ctx *ctx, bool adjoint, const T *x, T *y, void *stream);
@@ -615,8 +639,13 @@ __global__ void __launch_bounds__(256) IsoScatterOmKernel(const S *__restrict__ 
         node += (int64_t)gridDim.x * blockDim.x) {
       double sum = 0.0;
       const S *zn = z + node;
+      if (w) {
 #pragma unroll 8
-      for (int a = 0; a < A; a++) sum += (double)w[a] * (double)zn[(int64_t)a * n_nodes];
+         for (int a = 0; a < A; a++) sum += (double)w[a] * (double)zn[(int64_t)a * n_nodes];
+      } else {
+#pragma unroll 8
+         for (int a = 0; a < A; a++) sum += (double)zn[(int64_t)a * n_nodes];
+      }
       phi_out[node] = phi_in[node] - (double)sigma_s[node / nb] * inv_W * sum;
    }
 }
@@ -680,16 +709,29 @@ static int IsoPrecondition(ubolt_ctx *ctx, bool adjoint, const S *r0, const doub
                            const double *rho, const S *u, S *t, S *z, S *tmp, int64_t n, int igrid, void *stream,
                            bool ordinate_major)
 {
-   if (!adjoint) return SweepAffine<S>(ctx, r0, alpha, phi, rho, u, z, stream, ordinate_major);
-   // L^{-T} = V P L^{-1} P V^{-1}: the expansion and P V^{-1} in one pass,
-   // the sweep, then V P in place
-   IsoExpandKernel<S><<<igrid, 256, 0, (cudaStream_t)stream>>>(r0, alpha, phi, rho, u, ctx->A, ctx->n_nodes, t,
-                                                               ctx->d_opp, ctx->d_volume, ctx->nb);
-   CountLaunch();
-   int rc = Sweep<S>(ctx, t, z, stream);
+   if (!adjoint) return SweepAffine<S>(ctx, r0, alpha, phi, rho, u, z, stream, ordinate_major, false);
+   // L^{-T} = V P L^{-1} P V^{-1}: the expansion and P V^{-1} in one pass
+   // (or, for an isotropic source, in the sweep's own read of it: u = w is
+   // symmetric under the opposite, so P V^{-1} E_w phi = E_w (phi / V)), the
+   // sweep, then V P in place
+   int rc = 0;
+   if (!r0 && ordinate_major) {
+      rc = SweepAffine<S>(ctx, nullptr, alpha, phi, rho, u, z, stream, true, true);
+   } else {
+      IsoExpandKernel<S><<<igrid, 256, 0, (cudaStream_t)stream>>>(r0, alpha, phi, rho, u, ctx->A, ctx->n_nodes, t,
+                                                                  ctx->d_opp, ctx->d_volume, ctx->nb);
+      CountLaunch();
+      rc = Sweep<S>(ctx, t, z, stream, ordinate_major);
+   }
    if (rc) return rc;
-   OppositeScaleInPlaceKernel<S><<<RunGrid(ctx->n_nodes), 256, 0, (cudaStream_t)stream>>>(z, ctx->d_opp, ctx->d_volume,
-                                                                                       ctx->nb, ctx->A, ctx->n_nodes);
+   if (ordinate_major)
+      OppositeScaleInPlaceOmKernel<S><<<(int)std::min<int64_t>((ctx->n_nodes * ctx->A + 255) / 256, 148 * 16), 256, 0,
+                                        (cudaStream_t)stream>>>(z, ctx->d_opp, ctx->d_volume, ctx->nb, ctx->A,
+                                                                ctx->n_nodes);
+   else
+      OppositeScaleInPlaceKernel<S><<<RunGrid(ctx->n_nodes), 256, 0, (cudaStream_t)stream>>>(z, ctx->d_opp,
+                                                                                          ctx->d_volume, ctx->nb,
+                                                                                          ctx->A, ctx->n_nodes);
    (void)tmp;
    (void)n;
    return CheckLaunch("adjoint pc");
@@ -719,10 +761,11 @@ static int GmresIso(ubolt_ctx *ctx, const ubolt_solver *ws, S *work, const S *b,
       kappa = (double)A;
    // Full-length vectors live in the (unused) plain basis: r0, t, tmp, then
    // the preconditioned vectors z_j = M^{-1} v_j of the cycle, kept so the
-   // update x += sum_j y_j z_j needs no further sweep. The forward sweep
-   // writes them ordinate-major (each task's psi contiguous, whole sectors
-   // written), read back by the scatter and the update
-   const bool om = !adjoint && SweepWritesOrdinateMajor<S>(ctx);
+   // update x += sum_j y_j z_j needs no further sweep. The sweep (forward,
+   // or the adjoint's reversed-ordinate one) writes them ordinate-major (each
+   // task's psi contiguous, whole sectors written), read back by the scatter
+   // and the update, wherever the task kernel runs
+   const bool om = SweepWritesOrdinateMajor<S>(ctx);
    S *r0 = work, *t = work + n, *tmp = work + 2 * n, *Zb = work + 3 * n;
    double *Phi = ws->Phi, *alpha = ws->alpha, *scal = ws->scal;
    std::vector<double> H((size_t)(m + 1) * m, 0.0), cs(m), sn(m), gv(m + 1), y(m), h1(m + 1), h2(m + 2),

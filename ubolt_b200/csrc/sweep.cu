@@ -160,6 +160,7 @@ struct SweepDev {
    const double *aff_alpha, *aff_phi, *aff_rho;
    const void *aff_u;
    int32_t aff_iso;  // r0 is isotropic (r0 = E rho): the input is u_a phi(node), q is not read
+   int32_t aff_inv_volume;  // with aff_iso: the input is u_a phi(node) / V(cell) (the adjoint's P V^{-1} E_w phi)
    // psi(c, j, a) at psi[c os_c + j os_j + a os_a]: UBOLT's row layout
    // (NB A, A, 1), or ordinate-major (NB, 1, n_cells NB), where a task's
    // cells of one ordinate are contiguous and it writes whole sectors
@@ -414,7 +415,7 @@ __global__ void __launch_bounds__(128, SweepMinBlocks<T, NB, PL>()) SweepKernel(
 #pragma unroll
             for (int j = 0; j < NB; j++) {
                const int64_t node = c * NB + j;
-               r[j] = s.aff_iso ? (T)(ua * s.aff_phi[node])
+               r[j] = s.aff_iso ? (T)(ua * s.aff_phi[node] / (s.aff_inv_volume ? (double)g.volume[c] : 1.0))
                                 : (T)(al * (double)q[node * A + a] + ua * (s.aff_phi[node] - al * s.aff_rho[node]));
             }
          } else {
@@ -675,6 +676,7 @@ static SweepDev DevPlan(const ubolt_sweep_plan *pl)
    s.aff_alpha = s.aff_phi = s.aff_rho = nullptr;
    s.aff_u = nullptr;
    s.aff_iso = 0;
+   s.aff_inv_volume = 0;
    return s;
 }
 
@@ -786,6 +788,7 @@ static int LaunchSweep(ubolt_ctx *ctx, const T *q, T *psi, cudaStream_t st, cons
       // One block per ordinate over the store in wave order (no sentinel fill)
       if (!fac) return UBOLT_ERR_CUDA;  // the failed launch set the message
       if (ordinate_major) return SetError(UBOLT_ERR_STATE, "the wave sweep writes the row layout only");
+      if (affine && affine->aff_inv_volume) return SetError(UBOLT_ERR_STATE, "the wave sweep takes no 1 / V source");
       WaveDev w = pl->wave[which];
       w.ctrl = pl->ctrl;
       w.spin_limit = pl->spin_limit;
@@ -828,6 +831,7 @@ static int LaunchSweep(ubolt_ctx *ctx, const T *q, T *psi, cudaStream_t st, cons
       s.aff_rho = affine->aff_rho;
       s.aff_u = affine->aff_u;
       s.aff_iso = affine->aff_iso;
+      s.aff_inv_volume = affine->aff_inv_volume;
    }
    s.unmet_task = pl->unmet_task;
    pl->unmet_task = -1;
@@ -839,15 +843,21 @@ static int LaunchSweep(ubolt_ctx *ctx, const T *q, T *psi, cudaStream_t st, cons
 }
 
 template <typename T>
-int Sweep(ubolt_ctx *ctx, const T *q, T *psi, void *stream)
+int Sweep(ubolt_ctx *ctx, const T *q, T *psi, void *stream, bool ordinate_major)
 {
    int rc = CheckReady(ctx, true);
    if (rc) return rc;
    if (!ctx->sweep && (rc = BuildSweepPlan(ctx, 0))) return rc;
    if (!q || !psi || (const void *)q == (const void *)psi)
       return SetError(UBOLT_ERR_ARG, "sweep: q and psi must be distinct device arrays");
-   UBOLT_DISPATCH(ctx->nb, ctx->F, return (LaunchSweep<T, NB_, F_>(ctx, q, psi, (cudaStream_t)stream)));
+   UBOLT_DISPATCH(ctx->nb, ctx->F,
+                  return (LaunchSweep<T, NB_, F_>(ctx, q, psi, (cudaStream_t)stream, nullptr, ordinate_major)));
    return SetError(UBOLT_ERR_STATE, "no sweep kernel for this shape");
+}
+template <typename T>
+int Sweep(ubolt_ctx *ctx, const T *q, T *psi, void *stream)
+{
+   return Sweep<T>(ctx, q, psi, stream, false);
 }
 
 // True where the sweep is L^{-1} exactly: a plan with no lagged coupling and
@@ -861,19 +871,22 @@ bool SweepIsExact(ubolt_ctx *ctx)
 // psi = L^{-1} (alpha r0 + E_u (phi - alpha rho)) with the input formed as
 // the sweep reads it (u = 1, or u_a = u[a]); alpha, phi, rho on the device.
 // r0 == nullptr: r0 is isotropic, r0 = E_u rho, and the input is E_u phi.
+// inv_volume (r0 == nullptr only): the input is u_a phi(node) / V(cell).
 template <typename T>
 int SweepAffine(ubolt_ctx *ctx, const T *r0, const double *alpha, const double *phi, const double *rho, const T *u,
-                T *psi, void *stream, bool ordinate_major)
+                T *psi, void *stream, bool ordinate_major, bool inv_volume)
 {
    int rc = CheckReady(ctx, true);
    if (rc) return rc;
    if (!ctx->sweep && (rc = BuildSweepPlan(ctx, 0))) return rc;
+   if (inv_volume && r0) return SetError(UBOLT_ERR_ARG, "sweep: the 1 / V source is isotropic only");
    SweepDev aff{};
    aff.aff_alpha = alpha;
    aff.aff_phi = phi;
    aff.aff_rho = rho;
    aff.aff_u = u;
    aff.aff_iso = r0 == nullptr;
+   aff.aff_inv_volume = inv_volume;
    UBOLT_DISPATCH(ctx->nb, ctx->F,
                   return (LaunchSweep<T, NB_, F_>(ctx, r0, psi, (cudaStream_t)stream, &aff, ordinate_major)));
    return SetError(UBOLT_ERR_STATE, "no sweep kernel for this shape");
@@ -890,9 +903,11 @@ bool SweepWritesOrdinateMajor(ubolt_ctx *ctx)
 }
 
 template int SweepAffine<double>(ubolt_ctx *, const double *, const double *, const double *, const double *,
-                                 const double *, double *, void *, bool);
+                                 const double *, double *, void *, bool, bool);
 template int SweepAffine<float>(ubolt_ctx *, const float *, const double *, const double *, const double *,
-                                const float *, float *, void *, bool);
+                                const float *, float *, void *, bool, bool);
+template int Sweep<double>(ubolt_ctx *, const double *, double *, void *, bool);
+template int Sweep<float>(ubolt_ctx *, const float *, float *, void *, bool);
 template bool SweepWritesOrdinateMajor<double>(ubolt_ctx *);
 template bool SweepWritesOrdinateMajor<float>(ubolt_ctx *);
 template int Sweep<double>(ubolt_ctx *, const double *, double *, void *);
@@ -950,7 +965,7 @@ static int SweepIso(ubolt_ctx *ctx, const double *phi, const T *u, T *psi, int o
    if (!phi || !psi) return SetError(UBOLT_ERR_ARG, "sweep_iso: NULL array");
    if (ordinate_major && !SweepWritesOrdinateMajor<T>(ctx))
       return SetError(UBOLT_ERR_STATE, "sweep_iso: the wave kernel runs here, and it writes the row layout only");
-   return SweepAffine<T>(ctx, nullptr, nullptr, phi, nullptr, u, psi, stream, ordinate_major != 0);
+   return SweepAffine<T>(ctx, nullptr, nullptr, phi, nullptr, u, psi, stream, ordinate_major != 0, false);
 }
 
 extern "C" int ubolt_sweep_iso(ubolt_ctx *ctx, const double *phi, const double *u, double *psi, int ordinate_major,
