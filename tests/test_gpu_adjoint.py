@@ -176,3 +176,38 @@ def test_gradient_matches_oracle_adjoint():
     gg = T.response_source(ctx, dev(det))
     assert np.abs(gg.cpu().numpy() - gvec).max() <= 1e-14 * np.abs(gvec).max()
     ctx.close()
+
+
+def test_mixed_gradient_on_jittered_tets_matches_central_differences():
+    """The combined workload's shape, small: jittered Kuhn tetrahedra, DG1,
+    S4, lognormal(0, 1) sigma_t, c ~ U(0.5, 0.999), a central source box and
+    a corner detector box; the gradient of the mixed FP32 + FP64-refinement
+    solve with respect to every cell's sigma_t against central differences
+    of FP64 forward solves along seeded directions."""
+    rng = np.random.default_rng(44)
+    mesh = P.box_tets(4, 4, 4, jitter=0.2, rng=rng)
+    g = P.build_geometry(mesh, 1)
+    q = P.lqn(3, 4)
+    nc = g.n_cells
+    st = rng.lognormal(0.0, 1.0, nc)
+    ss = st * rng.uniform(0.5, 0.999, nc)
+    cen = g.centroid.reshape(nc, 3)
+    src = np.all((cen > 0.25) & (cen < 0.75), axis=1).astype(float)
+    det = np.all(cen > 0.55, axis=1).astype(float)
+    ctx = T.Context(g, q)
+    mixed = T.DetectorResponse(ctx, src, det, rtol=1e-12, max_it=3000, precision="mixed")
+    plain = T.DetectorResponse(ctx, src, det, rtol=1e-13, max_it=3000)
+    sigma_t = dev(st).requires_grad_(True)
+    J = mixed(sigma_t, dev(ss))
+    (gt,) = torch.autograd.grad(J, (sigma_t,))
+    for _ in range(3):
+        d = rng.standard_normal(nc)
+        d /= np.linalg.norm(d)
+        h = 1e-6
+        with torch.no_grad():
+            jp = plain(dev(st * (1 + h * d)), dev(ss)).item()
+            jm = plain(dev(st * (1 - h * d)), dev(ss)).item()
+        fd = (jp - jm) / (2 * h)
+        ad = float(torch.dot(gt, dev(st * d)))
+        assert abs(fd - ad) <= 1e-5 * abs(ad), (fd, ad)
+    ctx.close()
