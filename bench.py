@@ -456,6 +456,106 @@ def workload_tet44(args, stream):
     return out
 
 
+def workload_cg256(args, stream):
+    """The CG-SUPG backend at the named problem's size: 256 x 256 jittered
+    quads (66,049 vertices), S8, one group, the config-1 cross-section law
+    per element; GMRES with point Jacobi, and with the vertex DSA stage, FP64
+    and mixed, to 1e-8; the SUPG operator apply alone."""
+    import torch
+    from ubolt_b200 import problem as P
+    from ubolt_b200 import transport as T
+    t0 = time.perf_counter()
+    n = max(4, int(round(256 * args.scale)))
+    s_mesh, s_xs, _, _ = P._streams(6)
+    mesh = P.box_quads(n, n, jitter=0.2, rng=s_mesh)
+    g = P.build_cg_geometry(mesh)
+    q = P.lqn(2, 8)
+    ne = g.n_elements
+    st = s_xs.lognormal(0.0, 0.5, ne)
+    ss = st * s_xs.uniform(0.3, 0.99, ne)
+    ctx = T.Context(g, q)
+    keep = (torch.tensor(st, device="cuda"), torch.tensor(ss, device="cuda"))
+    ctx.set_group(*keep)
+    b = ctx.vector(fill=0.0)
+    src = torch.ones(ne, dtype=torch.float64, device="cuda")
+    from ubolt_b200 import _lib
+    _lib.check(_lib.lib.ubolt_add_source(ctx.handle, T._p(src), T._p(b), T._stream()))
+    out = {"workload": f"cg{n}_s8: CG-SUPG (Q1) on {n}x{n} jittered quads, {g.n_vertices} vertices, S8, 1 group",
+           "rows": ctx.n_rows, "setup_s": time.perf_counter() - t0}
+    xs = {}
+    for key, opts in (("jacobi_fp64", dict(precision="fp64", pc="block")),
+                      ("jacobi_dsa_fp64", dict(precision="fp64", pc="block+dsa")),
+                      ("jacobi_dsa_mixed", dict(precision="mixed", pc="block+dsa"))):
+        if "dsa" in key:
+            dsa = T.DSAPrecon(ctx)
+            dsa.set_group()
+        solver = T.TransportSolver(ctx, rtol=1e-8, restart=60, max_it=3000, **opts)
+        x = ctx.vector(fill=0.0)
+        res = {}
+
+        def run():
+            res["x"], res["stats"] = solver.solve(b, x)
+
+        ms = _events_ms(run, stream, reps=args.reps, warm=1)
+        xs[key] = res["x"].clone()
+        out[key] = {"s_per_solve": ms / 1e3, "iterations": res["stats"]["iterations"],
+                    "residual": res["stats"]["residual"]}
+    phi = T.angular_integral(ctx, xs["jacobi_fp64"])
+    for key in ("jacobi_dsa_fp64", "jacobi_dsa_mixed"):
+        out[key]["phi_rel_err_vs_jacobi_fp64"] = float((T.angular_integral(ctx, xs[key]) - phi).norm() / phi.norm())
+    A = T.TransportOperator(ctx)
+    xr = torch.rand(ctx.n_rows, dtype=torch.float64, device="cuda")
+    yr = torch.empty_like(xr)
+    us = _events_ms(lambda: A.mult(xr, yr), stream, reps=20, warm=3) * 1e3
+    byts = 2 * ctx.n_rows * 8 + 2 * ne * 8
+    out["apply_fp64"] = {"us": us, "bytes": byts, "gbs": byts / us / 1e3}
+    ctx.close()
+    return out
+
+
+def workload_upscatter(args, stream):
+    """The upscatter outer iteration: the 128 x 128 triangle mesh of the
+    named problem's family, DG1, S8, three groups with thermal upscatter
+    (2 -> 1), block Gauss-Seidel over the thermal block to an error
+    estimate of 1e-8, with the angular and the moments store."""
+    import torch
+    from ubolt_b200 import problem as P
+    from ubolt_b200 import transport as T
+    n = max(4, int(round(128 * args.scale)))
+    s_mesh, s_xs, _, _ = P._streams(7)
+    mesh = P.box_tris(n, n, jitter=0.2, rng=s_mesh, tile=8, diagonals="random")
+    g = P.build_geometry(mesh, 1)
+    q = P.lqn(2, 8)
+    nc, G = g.n_cells, 3
+    st = s_xs.lognormal(0.0, 0.5, (G, nc))
+    ss = np.zeros((G, G, nc))
+    for gg in range(G):
+        ss[gg, gg] = 0.5 * st[gg]
+    ss[0, 1], ss[0, 2], ss[1, 2] = 0.2 * st[0], 0.1 * st[0], 0.25 * st[1]
+    ss[2, 1] = 0.3 * st[2]
+    src = np.zeros((G, nc))
+    src[0] = 1.0
+    ctx = T.Context(g, q)
+    tables = T.group_tables(ctx, st, ss, src)
+    solver = T.TransportSolver(ctx, rtol=1e-8, restart=30, max_it=500)
+    out = {"workload": f"tri{n}_s8_g3_up: 2D DG1, {nc} triangles, S8, 3 groups, thermal upscatter 2 -> 1",
+           "rows_per_group": ctx.n_rows}
+    for store in ("angular", "moments"):
+        info = {}
+        res = {}
+
+        def run():
+            info.clear()
+            res["phis"], _ = T.solve_groups(ctx, *tables, solver=solver, outer_rtol=1e-8, outer_store=store,
+                                            outer_info=info)
+
+        ms = _events_ms(run, stream, reps=max(1, args.reps), warm=1)
+        out[store] = {"s_per_solve": ms / 1e3, "outer_iterations": info.get("outer_iterations"),
+                      "error_estimate": info.get("error_estimate"), "converged": info.get("converged")}
+    ctx.close()
+    return out
+
+
 def run_workload(args):
     """--workload hex128 | tet44: the other solve configs, FP64 and mixed, as one
     JSON line each (no CPU baseline: the restatement would take hours here)."""
@@ -748,6 +848,8 @@ def main():
         extra["hex128"] = workload_hex128(args, stream)
         torch.cuda.empty_cache()
         extra["tet44"] = workload_tet44(args, stream)
+        extra["cg256"] = workload_cg256(args, stream)
+        extra["upscatter"] = workload_upscatter(args, stream)
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "s/solve", "n_gpus": world, "steps": args.steps,
