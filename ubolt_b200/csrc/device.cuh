@@ -85,6 +85,36 @@ __device__ __forceinline__ void CpAsync(void *smem_dst, const void *src)
    const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(d), "l"(src), "n"(BYTES) : "memory");
 }
+// An L2 policy that evicts a line first: for data read once per launch
+// (streamed through, not to displace what other warps are about to read)
+__device__ __forceinline__ uint64_t EvictFirstPolicy()
+{
+   uint64_t p;
+   asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+   return p;
+}
+// CpAsync with an L2 cache policy
+template <int BYTES>
+__device__ __forceinline__ void CpAsyncHint(void *smem_dst, const void *src, uint64_t policy)
+{
+   const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+   asm volatile("cp.async.ca.shared.global.L2::cache_hint [%0], [%1], %2, %3;" ::"r"(d), "l"(src), "n"(BYTES),
+                "l"(policy)
+                : "memory");
+}
+// A load with an L2 cache policy
+__device__ __forceinline__ double LoadHint(const double *p, uint64_t policy)
+{
+   double v;
+   asm volatile("ld.global.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(policy));
+   return v;
+}
+__device__ __forceinline__ float LoadHint(const float *p, uint64_t policy)
+{
+   float v;
+   asm volatile("ld.global.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(policy));
+   return v;
+}
 __device__ __forceinline__ void CpAsyncWaitAll() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 __device__ __forceinline__ void CpAsyncCommit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 // Wait until at most N of this thread's committed groups are still in flight

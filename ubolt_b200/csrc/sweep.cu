@@ -321,6 +321,9 @@ __global__ void __launch_bounds__(128, SweepMinBlocks<T, NB, PL>()) SweepKernel(
    const size_t R = (size_t)NB * NB * (1 + S);
    constexpr int GS = GStride(NB, (int)sizeof(T));
    const int PS = PosStride(S, NB, (int)sizeof(T));
+   // The factor store is read once per sweep: its lines go first from L2, so
+   // that they do not push out psi and the schedule other warps are reading
+   const uint64_t stream_once = EvictFirstPolicy();
    // The task's five scalars, one lane each, in one round trip
    auto scalars = [&](int64_t tt) -> int64_t {
       if (tt >= s.n_tasks) return 0;
@@ -383,13 +386,13 @@ __global__ void __launch_bounds__(128, SweepMinBlocks<T, NB, PL>()) SweepKernel(
 #pragma unroll
                   for (int ii = 0; ii < NB; ii++)
 #pragma unroll
-                     for (int j = 0; j < NB; j++) W[k][ii][j] = ft[(size_t)(ii * NB + j) * ncell];
+                     for (int j = 0; j < NB; j++) W[k][ii][j] = LoadHint(ft + (size_t)(ii * NB + j) * ncell, stream_once);
                }
 #pragma unroll
                for (int e = 0; e < SM * NB * NB; e++)
                   if (e < S * NB * NB)
-                     CpAsync<sizeof(T)>(G + (size_t)i * PS + (e / (NB * NB)) * GS + e % (NB * NB),
-                                        ft + (size_t)(NB * NB + e) * ncell);
+                     CpAsyncHint<sizeof(T)>(G + (size_t)i * PS + (e / (NB * NB)) * GS + e % (NB * NB),
+                                            ft + (size_t)(NB * NB + e) * ncell, stream_once);
             }
          }
          if constexpr (kPrefetch) {
