@@ -343,7 +343,8 @@ typedef struct {
  * TASKS otherwise. */
 enum { UBOLT_SWEEP_AUTO = 0, UBOLT_SWEEP_TASKS = 1, UBOLT_SWEEP_WAVE = 2 };
 
-/* Build the sweep plan: patches of patch_size consecutive cells (0 picks 64;
+/* Build the sweep plan: patches of patch_size consecutive cells (0 picks 64,
+ * or 24 on tetrahedra;
  * at most 256), per-ordinate upwind orders, task list; then reserve the
  * factor stores (see ubolt_sweep_set_factor_limit). Host work, one upload
  * and the sweep's only device allocations; independent of the group.

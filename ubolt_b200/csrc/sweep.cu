@@ -43,6 +43,18 @@ constexpr int kCtrlCounter = 0, kCtrlError = ubolt::kSweepCtrlError, kCtrlNever 
 constexpr int kSweepBlocksPerSm = 8;  // of 4 warps
 constexpr int kDefaultPatch = 64;
 
+// The default patch: half a tile of the mesh builders' cell numbering (8 x 8
+// quads, 4^3 hexes), and four cubes' worth of Kuhn tetrahedra. Measured per
+// isotropic-source sweep at S8 (FP64 / FP32): 256^2 triangles 0.89 / 0.78 ms
+// at 64 cells against 0.97 / 0.83 at 32; 44^3 Kuhn tets 15.3 / 12.0 ms at 24
+// against 18.2 / 14.1 at 32 and 23.4 / 15.8 at 64. On the 128^3 hex box 64
+// stays: the 4-group FP64 solve, whose factors are built in the sweep, took
+// 1.64 s at 64 against 1.79 s at 32 (the mixed solve 1.08 / 1.07 s)
+static int DefaultPatch(const ubolt_ctx *ctx)
+{
+   return (ctx->dim == 3 && ctx->F == 4) ? 24 : kDefaultPatch;
+}
+
 struct ubolt_sweep_plan {
    int32_t P = 0, n_patches = 0, A = 0;
    int64_t n_tasks = 0, n_lagged = 0, n_split = 0, total_levels = 0;
@@ -586,7 +598,7 @@ int BuildSweepPlan(ubolt_ctx *ctx, int patch_size)
 {
    if (int rc = RequireDg(ctx, "the sweep")) return rc;
    const int64_t nc = ctx->n_cells;
-   int P = patch_size > 0 ? patch_size : kDefaultPatch;
+   int P = patch_size > 0 ? patch_size : DefaultPatch(ctx);
    if (P > 256) P = 256;
    if (P > nc) P = (int)nc;
    if (((nc + P - 1) / P) * (int64_t)ctx->A * 4 >= INT32_MAX) return SetError(UBOLT_ERR_ARG, "too many sweep tasks");
