@@ -104,7 +104,7 @@ __global__ void __launch_bounds__(256) CgApplyKernel(const CgDev<T> d, const T *
    for (int s = d.star_off[i]; s < s1; s++) {
       const int e = d.star_elem[s];
       const T st = d.sigma_t[e];
-      const T tau = SupgTau<T, DIM, NV>(d.cgrad + (int64_t)e * NV * DIM, om, st, d.zeta);
+      const T tau = d.tau[(int64_t)e * d.A + a];
       const T *rec = d.rec + (int64_t)s * NV * P;
       const int32_t *col = d.cols + (int64_t)s * NV;
       T srow = T(0);
@@ -252,7 +252,41 @@ static CgDev<T> DevOf(const ubolt_ctx *ctx)
    else d = ctx->cg->d32;
    d.sigma_t = ctx->geom<T>().sigma_t;
    d.sigma_s = ctx->geom<T>().sigma_s;
+   if constexpr (std::is_same<T, double>::value) d.tau = ctx->cg->tau64;
+   else d.tau = ctx->cg->tau32;
    return d;
+}
+
+// tau[e A + a] of the current group, in FP64 and rounded to FP32
+template <int DIM, int NV>
+__global__ void __launch_bounds__(256) CgTauKernel(const CgDev<double> d, int64_t n_elements,
+                                                   double *__restrict__ tau64, float *__restrict__ tau32)
+{
+   const int64_t total = n_elements * d.A;
+   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < total; k += (int64_t)gridDim.x * blockDim.x) {
+      const int64_t e = k / d.A;
+      const int a = (int)(k - e * d.A);
+      double om[DIM];
+#pragma unroll
+      for (int c = 0; c < DIM; c++) om[c] = d.omega[3 * a + c];
+      const double t = SupgTau<double, DIM, NV>(d.cgrad + e * NV * DIM, om, d.sigma_t[e], d.zeta);
+      tau64[k] = t;
+      tau32[k] = (float)t;
+   }
+}
+
+// The tau table for the current group (a kernel launch, no allocation)
+static int EnsureTau(ubolt_ctx *ctx, cudaStream_t s)
+{
+   ubolt_cg *cg = ctx->cg;
+   if (cg->tau_epoch == ctx->group_epoch) return UBOLT_OK;
+   const CgDev<double> d = DevOf<double>(ctx);
+   const int64_t total = cg->n_elements * ctx->A;
+   const int grid = (int)std::min<int64_t>((total + 255) / 256, 148 * 16);
+   UBOLT_CG_DISPATCH(cg->dim, cg->nv, (CgTauKernel<D_, N_><<<grid, 256, 0, s>>>(d, cg->n_elements, cg->tau64, cg->tau32)));
+   const int rc = CheckLaunch("cg tau");
+   if (!rc) cg->tau_epoch = ctx->group_epoch;
+   return rc;
 }
 
 template <typename T>
@@ -260,6 +294,7 @@ int CgApply(ubolt_ctx *ctx, const T *x, T *y, bool scatter, void *stream)
 {
    ubolt_cg *cg = ctx->cg;
    cudaStream_t s = (cudaStream_t)stream;
+   if (int rc = EnsureTau(ctx, s)) return rc;
    const CgDev<T> d = DevOf<T>(ctx);
    T *phi = nullptr;
    if (scatter) {
@@ -577,6 +612,10 @@ extern "C" int ubolt_ctx_create_cg(const ubolt_cg_geometry *geom, const ubolt_qu
    cg->jinv64 = static_cast<double *>(p);
    if ((rc = CtxAlloc(ctx, ctx->n_rows * sizeof(float), &p))) return fail(rc);
    cg->jinv32 = static_cast<float *>(p);
+   if ((rc = CtxAlloc(ctx, (size_t)ne * ctx->A * sizeof(double), &p))) return fail(rc);
+   cg->tau64 = static_cast<double *>(p);
+   if ((rc = CtxAlloc(ctx, (size_t)ne * ctx->A * sizeof(float), &p))) return fail(rc);
+   cg->tau32 = static_cast<float *>(p);
 
    // ~~~~~ Host copies for the DSA
    cg->elem_vertex.assign(geom->elem_vertex, geom->elem_vertex + ne * nv);

@@ -33,6 +33,7 @@ struct CgDev {
    const T *omega;            // [A][3]
    const int32_t *refl;       // [3][A]
    const T *sigma_t, *sigma_s;  // [n_elements] the group's
+   const T *tau;                // [n_elements][A] the group's SUPG tau (the apply's; built per group)
 };
 
 }  // namespace ubolt
@@ -50,6 +51,12 @@ struct ubolt_cg {
    double *jinv64 = nullptr;
    float *jinv32 = nullptr;
    uint64_t jacobi_epoch = 0;  // the group epoch jinv was built for (0: never)
+   // tau per (element, ordinate) of the current group, both precisions: it
+   // depends on the group's sigma_t, not on the vector, and each of an
+   // element's vertices would recompute it per row
+   double *tau64 = nullptr;
+   float *tau32 = nullptr;
+   uint64_t tau_epoch = 0;
    // Host copies the DSA assembles from
    std::vector<int64_t> elem_vertex, elem_face_neighbour, bface_offset;
    std::vector<int32_t> elem_face_bc, bface_bc;
