@@ -79,16 +79,43 @@ namespace ubolt {
 constexpr int kRedThreads = 256;
 constexpr int kChunk = 8;
 
+// One Gram-Schmidt pass's scalars of the compressed basis, formed by the
+// multi-dot's last block once every dot is in (see IsoCombine below)
+struct IsoCombineArgs {
+   double *alpha = nullptr;
+   int j1 = 0, first = 0, on = 0;
+   double rp2 = 0.0, kappa = 0.0;
+};
+
+// h[i] = alpha[i] alpha_w |r_perp|^2 + kappa d[i] for i < j1 (in place over
+// d), then alpha[j1] = alpha_w - sum_i h[i] alpha[i]: one Gram-Schmidt
+// pass's scalars. alpha_w is alpha[j1], or on the first pass alpha[j1 - 1]
+// (the new vector w = v_j - ... starts with v_j's scalar). One thread.
+__device__ __forceinline__ void IsoCombine(double *__restrict__ d, const IsoCombineArgs &c)
+{
+   double *alpha = c.alpha;
+   const int j1 = c.j1;
+   const double aw = c.first ? alpha[j1 - 1] : alpha[j1];
+   double upd = 0.0;
+   for (int i = 0; i < j1; i++) {
+      const double h = alpha[i] * aw * c.rp2 + c.kappa * d[i];
+      d[i] = h;
+      upd += h * alpha[i];
+   }
+   alpha[j1] = aw - upd;
+}
+
 // h[i0 + i] = V_{i0+i} . w for i < nc: each block's share to
 // partial[blk][i0 + i], then the last block to finish (an integer counter,
 // reset by that block) adds the shares in a fixed order, one warp per value:
 // per-lane strided sums, then a shuffle tree, the same every run. No block
-// waits on another.
+// waits on another. With cmb.on (the last chunk of a compressed-basis pass)
+// that block then forms the pass's scalars from all of h.
 template <typename S>
 __global__ void __launch_bounds__(kRedThreads) MultiDotKernel(const S *__restrict__ V, int64_t n, int i0, int nc,
                                                               const S *__restrict__ w, double *__restrict__ partial,
                                                               int stride, double *__restrict__ h,
-                                                              unsigned *__restrict__ count)
+                                                              unsigned *__restrict__ count, IsoCombineArgs cmb)
 {
    double acc[kChunk];
 #pragma unroll
@@ -129,6 +156,10 @@ __global__ void __launch_bounds__(kRedThreads) MultiDotKernel(const S *__restric
       if (lane == 0) h[i0 + warp] = s;
    }
    if (threadIdx.x == 0) *count = 0;
+   if (cmb.on) {
+      __syncthreads();
+      if (threadIdx.x == 0) IsoCombine(h, cmb);
+   }
 }
 
 // out[i] = sum over blocks of partial[blk][i]
@@ -197,15 +228,19 @@ static int GridFor(int64_t n)
 
 // h[0..nv) = V^T w, computed on the device
 template <typename S>
-static void MultiDot(const ubolt_solver *ws, const S *V, int nv, const S *w, int64_t n, double *h, cudaStream_t s)
+static void MultiDot(const ubolt_solver *ws, const S *V, int nv, const S *w, int64_t n, double *h, cudaStream_t s,
+                     IsoCombineArgs cmb = IsoCombineArgs())
 {
    const int stride = ws->restart + 2;
    // Four elements per thread: a short (node-space) vector still spreads
    // over a few hundred blocks, and the partials to reduce stay few
    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(ws->red_blocks, n / (4 * kRedThreads)));
-   for (int i0 = 0; i0 < nv; i0 += kChunk)
+   for (int i0 = 0; i0 < nv; i0 += kChunk) {
+      IsoCombineArgs c = cmb;
+      c.on = cmb.on && i0 + kChunk >= nv;  // after the last chunk's dots
       MultiDotKernel<S><<<blocks, kRedThreads, 0, s>>>(V, n, i0, std::min(kChunk, nv - i0), w, ws->partial, stride,
-                                                       h, ws->md_count);
+                                                       h, ws->md_count, c);
+   }
    CountLaunch((nv + kChunk - 1) / kChunk);
 }
 
@@ -684,23 +719,6 @@ __global__ void __launch_bounds__(256) MultiAxpyOmKernel(const S *__restrict__ Z
    }
 }
 
-// h[i] = alpha[i] alpha_w |r_perp|^2 + kappa d[i] for i < j1 (in place over
-// d), then alpha[j1] = alpha_w - sum_i h[i] alpha[i]: one Gram-Schmidt
-// pass's scalars. alpha_w is alpha[j1], or on the first pass alpha[j1 - 1]
-// (the new vector w = v_j - ... starts with v_j's scalar)
-__global__ void IsoCombineKernel(double *__restrict__ d, double *__restrict__ alpha, int j1, double rp2, double kappa,
-                                 int first)
-{
-   if (threadIdx.x != 0 || blockIdx.x != 0) return;
-   const double aw = first ? alpha[j1 - 1] : alpha[j1];
-   double upd = 0.0;
-   for (int i = 0; i < j1; i++) {
-      const double h = alpha[i] * aw * rp2 + kappa * d[i];
-      d[i] = h;
-      upd += h * alpha[i];
-   }
-   alpha[j1] = aw - upd;
-}
 
 // z = M^{-1} (alpha r_perp + E_u phi). The forward sweep forms its input as
 // it reads it; the adjoint's reversed-ordinate sweep takes it expanded in t.
@@ -832,10 +850,16 @@ static int GmresIso(ubolt_ctx *ctx, const ubolt_solver *ws, S *work, const S *b,
          // Classical Gram-Schmidt, twice, in the compressed inner product
          for (int pass = 0; pass < 2; pass++) {
             double *dh = pass ? dh2 : dh1;
-            MultiDot<double>(ws, Phi, j + 1, pn, nn, dh, s);
-            IsoCombineKernel<<<1, 32, 0, s>>>(dh, alpha, j + 1, rp2, kappa, pass == 0);
+            IsoCombineArgs cmb;
+            cmb.alpha = alpha;
+            cmb.j1 = j + 1;
+            cmb.first = pass == 0;
+            cmb.on = 1;
+            cmb.rp2 = rp2;
+            cmb.kappa = kappa;
+            MultiDot<double>(ws, Phi, j + 1, pn, nn, dh, s, cmb);
             MultiAxpyKernel<double><<<igrid, 256, 0, s>>>(Phi, nn, j + 1, dh, -1.0, pn, 1);
-            CountLaunch(2);
+            CountLaunch();
          }
          MultiDot<double>(ws, pn, 1, pn, nn, dh2 + j + 1, s);
          ToHost3(ws, MailRuns{{dh1, dh2, alpha + j + 1}, {kMbH1, kMbH1 + (m + 2), kMbScalars}, {j + 1, j + 2, 1}}, s);
