@@ -312,17 +312,17 @@ __global__ void __launch_bounds__(128) FactorKernel(const DevGeom<T> g, const Sw
 // Resident blocks of 4 warps the compiler should fit per SM: the sweep is
 // bound by per-task latency, and FP64 nb <= 3 with one cell per lane fits a
 // fifth block without spilling (with two, the spills cost more than the
-// block). With two cells per lane FP64 keeps a fourth block (at most 128
-// registers, no spill): left free it took 134 and three blocks, and the
-// 256^2 triangle sweep 0.969 ms against 0.941
-template <typename T, int NB, int PL>
+// block). On triangles with two cells per lane FP64 keeps a fourth block
+// (at most 128 registers, no spill): left free it took 134 and three
+// blocks, and the 256^2 triangle sweep 0.969 ms against 0.941
+template <typename T, int NB, int F, int PL>
 constexpr int SweepMinBlocks()
 {
-   return (sizeof(T) == 8 && NB <= 3 && PL == 1) ? 5 : (sizeof(T) == 8 && NB <= 3 && PL == 2) ? 4 : 1;
+   return (sizeof(T) == 8 && NB <= 3 && PL == 1) ? 5 : (sizeof(T) == 8 && NB <= 3 && F == 3 && PL == 2) ? 4 : 1;
 }
 
 template <typename T, int NB, int F, int PL, bool CACHED>
-__global__ void __launch_bounds__(128, SweepMinBlocks<T, NB, PL>()) SweepKernel(const DevGeom<T> g, const SweepDev s, const T *__restrict__ q,
+__global__ void __launch_bounds__(128, SweepMinBlocks<T, NB, F, PL>()) SweepKernel(const DevGeom<T> g, const SweepDev s, const T *__restrict__ q,
                                                    T *__restrict__ psi, const T *__restrict__ fac)
 {
    extern __shared__ __align__(16) unsigned char smem_raw[];
