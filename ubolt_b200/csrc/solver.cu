@@ -105,6 +105,34 @@ __device__ __forceinline__ void IsoCombine(double *__restrict__ d, const IsoComb
    alpha[j1] = aw - upd;
 }
 
+// The new Arnoldi vector's norm from its two parts, hn = sqrt(alpha_w^2
+// |r_perp|^2 + kappa |phi_w|^2); where it is positive and finite, alpha[j1]
+// = alpha_w / hn and inv[0] = 1 / hn, else inv[0] = 1 (the vector is left as
+// it is; the host sees the same hn and stops). The host forms the same hn
+// from the same values for the Hessenberg column.
+__global__ void IsoNormalizeKernel(const double *__restrict__ phi2, double *__restrict__ alpha, int j1, double rp2,
+                                   double kappa, double *__restrict__ inv)
+{
+   if (threadIdx.x != 0 || blockIdx.x != 0) return;
+   const double aw = alpha[j1];
+   // Rounded step by step (no fused multiply-add), as the host's expression is
+   const double hn = sqrt(__dadd_rn(__dmul_rn(__dmul_rn(aw, aw), rp2), __dmul_rn(kappa, phi2[0])));
+   if (hn > 0.0 && isfinite(hn)) {
+      alpha[j1] = aw / hn;
+      inv[0] = 1.0 / hn;
+   } else {
+      inv[0] = 1.0;
+   }
+}
+
+// x *= s[0], s on the device
+__global__ void ScaleByDeviceKernel(double *__restrict__ x, const double *__restrict__ sp, int64_t n)
+{
+   const double sc = sp[0];
+   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+      x[k] = sc * x[k];
+}
+
 // h[i0 + i] = V_{i0+i} . w for i < nc: each block's share to
 // partial[blk][i0 + i], then the last block to finish (an integer counter,
 // reset by that block) adds the shares in a fixed order, one warp per value:
@@ -863,6 +891,11 @@ static int GmresIso(ubolt_ctx *ctx, const ubolt_solver *ws, S *work, const S *b,
          }
          MultiDot<double>(ws, pn, 1, pn, nn, dh2 + j + 1, s);
          ToHost3(ws, MailRuns{{dh1, dh2, alpha + j + 1}, {kMbH1, kMbH1 + (m + 2), kMbScalars}, {j + 1, j + 2, 1}}, s);
+         // The new vector normalised on the device, behind the mailbox
+         // copy, so that the next sweep waits on nothing the host sends
+         IsoNormalizeKernel<<<1, 32, 0, s>>>(dh2 + j + 1, alpha, j + 1, rp2, kappa, scal + 3);
+         ScaleByDeviceKernel<<<igrid, 256, 0, s>>>(pn, scal + 3, nn);
+         CountLaunch(2);
          if ((rc = CudaCheck(cudaStreamSynchronize(s), "gmres"))) return rc;
          std::copy(ws->mb_h + kMbH1, ws->mb_h + kMbH1 + j + 1, h1.begin());
          std::copy(ws->mb_h + kMbH1 + (m + 2), ws->mb_h + kMbH1 + (m + 2) + j + 2, h2.begin());
@@ -872,12 +905,7 @@ static int GmresIso(ubolt_ctx *ctx, const ubolt_solver *ws, S *work, const S *b,
          const double hn = std::sqrt(aw * aw * rp2 + kappa * h2[j + 1]);
          if (!std::isfinite(hn)) return SetError(UBOLT_ERR_NONFINITE, "GMRES Arnoldi vector is not finite");
          for (int i = 0; i <= j; i++) H[i * m + j] = h1[i] + h2[i];
-         if (hn > 0.0) {
-            ScaleKernel<double, double><<<igrid, 256, 0, s>>>(pn, pn, 1.0 / hn, nn);
-            CountLaunch();
-            alpha_h[j + 1] = aw / hn;
-            ToDevice(ws, &alpha_h[j + 1], alpha + j + 1, kMbScalars, 1, s);
-         }
+         if (hn > 0.0) alpha_h[j + 1] = aw / hn;  // as the device has it
          for (int i = 0; i < j; i++) {
             const double tt = cs[i] * H[i * m + j] + sn[i] * H[(i + 1) * m + j];
             H[(i + 1) * m + j] = -sn[i] * H[i * m + j] + cs[i] * H[(i + 1) * m + j];
